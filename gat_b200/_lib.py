@@ -1,0 +1,76 @@
+"""ctypes binding of the C ABI declared in include/gat_b200.h.
+
+The shared library is built in-tree by gat_b200/build.py. There is no fallback: if the library
+is missing or fails to load, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgat_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: run `python -m gat_b200.build` (needs nvcc)")
+
+lib = C.CDLL(LIB_PATH)
+
+c_int, c_i64, c_u64, c_f, c_d, c_p = C.c_int, C.c_int64, C.c_uint64, C.c_float, C.c_double, C.c_void_p
+P_i32 = C.POINTER(C.c_int32)
+P_i64 = C.POINTER(C.c_int64)
+P_f32 = C.POINTER(C.c_float)
+
+
+class MBB(C.Structure):
+    """gat_mbb, field order of the reference's MBB (MBB.h:5)."""
+
+    _fields_ = [("xmin", c_f), ("ymin", c_f), ("xmax", c_f), ("ymax", c_f)]
+
+
+GAT_OK, GAT_ERR_ARG, GAT_ERR_OOM, GAT_ERR_CUDA, GAT_ERR_TRUNCATED, GAT_ERR_TIMEOUT, GAT_ERR_STATE = range(7)
+GAT_INDEX_GRID, GAT_INDEX_STIG, GAT_INDEX_FSG = 0, 1, 2
+GAT_RESULT_IDS, GAT_RESULT_POINTS = 0, 1
+GAT_EXEC_PLAIN, GAT_EXEC_BATCHED = 0, 1
+GAT_LEN_UNIFORM, GAT_LEN_LOGNORMAL, GAT_LEN_LOGUNIFORM = 0, 1, 2
+GAT_SIDE_FIXED, GAT_SIDE_LOGUNIFORM = 0, 1
+GAT_EDR_MAX_LEN = 16384
+
+# (name, restype, argtypes) for every symbol of include/gat_b200.h
+SIGNATURES = [
+    ("gat_ctx_create", c_int, [c_int, C.POINTER(c_p)]),
+    ("gat_ctx_destroy", None, [c_p]),
+    ("gat_last_error", C.c_char_p, [c_p]),
+    ("gat_ctx_stream", c_p, [c_p]),
+    ("gat_ctx_sync", c_int, [c_p]),
+    ("gat_ctx_launches", c_i64, [c_p]),
+    ("gat_ctx_scratch_bytes", c_i64, [c_p]),
+    ("gat_db_create", c_int, [c_p, c_int, P_i32, P_f32, P_f32, C.POINTER(c_p)]),
+    ("gat_db_destroy", None, [c_p]),
+    ("gat_db_info", c_int, [c_p, P_i64]),
+    ("gat_grid_build", c_int, [c_p, c_p, MBB, c_f, c_int, c_int, C.POINTER(c_p)]),
+    ("gat_stig_build", c_int, [c_p, c_p, c_int, C.POINTER(c_p)]),
+    ("gat_fsg_build", c_int, [c_p, c_p, MBB, c_f, C.POINTER(c_p)]),
+    ("gat_index_destroy", None, [c_p]),
+    ("gat_index_info", c_int, [c_p, P_i64]),
+    ("gat_index_points", c_int, [c_p, c_p, c_i64, P_f32, P_f32, P_i32, P_i32]),
+    ("gat_range_query", c_int, [c_p, c_p, c_p, c_int, c_int, c_int, P_i64, P_i32, P_i32, c_i64, P_i64]),
+    ("gat_range_query_dev", c_int, [c_p, c_p, c_p, c_int, c_int, c_int, c_p, c_p, c_p, c_i64, P_i64]),
+    ("gat_edr_pairs", c_int, [c_p, c_int, P_i32, P_i64, P_f32, c_i64, P_i32, P_i64, P_f32, c_i64, c_d, P_i32]),
+    ("gat_edr_pairs_dev", c_int, [c_p, c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_d, c_p]),
+    ("gat_fv_lower_bounds", c_int, [c_p, c_p, c_int, P_i32, P_f32, P_f32, P_i32]),
+    ("gat_topk", c_int, [c_p, c_p, c_int, P_i32, P_f32, P_f32, c_int, c_d, c_int, P_i32, P_i32, P_i64]),
+    ("gat_topk_dev", c_int, [c_p, c_p, c_int, c_p, c_p, c_p, c_int, c_int, c_d, c_int, c_p, c_p, P_i64]),
+    ("gat_gen_lengths", c_int, [c_int, c_int, c_d, c_d, c_int, c_int, c_u64, P_i32]),
+    ("gat_gen_walks", c_int, [c_int, P_i32, P_f32, c_d, c_u64, P_f32, P_f32]),
+    ("gat_gen_boxes", c_int, [c_int, c_int, c_d, c_d, P_f32, c_u64, P_f32]),
+    ("gat_gen_sample_ids", c_int, [c_int, c_int, c_u64, P_i32]),
+    ("gat_gen_pairs", c_int, [c_int, P_i32, P_i32, P_f32, c_d, c_d, c_u64, P_f32, P_f32]),
+]
+
+for _name, _res, _args in SIGNATURES:
+    _fn = getattr(lib, _name)  # raises AttributeError when the library lacks a declared symbol
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+EXPORTED = [s[0] for s in SIGNATURES]

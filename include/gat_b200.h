@@ -1,0 +1,172 @@
+/* gat_b200: trajectory range and EDR top-k queries on one NVIDIA B200 (sm_100a).
+ *
+ * C ABI of the library gat_b200/libgat_b200.so. Every entry point returns a gat_status; on
+ * failure gat_last_error(ctx) holds a message. Nothing aborts the process.
+ *
+ * Handles are opaque and owned by the library: a gat_db holds a trajectory set resident in
+ * device memory, a gat_index holds one of the reference's three range indexes (GT-quadtree
+ * "Grid" with its FVTable, STIG, FSG) built on the host in the reference's exact layout and
+ * resident in device memory. Host output buffers are owned by the caller; calls whose output
+ * size is data-dependent take a capacity and report the size needed (GAT_ERR_TRUNCATED when
+ * it did not fit, with nothing written beyond the capacity).
+ *
+ * Trajectory ids are 1..n, as in the reference (tradb[1..], main.cpp:116-121): lengths[i] and
+ * the concatenated lon/lat arrays describe trajectory i+1. Coordinates are float32.
+ *
+ * Reference interfaces replaced (file:line in the reference):
+ *   cudaRangeQueryTestHandler        cudaKernel.h:21  -> gat_range_query (GAT_INDEX_GRID, FSG)
+ *   cudaRangeQuerySTIGHandler        cudaKernel.h:28  -> gat_range_query (GAT_INDEX_STIG)
+ *   EDRDistance_Batch_Handler        cudaKernel.h:24  -> gat_edr_pairs
+ *   Similarity_Pruning_Handler       cudaKernel.h:26  -> gat_fv_lower_bounds
+ *   Grid::SimilarityQueryBatchOnGPU  Grid.h:65        -> gat_topk
+ *   Grid::Grid + addDatasetToGrid    Grid.h:39,42     -> gat_grid_build
+ *   STIG::initial                    STIG.h:57        -> gat_stig_build
+ *   FSG::FSG + addDatasetToGrid      FSG.h:35,38      -> gat_fsg_build
+ */
+#ifndef GAT_B200_H
+#define GAT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GAT_OK = 0,
+    GAT_ERR_ARG = 1,       /* invalid argument (size, pointer, out-of-grid point, ...) */
+    GAT_ERR_OOM = 2,       /* device or host allocation failed */
+    GAT_ERR_CUDA = 3,      /* CUDA runtime error */
+    GAT_ERR_TRUNCATED = 4, /* output larger than the capacity given; *needed holds the size */
+    GAT_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+    GAT_ERR_STATE = 6      /* handle used with the wrong context or kind */
+} gat_status;
+
+typedef struct gat_ctx gat_ctx;
+typedef struct gat_db gat_db;
+typedef struct gat_index gat_index;
+
+/* MBB.h:5 field order */
+typedef struct {
+    float xmin, ymin, xmax, ymax;
+} gat_mbb;
+
+enum { GAT_INDEX_GRID = 0, GAT_INDEX_STIG = 1, GAT_INDEX_FSG = 2 };
+/* GAT_RESULT_IDS: per query, the sorted set of trajectory ids with at least one point in the
+ * box (the reference's vector<bool> result row, QueryResult.h:4).
+ * GAT_RESULT_POINTS: per query, the sorted (trajectory id, point index) pairs in the box. */
+enum { GAT_RESULT_IDS = 0, GAT_RESULT_POINTS = 1 };
+/* GAT_EXEC_PLAIN: one query per launch sequence. GAT_EXEC_BATCHED: all queries in one. */
+enum { GAT_EXEC_PLAIN = 0, GAT_EXEC_BATCHED = 1 };
+
+/* ---------------------------------------------------------------- context */
+/* Creates a context bound to a CUDA device with its own stream. */
+int gat_ctx_create(int device, gat_ctx** out);
+void gat_ctx_destroy(gat_ctx* ctx);
+const char* gat_last_error(const gat_ctx* ctx);
+/* The cudaStream_t all work of the context is issued on (for event timing by callers). */
+void* gat_ctx_stream(gat_ctx* ctx);
+int gat_ctx_sync(gat_ctx* ctx);
+/* Kernel launches issued by the context since creation (all of them are this library's). */
+int64_t gat_ctx_launches(const gat_ctx* ctx);
+/* Device bytes currently held by the context's scratch arena. */
+int64_t gat_ctx_scratch_bytes(const gat_ctx* ctx);
+
+/* ---------------------------------------------------------------- trajectory set */
+int gat_db_create(gat_ctx* ctx, int n, const int32_t* lengths, const float* lon, const float* lat,
+                  gat_db** out);
+void gat_db_destroy(gat_db* db);
+/* info[0] = n, info[1] = total points, info[2] = longest trajectory */
+int gat_db_info(const gat_db* db, int64_t info[4]);
+
+/* ---------------------------------------------------------------- indexes */
+/* Grid::Grid(range, cell_size, virtual_cell_param) + addDatasetToGrid (Grid.cpp:97-316):
+ * Morton cells, cell-contiguous points, quadtree with leaves below leaf_cap points
+ * (MAXPOINTINNODE, ConstDefine.h:32), and the FVTable over virtual cells cell >> param. */
+int gat_grid_build(gat_ctx* ctx, const gat_db* db, gat_mbb range, float cell_size,
+                   int virtual_cell_param, int leaf_cap, gat_index** out);
+/* STIG::initial(block_size, 2, ...) (STIG.cpp:35-168) */
+int gat_stig_build(gat_ctx* ctx, const gat_db* db, int block_size, gat_index** out);
+/* FSG::FSG(range, cell_size) + addDatasetToGrid (FSG.cpp:7-143) */
+int gat_fsg_build(gat_ctx* ctx, const gat_db* db, gat_mbb range, float cell_size, gat_index** out);
+void gat_index_destroy(gat_index* index);
+/* info[0] = kind, [1] = points, [2] = leaves / blocks / cells, [3] = nodes, [4] = axis or
+ * cells along x, [5] = cells along y, [6] = device bytes */
+int gat_index_info(const gat_index* index, int64_t info[8]);
+/* Copies the index's point order back: x, y, trajectory id, point index within trajectory
+ * (any pointer may be NULL). n must equal info[1]. */
+int gat_index_points(gat_ctx* ctx, const gat_index* index, int64_t n, float* x, float* y,
+                     int32_t* tid, int32_t* pidx);
+
+/* ---------------------------------------------------------------- range query */
+/* Per query, the result set in the reference's inclusive MBB::pInBox semantics (MBB.cpp:21)
+ * over the index's candidate leaves / blocks / cells. offsets has nq + 1 entries (CSR);
+ * out_tid receives trajectory ids, out_pidx point indices (GAT_RESULT_POINTS only; may be
+ * NULL for GAT_RESULT_IDS). capacity counts entries of out_tid. */
+int gat_range_query(gat_ctx* ctx, const gat_index* index, const gat_mbb* queries, int nq,
+                    int result_kind, int exec, int64_t* offsets, int32_t* out_tid,
+                    int32_t* out_pidx, int64_t capacity, int64_t* needed);
+/* Same with every array in device memory (queries, offsets, out_tid, out_pidx); needed is a
+ * host pointer. Work is enqueued on the context stream; the call returns after the result
+ * size is known. */
+int gat_range_query_dev(gat_ctx* ctx, const gat_index* index, const gat_mbb* d_queries, int nq,
+                        int result_kind, int exec, int64_t* d_offsets, int32_t* d_tid,
+                        int32_t* d_pidx, int64_t capacity, int64_t* needed);
+
+/* ---------------------------------------------------------------- EDR */
+/* EDR of (query, candidate) pairs with the reference's recurrence (Grid.cpp:1274-1306) and
+ * match test |dx| < eps && |dy| < eps evaluated as float differences compared in double.
+ * Points are interleaved (x, y); pair i uses q_xy[2*q_off[i] ...] for q_len[i] points and
+ * c_xy[2*c_off[i] ...] for c_len[i] points. Lengths must be 1..GAT_EDR_MAX_LEN. */
+#define GAT_EDR_MAX_LEN 16384
+int gat_edr_pairs(gat_ctx* ctx, int npairs, const int32_t* q_len, const int64_t* q_off,
+                  const float* q_xy, int64_t q_points, const int32_t* c_len,
+                  const int64_t* c_off, const float* c_xy, int64_t c_points, double eps,
+                  int32_t* out);
+/* Same, device arrays. */
+int gat_edr_pairs_dev(gat_ctx* ctx, int npairs, const int32_t* d_q_len, const int64_t* d_q_off,
+                      const float* d_q_xy, const int32_t* d_c_len, const int64_t* d_c_off,
+                      const float* d_c_xy, double eps, int32_t* d_out);
+
+/* ---------------------------------------------------------------- top-k similarity */
+/* FVTable::formPriorityQueue lower bounds (FVTable.cpp:77-207) of every trajectory of the
+ * grid's set against each query: out[q * (n + 1) + t], t = 0..n (t = 0 unused). */
+int gat_fv_lower_bounds(gat_ctx* ctx, const gat_index* grid, int nq, const int32_t* q_len,
+                        const float* q_lon, const float* q_lat, int32_t* out);
+/* The k trajectories of the grid's set with the smallest EDR to each query, sorted by
+ * (distance, trajectory id). Candidates are evaluated in frequency-vector lower-bound order
+ * and pruned once the bound exceeds the current k-th distance (Grid.cpp:852-1019), so the
+ * result equals the exhaustive one. stats (may be NULL): [0] EDR pairs evaluated, [1] DP
+ * cells evaluated, [2] launches issued. */
+int gat_topk(gat_ctx* ctx, const gat_index* grid, int nq, const int32_t* q_len,
+             const float* q_lon, const float* q_lat, int k, double eps, int exec,
+             int32_t* out_ids, int32_t* out_dist, int64_t* stats);
+/* Same with query points and outputs in device memory: d_q_off[nq+1] point offsets. */
+int gat_topk_dev(gat_ctx* ctx, const gat_index* grid, int nq, const int32_t* d_q_len,
+                 const int64_t* d_q_off, const float* d_q_xy, int max_q_len, int k, double eps,
+                 int exec, int32_t* d_ids, int32_t* d_dist, int64_t* stats);
+
+/* ---------------------------------------------------------------- synthetic inputs */
+enum { GAT_LEN_UNIFORM = 0, GAT_LEN_LOGNORMAL = 1, GAT_LEN_LOGUNIFORM = 2 };
+enum { GAT_SIDE_FIXED = 0, GAT_SIDE_LOGUNIFORM = 1 };
+/* n lengths: uniform integers in [lo, hi]; round(exp(N(p0, p1))) clipped to [lo, hi]; or
+ * round(log-uniform(lo, hi)). */
+int gat_gen_lengths(int n, int kind, double p0, double p1, int lo, int hi, uint64_t seed,
+                    int32_t* out);
+/* Clamped random walks in box: start uniform, N(0, step) increments per axis. */
+int gat_gen_walks(int n, const int32_t* lengths, const float box[4], double step, uint64_t seed,
+                  float* lon, float* lat);
+/* Query rectangles with centres uniform in box; side s0 (GAT_SIDE_FIXED) or log-uniform in
+ * [s0, s1] per axis. out4 = (xmin, ymin, xmax, ymax) per rectangle. */
+int gat_gen_boxes(int n, int kind, double s0, double s1, const float box[4], uint64_t seed,
+                  float* out4);
+/* k distinct ids from 1..n */
+int gat_gen_sample_ids(int k, int n, uint64_t seed, int32_t* out);
+/* EDR pairs: A a random walk, B A's path resampled to B's length plus N(0, jitter) noise. */
+int gat_gen_pairs(int n, const int32_t* len_a, const int32_t* len_b, const float box[4],
+                  double step, double jitter, uint64_t seed, float* a_xy, float* b_xy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GAT_B200_H */
