@@ -5,7 +5,8 @@ Host C++ is compiled by g++ through nvcc; CUDA sources are compiled for sm_100a 
 so that it travels with the source tree. Incremental: an object is rebuilt when its source or
 any header under csrc/ or include/ is newer.
 
-Usage: python -m gat_b200.build [--force] [--no-oracle] [-j N]
+Usage: python gat_b200/build.py [--force] [--no-oracle] [-j N]   (run by path: importing the
+package would load the library being built)
 """
 from __future__ import annotations
 
@@ -26,7 +27,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-I", INCLUDE, "-I", CSRC, "-Xcompiler", "-fPIC"]
 # float expressions on the host must round exactly like the reference's (no contraction)
-HOST_FLAGS = ["-Xcompiler", "-ffp-contract=off,-pthread,-Wall,-Wno-unused-function"]
+HOST_FLAGS = ARCH + ["-Xcompiler", "-ffp-contract=off,-pthread,-Wall,-Wno-unused-function"]
 # no fast-math: the EDR match test and cell assignment need IEEE float subtraction/division
 CUDA_FLAGS = ARCH + ["-lineinfo", "--fmad=false", "-Xptxas", "-warn-spills"]
 

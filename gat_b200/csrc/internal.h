@@ -1,0 +1,216 @@
+/* Internal types of libgat_b200: context, device-resident trajectory set and indexes.
+ *
+ * Device layout (all arrays in HBM, owned by the handle):
+ *   trajectory set : xy[P] float2 in trajectory order (trajectory t at off[t] .. off[t+1]),
+ *                    len[n+1] (len[0] = 0), off[n+2]
+ *   index points   : x[P], y[P] float SoA in the index's point order (Morton-cell order for
+ *                    the Grid, the STIG leaf order, row-major cell order for FSG), key[P] =
+ *                    (tid << pidx_bits) | point index within trajectory, tid[P]
+ *   Grid tree      : breadth-first node arrays, children of node i at child[i] .. child[i]+3,
+ *                    child = -1 for leaves, leaf point range [pbeg, pend)
+ *   STIG tree      : node arrays (leaf flag, split dim, median, children, leaf range + MBB)
+ *   FSG            : per-cell point range, cells along x/y
+ *   FVTable        : CSR over trajectory ids: fv_off[n+2], (vcell, count) entries sorted by vcell
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gat_b200.h"
+
+namespace gat {
+
+/* ---------------------------------------------------------------- device structs */
+struct GridDev {
+    float rxmin, rymin, rxmax, rymax; /* grid range (the Grid's MBB) */
+    float cell;
+    int axis, cellnum, total_level, vparam;
+    int nnodes;
+    const float4* node_mbb;
+    const int32_t* node_child;
+    const int32_t* node_pbeg;
+    const int32_t* node_pend;
+};
+
+struct StigDev {
+    int nnodes;
+    const int32_t* kind;   /* 1 leaf, 0 internal */
+    const int32_t* dim;    /* depth % 2 */
+    const float* median;
+    const int32_t* left;
+    const int32_t* right;
+    const int32_t* lo;     /* leaf: inclusive range */
+    const int32_t* hi;
+    const float4* mbb;     /* leaf MBB */
+};
+
+struct FsgDev {
+    float rxmin, rymin, rxmax, rymax;
+    float cell;
+    int nx, ny, cellnum;
+    const int32_t* cbeg; /* point range of cell c: [cbeg[c], cend[c]) */
+    const int32_t* cend;
+};
+
+/* One EDR problem: query side (a) and candidate side (b), offsets into two point arrays. */
+struct EdrPair {
+    int64_t a_off;
+    int64_t b_off;
+    int32_t a_len;
+    int32_t b_len;
+};
+
+}  // namespace gat
+
+/* ---------------------------------------------------------------- handles */
+struct gat_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::mutex mu;           /* serialises calls on one context */
+    int64_t launches = 0;
+    /* scratch arena: slot -> device buffer, grown on demand, freed with the context */
+    std::vector<void*> slot_ptr;
+    std::vector<size_t> slot_bytes;
+    int32_t* d_flag = nullptr; /* device status word written by kernels (0 = ok) */
+    /* optional per-kernel-class event timing (gat_ctx_set_timing) */
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[GAT_KERNEL_CLASSES];
+    std::vector<cudaEvent_t> ev_free;
+    double t_ms[GAT_KERNEL_CLASSES] = {0, 0, 0};
+    int64_t t_launches[GAT_KERNEL_CLASSES] = {0, 0, 0};
+    double t_work[GAT_KERNEL_CLASSES] = {0, 0, 0};
+    int64_t* h_pinned = nullptr; /* pinned host words for small D2H reads */
+};
+
+struct gat_db {
+    gat_ctx* ctx = nullptr;
+    int n = 0;
+    int64_t npoints = 0;
+    int maxlen = 0;
+    std::vector<int32_t> h_len;  /* [n+1], h_len[0] = 0 */
+    std::vector<int64_t> h_off;  /* [n+2] */
+    std::vector<float> h_x, h_y; /* trajectory order */
+    int32_t* d_len = nullptr;
+    int64_t* d_off = nullptr;
+    float2* d_xy = nullptr;
+};
+
+struct gat_index {
+    gat_ctx* ctx = nullptr;
+    const gat_db* db = nullptr;
+    int kind = 0;
+    int64_t npoints = 0;
+    int pidx_bits = 0;
+    size_t device_bytes = 0;
+    std::vector<void*> allocs;
+    /* points in index order */
+    float* d_x = nullptr;
+    float* d_y = nullptr;
+    uint32_t* d_key = nullptr;
+    int32_t* d_tid = nullptr;
+    /* host copies kept for gat_index_points and the tree walks of the builders */
+    std::vector<int32_t> h_tid, h_pidx;
+    std::vector<float> h_x, h_y;
+    int64_t leaves = 0, nodes = 0;
+    gat::GridDev grid{};
+    gat::StigDev stig{};
+    gat::FsgDev fsg{};
+    /* Grid FVTable (CSR over tids 0..n) */
+    int64_t* d_fv_off = nullptr;
+    int32_t* d_fv_cell = nullptr;
+    int32_t* d_fv_cnt = nullptr;
+    int fv_max_nnz = 0;
+    int64_t fv_entries = 0;
+};
+
+/* ---------------------------------------------------------------- helpers (context.cpp) */
+namespace gat {
+
+int fail(gat_ctx* ctx, int code, const std::string& msg);
+int cuda_fail(gat_ctx* ctx, cudaError_t e, const char* what);
+/* device scratch slot of at least `bytes` bytes; contents undefined */
+void* scratch(gat_ctx* ctx, int slot, size_t bytes, int* status);
+/* cudaMalloc tracked by an index (freed by gat_index_destroy) */
+void* index_alloc(gat_index* ix, size_t bytes, int* status);
+template <class T>
+T* index_upload(gat_index* ix, const std::vector<T>& v, int* status) {
+    T* p = (T*)index_alloc(ix, v.size() * sizeof(T) + sizeof(T), status);
+    if (!p) return nullptr;
+    if (!v.empty()) {
+        cudaError_t e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            *status = cuda_fail(ix->ctx, e, "upload");
+            return nullptr;
+        }
+    }
+    return p;
+}
+/* reads and clears the device status word; returns GAT_OK or the code a kernel stored */
+int check_device_flag(gat_ctx* ctx, const char* what);
+inline void count_launch(gat_ctx* ctx, int n = 1) { ctx->launches += n; }
+/* brackets one launch of a timed kernel class (no-ops unless timing is on) */
+void timed_begin(gat_ctx* ctx, int cls);
+void timed_end(gat_ctx* ctx, int cls, double work);
+/* device-side work counter for classes whose work is only known on the device (EDR cells) */
+void timed_add_work(gat_ctx* ctx, int cls, double work);
+
+/* GAT_ERR_STATE for a host-only context (device -1) */
+int require_device(gat_ctx* ctx, const char* what);
+
+/* smallest float >= eps (the reference compares |float diff| < (double)EPSILON) */
+float match_threshold(double eps);
+
+/* scratch slot ids */
+enum Slot {
+    S_SCAN_TMP = 0,
+    S_RANGE_Q,
+    S_RANGE_ICNT,
+    S_RANGE_IOFF,
+    S_RANGE_ITEMS,
+    S_RANGE_SEGBASE,
+    S_RANGE_SEGCNT,
+    S_RANGE_ARENA,
+    S_RANGE_ARENA2,
+    S_RANGE_OFF,
+    S_RANGE_OUT_T,
+    S_RANGE_OUT_P,
+    S_RANGE_CURSOR,
+    S_RANGE_CSR,
+    S_EDR_PAIRS,
+    S_EDR_CARRY,
+    S_EDR_COUNTERS,
+    S_EDR_IO,
+    S_TOPK_QFV,
+    S_TOPK_LB,
+    S_TOPK_PAIRS,
+    S_TOPK_DIST,
+    S_TOPK_QSTATE,
+    S_TOPK_SEG,
+    S_TOPK_IO,
+    S_TOPK_OUT,
+    S_COUNT
+};
+
+/* ---------------------------------------------------------------- launchers (.cu) */
+/* exclusive scan of n int64 counts into out[0..n] (out[n] = total); in may alias out */
+int scan_i64(gat_ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
+/* EDR of pairs (a_off, a_len, b_off, b_len) over point arrays A and B; the count is read
+ * from d_npairs when non-NULL, else npairs (edr.cu) */
+int edr_launch_soa(gat_ctx* ctx, int npairs, const int* d_npairs, const int64_t* a_off, const int32_t* a_len,
+                   const int64_t* b_off, const int32_t* b_len, int rows_hint, int max_cols, const float2* A,
+                   const float2* B, float u, int32_t* d_out, unsigned long long* d_cells);
+
+}  // namespace gat
+
+#define GAT_CUDA_TRY(ctx, expr, what)                    \
+    do {                                                 \
+        cudaError_t e__ = (expr);                        \
+        if (e__ != cudaSuccess) return gat::cuda_fail((ctx), e__, (what)); \
+    } while (0)

@@ -1,0 +1,632 @@
+/* Range queries over the Grid (GT-quadtree), STIG and FSG indexes.
+ *
+ * Pipeline for a batch of queries (all launches on the context stream):
+ *   1. candidates  one thread per query walks the index (Grid: quadtree with BoxIntersect,
+ *                  Grid.cpp:428-446; STIG: median slabs + leaf MBBs, STIG.cpp:179-252; FSG:
+ *                  the rows of the candidate cell rectangle, FSG.cpp:183-262) and emits point
+ *                  ranges; a count pass and a scan give each query its item slice.
+ *   2. scan        one CTA per query tests every candidate point with the inclusive
+ *                  MBB::pInBox (MBB.cpp:21-26) on SoA float32 x/y read with 128-bit loads,
+ *                  and either sets trajectory bits in a shared-memory bitmap (id sets: the
+ *                  reference's per-query vector<bool>, Grid.cpp:384-387) or compacts hit keys
+ *                  with warp ballots and prefix sums (point lists), which it then sorts with a
+ *                  stable in-CTA radix sort and de-duplicates.
+ *   3. offsets     scan of per-query result counts; one CTA per query copies its segment.
+ * Plain execution runs the same pipeline once per query.
+ */
+#include <algorithm>
+
+#include "internal.h"
+
+namespace gat {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kStack = 96;
+
+struct Box {
+    float xmin, ymin, xmax, ymax;
+};
+
+__device__ __forceinline__ bool in_box(const Box& q, float x, float y) {
+    /* MBB::pInBox (MBB.cpp:21-26) */
+    return x <= q.xmax && x >= q.xmin && y <= q.ymax && y >= q.ymin;
+}
+
+/* BoxIntersect (MBB.cpp:28-73) reduced to its zero / non-zero outcome, the only use the
+ * traversals make of it. */
+__device__ __forceinline__ bool box_intersect(const Box& a1, const Box& b1) {
+    Box a, b;
+    if (a1.xmin < b1.xmin) {
+        a = a1;
+        b = b1;
+    } else if (a1.xmin == b1.xmin) {
+        if (a1.xmax > b1.xmax) {
+            a = a1;
+            b = b1;
+        } else {
+            b = a1;
+            a = b1;
+        }
+    } else {
+        b = a1;
+        a = b1;
+    }
+    if (b.xmin >= a.xmax) return false;
+    if (b.ymax <= a.ymin) return false;
+    if (b.ymin >= a.ymax) return false;
+    return true;
+}
+
+__device__ __forceinline__ Box load_box(const gat_mbb* q, int i) {
+    gat_mbb m = q[i];
+    return Box{m.xmin, m.ymin, m.xmax, m.ymax};
+}
+
+__device__ __forceinline__ void set_flag(int32_t* flag, int code) { atomicCAS(flag, 0, code); }
+
+/* ---------------------------------------------------------------- candidates */
+/* emit(pbeg, pend) for each candidate leaf; returns false on stack overflow */
+template <class Emit>
+__device__ bool grid_walk(const GridDev& g, const Box& q, Emit emit) {
+    int stack[kStack];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        int nd = stack[--sp];
+        int ch = g.node_child[nd];
+        if (ch < 0) {
+            /* leaves are taken without a test (Grid.cpp:430-433) */
+            emit(g.node_pbeg[nd], g.node_pend[nd]);
+            continue;
+        }
+        /* push in reverse so children are visited UL, UR, DL, DR (Grid.cpp:436-443) */
+        for (int c = 3; c >= 0; c--) {
+            float4 m = g.node_mbb[ch + c];
+            if (box_intersect(q, Box{m.x, m.y, m.z, m.w})) {
+                if (sp >= kStack) return false;
+                stack[sp++] = ch + c;
+            }
+        }
+    }
+    return true;
+}
+
+template <class Emit>
+__device__ bool stig_walk(const StigDev& s, const Box& q, Emit emit) {
+    int stack[kStack];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        int nd = stack[--sp];
+        if (s.kind[nd]) {
+            /* STIG::searchNode(LeafNode*) (STIG.cpp:241-252): leaf MBB against the query */
+            float4 m = s.mbb[nd];
+            if (box_intersect(Box{m.x, m.y, m.z, m.w}, q)) emit(s.lo[nd], s.hi[nd] + 1);
+            continue;
+        }
+        /* STIG::searchNode(InternalNode*) (STIG.cpp:201-239) with intersectBlock (:340-347) */
+        float lo = s.dim[nd] == 0 ? q.xmin : q.ymin;
+        float hi = s.dim[nd] == 0 ? q.xmax : q.ymax;
+        float med = s.median[nd];
+        bool go_left = !(hi < 0.0f) && !(lo > med);
+        bool go_right = !(hi < med) && !(lo > 180.0f);
+        if (sp + 2 > kStack) return false;
+        if (go_right) stack[sp++] = s.right[nd];
+        if (go_left) stack[sp++] = s.left[nd];
+    }
+    return true;
+}
+
+template <class Emit>
+__device__ void fsg_walk(const FsgDev& f, const Box& q, Emit emit) {
+    /* FSG::rangeQueryBatchGPU (FSG.cpp:183-262): the border ring plus the interior cover the
+     * cells (row, col) for rows g3..g4 and cols g1..g2, addressed row * nx + col without
+     * clamping. Row r is one contiguous run of cell ids; ids outside the grid are skipped (the
+     * reference reads out of bounds there and no point lies in such a cell). */
+    int g1 = (int)__fdiv_rn(__fsub_rn(q.xmin, f.rxmin), f.cell);
+    int g2 = (int)__fdiv_rn(__fsub_rn(q.xmax, f.rxmin), f.cell);
+    int g3 = (int)__fdiv_rn(__fsub_rn(f.rymax, q.ymax), f.cell);
+    int g4 = (int)__fdiv_rn(__fsub_rn(f.rymax, q.ymin), f.cell);
+    for (int r = g3; r <= g4; r++) {
+        long long lo = (long long)g1 + (long long)r * f.nx;
+        long long hi = (long long)g2 + (long long)r * f.nx;
+        if (lo < 0) lo = 0;
+        if (hi > f.cellnum - 1) hi = f.cellnum - 1;
+        if (lo > hi) continue;
+        int b = f.cbeg[lo], e = f.cend[hi];
+        if (b < e) emit(b, e);
+    }
+}
+
+template <int KIND>
+__global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, int nq, const int64_t* ioff,
+                        int64_t* icnt, int2* items, int32_t* flag) {
+    int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= nq) return;
+    Box q = load_box(queries, qi);
+    int64_t cnt = 0;
+    int64_t w = ioff ? ioff[qi] : 0;
+    auto emit = [&](int b, int e) {
+        if (b >= e) return;
+        if (ioff) items[w + cnt] = make_int2(b, e);
+        cnt++;
+    };
+    bool ok = true;
+    if (KIND == GAT_INDEX_GRID) ok = grid_walk(g, q, emit);
+    if (KIND == GAT_INDEX_STIG) ok = stig_walk(s, q, emit);
+    if (KIND == GAT_INDEX_FSG) fsg_walk(f, q, emit);
+    if (!ok) set_flag(flag, GAT_ERR_ARG);
+    if (!ioff) icnt[qi] = cnt;
+}
+
+/* ---------------------------------------------------------------- block helpers */
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+/* exclusive block scan of one int per thread; kThreads threads */
+__device__ int block_scan_excl(int v, int* total, int* sh /* kThreads/32 + 1 */) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int w = 0; w < kThreads / 32; w++) {
+            int t = sh[w];
+            sh[w] = run;
+            run += t;
+        }
+        sh[kThreads / 32] = run;
+    }
+    __syncthreads();
+    int r = sh[warp] + x - v;
+    *total = sh[kThreads / 32];
+    __syncthreads();
+    return r;
+}
+
+/* Tests the points [b, e) against q, calling hit(i) for every point inside. The aligned body
+ * is read as float4 pairs (four x and four y per thread per step). */
+template <class Hit>
+__device__ __forceinline__ void scan_range(const float* __restrict__ X, const float* __restrict__ Y, int b, int e,
+                                           const Box& q, Hit hit) {
+    int head_end = min(e, (b + 3) & ~3);
+    for (int i = b + (int)threadIdx.x; i < head_end; i += blockDim.x)
+        if (in_box(q, __ldg(X + i), __ldg(Y + i))) hit(i);
+    int vb = head_end, ve = head_end + ((e - head_end) & ~3);
+    const float4* X4 = reinterpret_cast<const float4*>(X + vb);
+    const float4* Y4 = reinterpret_cast<const float4*>(Y + vb);
+    int nv = (ve - vb) >> 2;
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+        float4 x = __ldg(X4 + k), y = __ldg(Y4 + k);
+        int i = vb + 4 * k;
+        if (in_box(q, x.x, y.x)) hit(i);
+        if (in_box(q, x.y, y.y)) hit(i + 1);
+        if (in_box(q, x.z, y.z)) hit(i + 2);
+        if (in_box(q, x.w, y.w)) hit(i + 3);
+    }
+    for (int i = ve + (int)threadIdx.x; i < e; i += blockDim.x)
+        if (in_box(q, __ldg(X + i), __ldg(Y + i))) hit(i);
+}
+
+/* ---------------------------------------------------------------- id sets */
+/* One CTA per query (grid-stride over queries): a bitmap of n+1 trajectory bits in shared
+ * memory (or in a per-CTA global slice when it does not fit), set by every candidate hit,
+ * then emitted in ascending id order into the arena. */
+__global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, int nq, const int64_t* ioff,
+                                                        const int2* items, const float* X, const float* Y,
+                                                        const int32_t* tid, int words, uint32_t* gbitmap,
+                                                        uint32_t* arena, int64_t cap, unsigned long long* cursor,
+                                                        int64_t* segbase, int64_t* segcnt) {
+    extern __shared__ uint32_t smem_bm[];
+    __shared__ int sh[kThreads / 32 + 1];
+    __shared__ unsigned long long base_sh;
+    uint32_t* bm = gbitmap ? gbitmap + (size_t)blockIdx.x * words : smem_bm;
+    int per = (words + kThreads - 1) / kThreads;
+    for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+        for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
+        __syncthreads();
+        Box q = load_box(queries, qi);
+        for (int64_t it = ioff[qi]; it < ioff[qi + 1]; it++) {
+            int2 r = items[it];
+            scan_range(X, Y, r.x, r.y, q, [&](int i) {
+                int t = __ldg(tid + i);
+                atomicOr(&bm[t >> 5], 1u << (t & 31));
+            });
+        }
+        __syncthreads();
+        int w0 = threadIdx.x * per, w1 = min(words, w0 + per);
+        int c = 0;
+        for (int w = w0; w < w1; w++) c += __popc(bm[w]);
+        int total;
+        int pre = block_scan_excl(c, &total, sh);
+        if (threadIdx.x == 0) {
+            base_sh = atomicAdd(cursor, (unsigned long long)total);
+            segcnt[qi] = total;
+            segbase[qi] = (int64_t)base_sh;
+        }
+        __syncthreads();
+        int64_t base = (int64_t)base_sh;
+        if (base + total <= cap) {
+            int64_t o = base + pre;
+            for (int w = w0; w < w1; w++) {
+                uint32_t v = bm[w];
+                while (v) {
+                    int b = __ffs(v) - 1;
+                    v &= v - 1;
+                    arena[o++] = (uint32_t)(w * 32 + b);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/* ---------------------------------------------------------------- point lists */
+/* One CTA per query: count hits, reserve 2*count arena entries, compact the hit keys
+ * ((tid << pidx_bits) | pidx) with ballots, sort them with a stable LSD radix sort over the
+ * key's significant bits, drop duplicates (a STIG point can sit in two leaves). */
+__global__ void __launch_bounds__(kThreads) k_range_points(const gat_mbb* queries, int nq, const int64_t* ioff,
+                                                           const int2* items, const float* X, const float* Y,
+                                                           const uint32_t* key, int key_bits, uint32_t* arena,
+                                                           int64_t cap, unsigned long long* cursor,
+                                                           int64_t* segbase, int64_t* segcnt) {
+    __shared__ int sh[kThreads / 32 + 1];
+    __shared__ int hist[256];
+    __shared__ int wcount[kThreads / 32][257];
+    __shared__ int running[256];
+    __shared__ unsigned long long base_sh;
+    __shared__ int wtot[kThreads / 32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+        Box q = load_box(queries, qi);
+        /* pass 1: count */
+        int c = 0;
+        for (int64_t it = ioff[qi]; it < ioff[qi + 1]; it++) {
+            int2 r = items[it];
+            scan_range(X, Y, r.x, r.y, q, [&](int) { c++; });
+        }
+        int total;
+        block_scan_excl(c, &total, sh);
+        if (threadIdx.x == 0) base_sh = atomicAdd(cursor, 2ull * (unsigned long long)total);
+        __syncthreads();
+        int64_t base = (int64_t)base_sh;
+        if (base + 2 * (int64_t)total > cap) {
+            if (threadIdx.x == 0) {
+                segcnt[qi] = total;
+                segbase[qi] = base;
+            }
+            __syncthreads();
+            continue;
+        }
+        uint32_t* A = arena + base;
+        uint32_t* B = A + total;
+        /* pass 2: compact keys in item order, tile by tile (kThreads points per tile) */
+        int written = 0;
+        for (int64_t it = ioff[qi]; it < ioff[qi + 1]; it++) {
+            int2 r = items[it];
+            for (int t0 = r.x; t0 < r.y; t0 += kThreads) {
+                int i = t0 + threadIdx.x;
+                bool h = i < r.y && in_box(q, __ldg(X + i), __ldg(Y + i));
+                unsigned bal = __ballot_sync(0xffffffffu, h);
+                if (lane == 0) wtot[warp] = __popc(bal);
+                __syncthreads();
+                int wb = 0, tt = 0;
+                for (int w = 0; w < kThreads / 32; w++) {
+                    if (w < warp) wb += wtot[w];
+                    tt += wtot[w];
+                }
+                if (h) A[written + wb + __popc(bal & lanemask_lt())] = __ldg(key + i);
+                written += tt;
+                __syncthreads();
+            }
+        }
+        /* stable LSD radix sort, 8 bits per pass */
+        int passes = (key_bits + 7) / 8;
+        uint32_t* src = A;
+        uint32_t* dst = B;
+        for (int p = 0; p < passes; p++) {
+            int shift = 8 * p;
+            for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d] = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < total; i += blockDim.x) atomicAdd(&hist[(src[i] >> shift) & 255], 1);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int run = 0;
+                for (int d = 0; d < 256; d++) {
+                    running[d] = run;
+                    run += hist[d];
+                }
+            }
+            for (int d = threadIdx.x; d < 257; d += blockDim.x)
+                for (int w = 0; w < kThreads / 32; w++) wcount[w][d] = 0;
+            __syncthreads();
+            for (int t0 = 0; t0 < total; t0 += kThreads) {
+                int i = t0 + threadIdx.x;
+                bool valid = i < total;
+                uint32_t k = valid ? src[i] : 0u;
+                int d = valid ? (int)((k >> shift) & 255) : 256;
+                unsigned peers = __match_any_sync(0xffffffffu, d);
+                int rank = __popc(peers & lanemask_lt());
+                if (rank == 0) wcount[warp][d] = __popc(peers);
+                __syncthreads();
+                for (int dd = threadIdx.x; dd < 256; dd += blockDim.x) {
+                    int run = running[dd];
+                    for (int w = 0; w < kThreads / 32; w++) {
+                        int t = wcount[w][dd];
+                        wcount[w][dd] = run;
+                        run += t;
+                    }
+                    running[dd] = run;
+                }
+                __syncthreads();
+                if (valid) dst[wcount[warp][d] + rank] = k;
+                __syncthreads();
+                for (int dd = threadIdx.x; dd < 257; dd += blockDim.x)
+                    for (int w = 0; w < kThreads / 32; w++) wcount[w][dd] = 0;
+                __syncthreads();
+            }
+            uint32_t* t = src;
+            src = dst;
+            dst = t;
+        }
+        /* unique: sorted keys in src, compacted into dst */
+        int uniq = 0;
+        for (int t0 = 0; t0 < total; t0 += kThreads) {
+            int i = t0 + threadIdx.x;
+            bool keep = i < total && (i == 0 || src[i] != src[i - 1]);
+            unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) wtot[warp] = __popc(bal);
+            __syncthreads();
+            int wb = 0, tt = 0;
+            for (int w = 0; w < kThreads / 32; w++) {
+                if (w < warp) wb += wtot[w];
+                tt += wtot[w];
+            }
+            if (keep) dst[uniq + wb + __popc(bal & lanemask_lt())] = src[i];
+            uniq += tt;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            segcnt[qi] = uniq;
+            segbase[qi] = base + (dst == A ? 0 : total);
+        }
+        __syncthreads();
+    }
+}
+
+/* ---------------------------------------------------------------- gather */
+__global__ void k_gather(int nq, const int64_t* segbase, const int64_t* segcnt, const int64_t* off,
+                         const uint32_t* arena, int mode, int pidx_bits, int32_t* out_tid, int32_t* out_pidx) {
+    for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+        int64_t b = segbase[qi], n = segcnt[qi], o = off[qi];
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            uint32_t k = arena[b + i];
+            if (mode == GAT_RESULT_IDS) {
+                out_tid[o + i] = (int32_t)k;
+            } else {
+                out_tid[o + i] = (int32_t)(k >> pidx_bits);
+                if (out_pidx) out_pidx[o + i] = (int32_t)(k & ((1u << pidx_bits) - 1u));
+            }
+        }
+    }
+}
+
+int key_bits_of(const gat_index* ix) {
+    int b = 1;
+    while (b < 32 && ((int64_t)ix->db->n << ix->pidx_bits) >= ((int64_t)1 << b)) b++;
+    return b;
+}
+
+/* Runs the pipeline for queries d_q[0..nq) and leaves per-query (segbase, segcnt) in scratch.
+ * Returns the total result count in *total. */
+int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int mode, int64_t* d_off_out,
+              int64_t* total) {
+    cudaStream_t s = ctx->stream;
+    int st = GAT_OK;
+    int64_t* icnt = (int64_t*)scratch(ctx, S_RANGE_ICNT, (nq + 1) * sizeof(int64_t), &st);
+    if (!icnt) return st;
+    int tb = 128, gb = (nq + tb - 1) / tb;
+    auto launch_items = [&](const int64_t* ioff, int64_t* cnt, int2* items) {
+        switch (ix->kind) {
+            case GAT_INDEX_GRID:
+                k_items<GAT_INDEX_GRID><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, d_q, nq, ioff, cnt, items, ctx->d_flag);
+                break;
+            case GAT_INDEX_STIG:
+                k_items<GAT_INDEX_STIG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, d_q, nq, ioff, cnt, items, ctx->d_flag);
+                break;
+            default:
+                k_items<GAT_INDEX_FSG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, d_q, nq, ioff, cnt, items, ctx->d_flag);
+        }
+        count_launch(ctx);
+    };
+    launch_items(nullptr, icnt, nullptr);
+    int64_t* ioff = (int64_t*)scratch(ctx, S_RANGE_IOFF, (nq + 1) * sizeof(int64_t), &st);
+    if (!ioff) return st;
+    if ((st = scan_i64(ctx, icnt, ioff, nq)) != GAT_OK) return st;
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, ioff + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
+    int64_t nitems = ctx->h_pinned[0];
+    int2* items = (int2*)scratch(ctx, S_RANGE_ITEMS, (nitems + 1) * sizeof(int2), &st);
+    if (!items) return st;
+    launch_items(ioff, nullptr, items);
+    if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
+
+    int64_t* segbase = (int64_t*)scratch(ctx, S_RANGE_SEGBASE, (nq + 1) * sizeof(int64_t), &st);
+    int64_t* segcnt = (int64_t*)scratch(ctx, S_RANGE_SEGCNT, (nq + 1) * sizeof(int64_t), &st);
+    unsigned long long* cursor = (unsigned long long*)scratch(ctx, S_RANGE_CURSOR, 64, &st);
+    if (!segbase || !segcnt || !cursor) return st;
+    int words = (ix->db->n + 1 + 31) / 32;
+    size_t smem_bm = (size_t)words * 4;
+    bool bm_in_smem = smem_bm <= 200 * 1024;
+    int blocks_per_sm = 0;
+    if (mode == GAT_RESULT_IDS) {
+        if (bm_in_smem && smem_bm > 48 * 1024)
+            cudaFuncSetAttribute(k_range_ids, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bm);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_range_ids, kThreads, bm_in_smem ? smem_bm : 0);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_range_points, kThreads, 0);
+    }
+    int grid = std::max(1, std::min(nq, std::max(1, blocks_per_sm) * ctx->sm_count));
+    uint32_t* gbm = nullptr;
+    if (mode == GAT_RESULT_IDS && !bm_in_smem) {
+        gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, (size_t)grid * words * 4, &st);
+        if (!gbm) return st;
+    }
+    int key_bits = key_bits_of(ix);
+    /* result arena: start from a size guess and grow once if the cursor overshoots */
+    int64_t cap = std::max<int64_t>(1 << 20, (int64_t)nq * 256);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        uint32_t* arena = (uint32_t*)scratch(ctx, S_RANGE_ARENA, (size_t)cap * 4, &st);
+        if (!arena) return st;
+        cap = (int64_t)(ctx->slot_bytes[S_RANGE_ARENA] / 4);
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s), "range");
+        timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
+        if (mode == GAT_RESULT_IDS)
+            k_range_ids<<<grid, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid,
+                                                                       words, gbm, arena, cap, cursor, segbase, segcnt);
+        else
+            k_range_points<<<grid, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits, arena,
+                                                     cap, cursor, segbase, segcnt);
+        timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
+        count_launch(ctx);
+        GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
+        int64_t used = ctx->h_pinned[0];
+        if (used <= cap) break;
+        if (attempt == 1) return fail(ctx, GAT_ERR_OOM, "range: result arena overflow");
+        cap = used;
+    }
+    if ((st = scan_i64(ctx, segcnt, d_off_out, nq)) != GAT_OK) return st;
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, d_off_out + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
+    *total = ctx->h_pinned[0];
+    return GAT_OK;
+}
+
+int run_gather(gat_ctx* ctx, const gat_index* ix, int nq, int mode, const int64_t* d_off, int32_t* d_tid,
+               int32_t* d_pidx) {
+    int st = GAT_OK;
+    int64_t* segbase = (int64_t*)scratch(ctx, S_RANGE_SEGBASE, (nq + 1) * sizeof(int64_t), &st);
+    int64_t* segcnt = (int64_t*)scratch(ctx, S_RANGE_SEGCNT, (nq + 1) * sizeof(int64_t), &st);
+    uint32_t* arena = (uint32_t*)ctx->slot_ptr[S_RANGE_ARENA];
+    int grid = std::max(1, std::min(nq, ctx->sm_count * 8));
+    k_gather<<<grid, kThreads, 0, ctx->stream>>>(nq, segbase, segcnt, d_off, arena, mode, ix->pidx_bits, d_tid, d_pidx);
+    count_launch(ctx);
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "range gather launch");
+    return GAT_OK;
+}
+
+
+/* Device-side entry shared by the host and device APIs. Offsets, tids and pidx go to device
+ * buffers with the given capacity; needed receives the total. */
+int range_dev(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int mode, int exec, int64_t* d_off,
+              int32_t* d_tid, int32_t* d_pidx, int64_t capacity, int64_t* needed) {
+    if (mode == GAT_RESULT_POINTS && ix->pidx_bits < 0)
+        return fail(ctx, GAT_ERR_ARG, "range: trajectory ids and point indices do not fit a 32-bit key");
+    if (nq == 0) {
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(d_off, 0, sizeof(int64_t), ctx->stream), "range");
+        *needed = 0;
+        return gat_ctx_sync(ctx);
+    }
+    int st;
+    if (exec == GAT_EXEC_BATCHED) {
+        int64_t total = 0;
+        if ((st = run_batch(ctx, ix, d_q, nq, mode, d_off, &total)) != GAT_OK) return st;
+        *needed = total;
+        if (total > capacity) return fail(ctx, GAT_ERR_TRUNCATED, "range: output capacity too small");
+        if ((st = run_gather(ctx, ix, nq, mode, d_off, d_tid, d_pidx)) != GAT_OK) return st;
+        return gat_ctx_sync(ctx);
+    }
+    /* plain: one query per pipeline run */
+    int64_t done = 0;
+    int64_t* off1 = (int64_t*)scratch(ctx, S_RANGE_OFF, 2 * sizeof(int64_t), &st);
+    if (!off1) return st;
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(d_off, 0, sizeof(int64_t), ctx->stream), "range");
+    bool truncated = false;
+    for (int qi = 0; qi < nq; qi++) {
+        int64_t total = 0;
+        if ((st = run_batch(ctx, ix, d_q + qi, 1, mode, off1, &total)) != GAT_OK) return st;
+        if (!truncated && done + total <= capacity) {
+            if ((st = run_gather(ctx, ix, 1, mode, off1, d_tid + done, d_pidx ? d_pidx + done : nullptr)) != GAT_OK)
+                return st;
+        } else {
+            truncated = true;
+        }
+        done += total;
+        ctx->h_pinned[1] = done;
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(d_off + qi + 1, ctx->h_pinned + 1, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream), "range");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "range");
+    }
+    *needed = done;
+    if (truncated) return fail(ctx, GAT_ERR_TRUNCATED, "range: output capacity too small");
+    return GAT_OK;
+}
+
+}  // namespace
+}  // namespace gat
+
+using namespace gat;
+
+extern "C" {
+
+int gat_range_query_dev(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_queries, int nq, int result_kind, int exec,
+                        int64_t* d_offsets, int32_t* d_tid, int32_t* d_pidx, int64_t capacity, int64_t* needed) {
+    if (!ctx || !ix || nq < 0 || (nq > 0 && (!d_queries || !d_tid)) || !d_offsets || !needed ||
+        (result_kind != GAT_RESULT_IDS && result_kind != GAT_RESULT_POINTS) ||
+        (exec != GAT_EXEC_PLAIN && exec != GAT_EXEC_BATCHED))
+        return fail(ctx, GAT_ERR_ARG, "gat_range_query_dev: bad arguments");
+    if (ix->ctx != ctx) return fail(ctx, GAT_ERR_STATE, "gat_range_query_dev: index from another context");
+    if (int rq = require_device(ctx, "gat_range_query_dev")) return rq;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return range_dev(ctx, ix, d_queries, nq, result_kind, exec, d_offsets, d_tid, d_pidx, capacity, needed);
+}
+
+int gat_range_query(gat_ctx* ctx, const gat_index* ix, const gat_mbb* queries, int nq, int result_kind, int exec,
+                    int64_t* offsets, int32_t* out_tid, int32_t* out_pidx, int64_t capacity, int64_t* needed) {
+    if (!ctx || !ix || nq < 0 || (nq > 0 && !queries) || !offsets || !needed || capacity < 0 ||
+        (capacity > 0 && !out_tid) || (result_kind == GAT_RESULT_POINTS && capacity > 0 && !out_pidx) ||
+        (result_kind != GAT_RESULT_IDS && result_kind != GAT_RESULT_POINTS) ||
+        (exec != GAT_EXEC_PLAIN && exec != GAT_EXEC_BATCHED))
+        return fail(ctx, GAT_ERR_ARG, "gat_range_query: bad arguments");
+    if (ix->ctx != ctx) return fail(ctx, GAT_ERR_STATE, "gat_range_query: index from another context");
+    if (int rq = require_device(ctx, "gat_range_query")) return rq;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    int st = GAT_OK;
+    gat_mbb* dq = (gat_mbb*)scratch(ctx, S_RANGE_Q, (size_t)(nq + 1) * sizeof(gat_mbb), &st);
+    if (!dq) return st;
+    if (nq > 0) GAT_CUDA_TRY(ctx, cudaMemcpyAsync(dq, queries, nq * sizeof(gat_mbb), cudaMemcpyHostToDevice, s), "range H2D");
+    /* outputs land in device scratch first, sized to the host capacity */
+    int64_t dcap = std::max<int64_t>(capacity, 1);
+    int32_t* dt = (int32_t*)scratch(ctx, S_RANGE_OUT_T, (size_t)dcap * 4, &st);
+    int32_t* dp = result_kind == GAT_RESULT_POINTS ? (int32_t*)scratch(ctx, S_RANGE_OUT_P, (size_t)dcap * 4, &st) : nullptr;
+    int64_t* csr = (int64_t*)scratch(ctx, S_RANGE_CSR, (size_t)(nq + 2) * sizeof(int64_t), &st);
+    if (!dt || !csr || (result_kind == GAT_RESULT_POINTS && !dp)) return st;
+    int64_t need = 0;
+    st = range_dev(ctx, ix, dq, nq, result_kind, exec, csr, dt, dp, capacity, &need);
+    *needed = need;
+    if (st == GAT_OK || st == GAT_ERR_TRUNCATED)
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(offsets, csr, (size_t)(nq + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range D2H");
+    if (st == GAT_OK && need > 0) {
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(out_tid, dt, (size_t)need * 4, cudaMemcpyDeviceToHost, s), "range D2H");
+        if (result_kind == GAT_RESULT_POINTS)
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(out_pidx, dp, (size_t)need * 4, cudaMemcpyDeviceToHost, s), "range D2H");
+    }
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
+    return st;
+}
+
+}  // extern "C"

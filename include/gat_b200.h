@@ -3,7 +3,8 @@
  * C ABI of the library gat_b200/libgat_b200.so. Every entry point returns a gat_status; on
  * failure gat_last_error(ctx) holds a message. Nothing aborts the process.
  *
- * Handles are opaque and owned by the library: a gat_db holds a trajectory set resident in
+ * Handles are opaque and owned by the library (destroy indexes, then trajectory sets, then the
+ * context they were made on): a gat_db holds a trajectory set resident in
  * device memory, a gat_index holds one of the reference's three range indexes (GT-quadtree
  * "Grid" with its FVTable, STIG, FSG) built on the host in the reference's exact layout and
  * resident in device memory. Host output buffers are owned by the caller; calls whose output
@@ -60,7 +61,9 @@ enum { GAT_RESULT_IDS = 0, GAT_RESULT_POINTS = 1 };
 enum { GAT_EXEC_PLAIN = 0, GAT_EXEC_BATCHED = 1 };
 
 /* ---------------------------------------------------------------- context */
-/* Creates a context bound to a CUDA device with its own stream. */
+/* Creates a context bound to a CUDA device with its own stream. device = -1 creates a
+ * host-only context: trajectory sets and indexes are built on the host (layout inspection via
+ * gat_index_points / gat_index_info) and every call that needs a GPU returns GAT_ERR_STATE. */
 int gat_ctx_create(int device, gat_ctx** out);
 void gat_ctx_destroy(gat_ctx* ctx);
 const char* gat_last_error(const gat_ctx* ctx);
@@ -71,6 +74,13 @@ int gat_ctx_sync(gat_ctx* ctx);
 int64_t gat_ctx_launches(const gat_ctx* ctx);
 /* Device bytes currently held by the context's scratch arena. */
 int64_t gat_ctx_scratch_bytes(const gat_ctx* ctx);
+/* Per-kernel timing: when on, launches of the kernel classes below are bracketed by CUDA
+ * events on the context stream; gat_ctx_kernel_stats returns their summed device time (ms),
+ * launch count and algorithmic work (DP cells for EDR, bytes for the others) since the last
+ * reset. Turning timing on resets the counters. */
+enum { GAT_KERNEL_EDR = 0, GAT_KERNEL_BOUNDS = 1, GAT_KERNEL_RANGE_SCAN = 2, GAT_KERNEL_CLASSES = 3 };
+int gat_ctx_set_timing(gat_ctx* ctx, int on);
+int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* launches, double* work);
 
 /* ---------------------------------------------------------------- trajectory set */
 int gat_db_create(gat_ctx* ctx, int n, const int32_t* lengths, const float* lon, const float* lat,
@@ -85,7 +95,8 @@ int gat_db_info(const gat_db* db, int64_t info[4]);
  * (MAXPOINTINNODE, ConstDefine.h:32), and the FVTable over virtual cells cell >> param. */
 int gat_grid_build(gat_ctx* ctx, const gat_db* db, gat_mbb range, float cell_size,
                    int virtual_cell_param, int leaf_cap, gat_index** out);
-/* STIG::initial(block_size, 2, ...) (STIG.cpp:35-168) */
+/* STIG::initial(block_size, 2, ...) (STIG.cpp:35-168); block_size >= 2 (smaller sizes make the
+ * reference's recursion endless) */
 int gat_stig_build(gat_ctx* ctx, const gat_db* db, int block_size, gat_index** out);
 /* FSG::FSG(range, cell_size) + addDatasetToGrid (FSG.cpp:7-143) */
 int gat_fsg_build(gat_ctx* ctx, const gat_db* db, gat_mbb range, float cell_size, gat_index** out);

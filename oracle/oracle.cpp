@@ -457,6 +457,7 @@ struct orc_stig {
 
 extern "C" orc_stig* orc_stig_build(int n, const int32_t* lengths, const float* lon, const float* lat,
                                     int block_size) {
+    if (block_size < 2) return nullptr; /* STIG.cpp:120-130 recurses without end below 2 */
     orc_stig* s = new orc_stig();
     s->block = block_size;
     /* STIG::initial (STIG.cpp:35-66): points in trajectory order */

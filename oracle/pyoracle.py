@@ -396,11 +396,12 @@ class RefRunner:
         r = read_out(o)
         return r["lb"].reshape(len(qids), traj.n + 1)
 
-    def topk(self, traj, qids, box, cell, k, eps):
+    def topk(self, traj, qids, box, cell, k, eps, reps=1, timeout=3600):
         d, i, o = self._path("d.bin"), self._path("i.bin"), self._path("o.bin")
         write_data(d, traj)
         write_ids(i, qids)
-        self._run(["topk", d, i, o, repr(float(cell)), k, repr(float(eps)), *[repr(float(v)) for v in box]])
+        self._run(["topk", d, i, o, repr(float(cell)), k, repr(float(eps)), *[repr(float(v)) for v in box], reps],
+                  timeout=timeout)
         r = read_out(o)
         r["ids"] = r["ids"].reshape(len(qids), k)
         r["dist"] = r["dist"].reshape(len(qids), k)

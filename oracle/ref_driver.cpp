@@ -613,7 +613,7 @@ int cmd_fvlb(int argc, char** argv) {
     return 0;
 }
 
-/* topk DATA QIDS OUT cell k eps bx0 by0 bx1 by1 : Grid::SimilarityQueryBatchCPUParallel
+/* topk DATA QIDS OUT cell k eps bx0 by0 bx1 by1 [reps] : Grid::SimilarityQueryBatchCPUParallel
  * (Grid.cpp:1133) with query j = tradb[qid[j]], the README's similarityQueryTest(queryTrajNo,..)
  * form. Output ids are in the reference's order (worst first, Grid.cpp:1202-1209); the EDR of
  * each returned id is recomputed with Grid::SimilarityExecuter so distance multisets can be
@@ -640,9 +640,14 @@ int cmd_topk(int argc, char** argv) {
     FILE* saved = stdout;
     stdout = fopen("/dev/null", "w");
     std::streambuf* old = std::cout.rdbuf(nullptr);
-    t0 = now_s();
-    g->SimilarityQueryBatchCPUParallel(qTra, nq, out.data(), k);
-    double t_query = now_s() - t0;
+    int reps = argc > 12 ? std::max(1, atoi(argv[12])) : 1;
+    std::vector<double> t_reps;
+    for (int r = 0; r < reps; r++) {
+        t0 = now_s();
+        g->SimilarityQueryBatchCPUParallel(qTra, nq, out.data(), k);
+        t_reps.push_back(now_s() - t0);
+    }
+    double t_query = t_reps.back();
     std::cout.rdbuf(old);
     fclose(stdout);
     stdout = saved;
@@ -665,6 +670,7 @@ int cmd_topk(int argc, char** argv) {
     w.i32("dist", dist);
     w.f64("t_build", {t_build});
     w.f64("t_query", {t_query});
+    w.f64("t_reps", t_reps);
     return 0;
 }
 

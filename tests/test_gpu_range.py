@@ -1,0 +1,104 @@
+"""Range queries on the GPU against the oracle (Grid.cpp:341-405 restated), all three indexes,
+plain and batched execution, id sets and point lists. Bit-exact: integer results."""
+import numpy as np
+import pytest
+
+import gat_b200 as G
+from gat_b200 import data as D
+from oracle import pyoracle as po
+from tests.conftest import csr_equal
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c1(gpu_ctx):
+    """config-1 shaped: 10k walks U[20,200], leaf cap 512, CELL_LEN 0.01; mixed query sizes."""
+    t, q = D.config1(seed=0)
+    q2 = D.boxes(500, 1, 0.001, 0.05, 11)  # uneven selectivity, some boxes cross the grid edge
+    edge = np.array([[121.0, 30.7, 121.01, 30.71], [121.995, 31.69, 122.05, 31.8], [120.9, 30.6, 121.2, 30.75],
+                     [121.5, 31.2, 121.5, 31.2], [121.3, 31.0, 121.3000001, 31.4], [122.5, 32.0, 122.6, 32.1]],
+                    np.float32)
+    qs = np.concatenate([q, q2, edge])
+    db = G.TrajectorySet(gpu_ctx, t)
+    return t, qs, db
+
+
+@pytest.mark.parametrize("execution", ["batched", "plain"])
+def test_grid_ids(gpu_ctx, c1, execution):
+    t, q, db = c1
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512)
+    o = po.OracleGrid(t, D.BOX, 0.01, 2, 512)
+    qq = q if execution == "batched" else q[::7]
+    r = g.range_query(qq, "ids", execution)
+    off, ids = o.range(qq, 0)
+    assert csr_equal(r.offsets, r.tids, off, ids)
+    assert gpu_ctx.launches > 0
+
+
+@pytest.mark.parametrize("execution", ["batched", "plain"])
+def test_grid_points(gpu_ctx, c1, execution):
+    t, q, db = c1
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512)
+    o = po.OracleGrid(t, D.BOX, 0.01, 2, 512)
+    qq = q if execution == "batched" else q[::9]
+    r = g.range_query(qq, "points", execution)
+    off, tid, pidx = o.range(qq, 1)
+    assert csr_equal(r.offsets, r.tids, off, tid)
+    assert np.array_equal(r.pidx, pidx)
+
+
+@pytest.mark.parametrize("result", ["ids", "points"])
+def test_stig(gpu_ctx, c1, result):
+    t, q, db = c1
+    s = G.STIG(gpu_ctx, db, 512)
+    o = po.OracleSTIG(t, 512)
+    r = s.range_query(q, result)
+    ref = o.range(q, 0 if result == "ids" else 1)
+    assert csr_equal(r.offsets, r.tids, ref[0], ref[1])
+    if result == "points":
+        assert np.array_equal(r.pidx, ref[2])
+
+
+@pytest.mark.parametrize("result", ["ids", "points"])
+def test_fsg(gpu_ctx, c1, result):
+    t, q, db = c1
+    f = G.FSG(gpu_ctx, db, D.BOX, 0.01)
+    o = po.OracleFSG(t, D.BOX, 0.01)
+    r = f.range_query(q, result)
+    ref = o.range(q, 0 if result == "ids" else 1)
+    assert csr_equal(r.offsets, r.tids, ref[0], ref[1])
+    if result == "points":
+        assert np.array_equal(r.pidx, ref[2])
+
+
+def test_empty_and_single(gpu_ctx, c1):
+    t, q, db = c1
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512)
+    r = g.range_query(np.zeros((0, 4), np.float32))
+    assert r.offsets.tolist() == [0] and len(r.tids) == 0
+    far = np.array([[10.0, 10.0, 11.0, 11.0]], np.float32)
+    r = g.range_query(far)
+    assert r.offsets.tolist() == [0, 0]
+
+
+def test_truncation_reports_needed(gpu_ctx, c1):
+    t, q, db = c1
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512)
+    full = g.range_query(q[:50])
+    with pytest.raises(G.GatError) as e:
+        g.range_query(q[:50], capacity=max(0, len(full.tids) - 1))
+    assert e.value.status == 4
+
+
+def test_tiny_leaf_cap_and_single_leaf(gpu_ctx):
+    """leaf cap 1 drives every node to the maximum level; a huge cap keeps the root a leaf."""
+    t = D.walks(D.lengths(300, 0, 0, 0, 1, 40, 5), 5)
+    q = D.boxes(100, 1, 0.001, 0.2, 6)
+    db = G.TrajectorySet(gpu_ctx, t)
+    for cap in (1, 10_000_000):
+        g = G.Grid(gpu_ctx, db, D.BOX, 0.02, 2, cap)
+        o = po.OracleGrid(t, D.BOX, 0.02, 2, cap)
+        r = g.range_query(q)
+        off, ids = o.range(q, 0)
+        assert csr_equal(r.offsets, r.tids, off, ids)

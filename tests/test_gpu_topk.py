@@ -1,0 +1,67 @@
+"""FV lower bounds and top-k on the GPU against the oracle (FVTable.cpp:77-207 and an
+exhaustive (distance, id) ranking over Grid::SimilarityExecuter)."""
+import numpy as np
+import pytest
+
+import gat_b200 as G
+from gat_b200 import data as D
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small(gpu_ctx):
+    t = D.walks(D.lengths(6000, 1, float(np.log(200.0)), 0.6, 32, 1024, 3), 3)
+    db = G.TrajectorySet(gpu_ctx, t)
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.0025, 2, 512)
+    o = po.OracleGrid(t, D.BOX, 0.0025, 2, 512)
+    qids = D.sample_ids(12, t.n, 4)
+    return t, g, o, qids
+
+
+def test_lower_bounds(small):
+    t, g, o, qids = small
+    q = t.subset(qids)
+    lb = g.fv_lower_bounds(q)
+    for j, qid in enumerate(qids):
+        lon, lat = t.points(int(qid))
+        want = o.fv_lb(lon, lat)
+        assert np.array_equal(lb[j, 1:], want[1:])
+
+
+@pytest.mark.parametrize("execution", ["batched", "plain"])
+@pytest.mark.parametrize("k", [1, 5, 32])
+def test_topk_matches_exhaustive(small, execution, k):
+    t, g, o, qids = small
+    q = t.subset(qids)
+    ids, dist, stats = g.topk(q, k, 5e-4, execution)
+    for j, qid in enumerate(qids):
+        lon, lat = t.points(int(qid))
+        wi, wd, _ = o.topk(lon, lat, k, 5e-4, pruned=False)
+        assert np.array_equal(dist[j], wd), (j, dist[j], wd)
+        assert np.array_equal(ids[j], wi), (j, ids[j], wi)
+    assert stats["pairs"] > 0 and stats["cells"] > 0
+
+
+def test_topk_external_queries_and_big_eps(small):
+    """queries that are not in the set (lengths 16..900) and a coarse eps = 0.005"""
+    t, g, o, _ = small
+    q = D.walks(D.lengths(6, 2, 0, 0, 16, 900, 9), 9)
+    ids, dist, _ = g.topk(q, 8, 0.005)
+    for j in range(q.n):
+        lon, lat = q.points(j + 1)
+        wi, wd, _ = o.topk(lon, lat, 8, 0.005, pruned=False)
+        assert np.array_equal(dist[j], wd) and np.array_equal(ids[j], wi)
+
+
+def test_k_larger_than_set(gpu_ctx):
+    t = D.walks(D.lengths(20, 0, 0, 0, 5, 30, 12), 12)
+    db = G.TrajectorySet(gpu_ctx, t)
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.0025, 2, 512)
+    o = po.OracleGrid(t, D.BOX, 0.0025, 2, 512)
+    q = t.subset([3])
+    ids, dist, _ = g.topk(q, 25, 5e-4)
+    wi, wd, _ = o.topk(*t.points(3), 25, 5e-4, pruned=False)
+    assert np.array_equal(ids[0], wi) and np.array_equal(dist[0], wd)
+    assert np.all(ids[0, 20:] == -1)
