@@ -195,6 +195,7 @@ enum Slot {
     S_TOPK_SEG,
     S_TOPK_IO,
     S_TOPK_OUT,
+    S_TOPK_NEAR,
     S_COUNT
 };
 

@@ -20,23 +20,14 @@
 #include <algorithm>
 #include <climits>
 
+#include "edr_kernel.cuh"
 #include "internal.h"
 
 namespace gat {
 namespace {
 
 constexpr int kT = 256;
-constexpr int kMaxRounds = 24;
 constexpr int kMaxFv = 128; /* merged frequency-vector entries per (query, trajectory) */
-
-/* per-query state words: the walk position (bound, id) of the last candidate taken, the
- * chunk end chosen for the current round, the k-th distance, the done flag */
-enum { QS_POS_LB = 0, QS_POS_ID, QS_END_LB, QS_END_ID, QS_W, QS_DONE, QS_EVAL, QS_WORDS };
-
-/* (bound, id) strictly after (plb, pid) in the walk order */
-__device__ __forceinline__ bool after(int v, int t, int plb, int pid) { return v > plb || (v == plb && t > pid); }
-/* (bound, id) at or before (elb, eid) */
-__device__ __forceinline__ bool upto(int v, int t, int elb, int eid) { return v < elb || (v == elb && t <= eid); }
 
 /* ---------------------------------------------------------------- reference cell ids */
 /* getIdxFromXY (Grid.cpp:25-54) as the x86-64 build evaluates it, negative inputs included:
@@ -47,20 +38,21 @@ __device__ __forceinline__ int ref_len(int v) {
     if (v < 0) return INT_MIN + 1;
     return 32 - __clz(v);
 }
-__device__ int ref_morton(int x, int y) {
-    int lx = ref_len(x), ly = ref_len(y);
-    long long lim = 2LL * max(lx, ly);
-    int result = 0, xbit = 1, ybit = 1;
-    for (int i = 1; i <= lim; i++) {
-        if (i & 1) {
-            result += ((x >> (xbit - 1)) & 1) * (1 << (i - 1));
-            xbit++;
-        } else {
-            result += ((y >> (ybit - 1)) & 1) * (1 << (i - 1));
-            ybit++;
-        }
-    }
-    return result;
+__device__ __forceinline__ uint32_t spread16(uint32_t v) {
+    v &= 0xFFFF;
+    v = (v | (v << 8)) & 0x00FF00FF;
+    v = (v | (v << 4)) & 0x0F0F0F0F;
+    v = (v | (v << 2)) & 0x33333333;
+    v = (v | (v << 1)) & 0x55555555;
+    return v;
+}
+/* Closed form of that loop: it interleaves the low L bits of x and y, L = the larger bit
+ * length (a negative input's length never wins), and yields 0 when both are negative. */
+__device__ __forceinline__ int ref_morton(int x, int y) {
+    if (x < 0 && y < 0) return 0;
+    int L = max(x < 0 ? 0 : ref_len(x), y < 0 ? 0 : ref_len(y));
+    uint32_t m = L >= 16 ? 0xFFFFu : ((1u << L) - 1u);
+    return (int)(spread16((uint32_t)x & m) | (spread16((uint32_t)y & m) << 1));
 }
 
 /* Grid::WhichCellPointIn (Grid.cpp:202-208) */
@@ -71,27 +63,60 @@ __device__ __forceinline__ int cell_of(const GridDev& g, float lon, float lat) {
 }
 
 /* ---------------------------------------------------------------- 1. query FV */
-/* one CTA per query: virtual cell of each point, bitonic sort in shared memory, run lengths.
+/* one CTA per query: virtual cell of each point, then runs of equal consecutive cells
+ * (a trajectory stays in a cell for many points), then the few runs sorted and merged.
  * qfv rows have stride `stride` (>= longest query); nnz in qfv_n. */
 __global__ void k_query_fv(GridDev g, int nq, const int32_t* q_len, const int64_t* q_off, const float2* Q,
                            int stride, int pow2, int32_t* qfv_cell, int32_t* qfv_cnt, int32_t* qfv_n) {
-    extern __shared__ int sk[];
+    extern __shared__ unsigned long long rkey[]; /* pow2 run keys (cell << 32 | count), then pow2 cells */
+    int* sk = reinterpret_cast<int*>(rkey + pow2);
+    __shared__ int wsum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
-        int L = q_len[qi];
-        int64_t o = q_off[qi];
-        for (int i = threadIdx.x; i < pow2; i += blockDim.x)
-            sk[i] = i < L ? (cell_of(g, Q[o + i].x, Q[o + i].y) >> g.vparam) : INT_MAX;
+        const int L = q_len[qi];
+        const int64_t o = q_off[qi];
+        for (int i = threadIdx.x; i < L; i += blockDim.x) sk[i] = cell_of(g, Q[o + i].x, Q[o + i].y) >> g.vparam;
         __syncthreads();
-        for (int k = 2; k <= pow2; k <<= 1)
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = threadIdx.x; i < pow2; i += blockDim.x) {
+        /* run heads, compacted in order (L <= pow2 <= blockDim.x * chunks) */
+        int base = 0;
+        for (int c0 = 0; c0 < L; c0 += blockDim.x) {
+            int i = c0 + threadIdx.x;
+            bool head = i < L && (i == 0 || sk[i] != sk[i - 1]);
+            unsigned bal = __ballot_sync(0xffffffffu, head);
+            if (lane == 0) wsum[warp] = __popc(bal);
+            __syncthreads();
+            int wb = 0, tot = 0;
+            for (int w = 0; w < nw; w++) {
+                if (w < warp) wb += wsum[w];
+                tot += wsum[w];
+            }
+            unsigned lt;
+            asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+            if (head) {
+                int r = base + wb + __popc(bal & lt);
+                int e = i + 1;
+                while (e < L && sk[e] == sk[i]) e++;
+                rkey[r] = ((unsigned long long)(unsigned)sk[i] << 32) | (unsigned)(e - i);
+            }
+            base += tot;
+            __syncthreads();
+        }
+        /* sort the runs by cell (bitonic over 64-bit (cell, count) keys in the run area),
+         * then one thread merges equal cells; runs are few, the sort is short */
+        const int R = base;
+        int p2 = 1;
+        while (p2 < R) p2 <<= 1;
+        for (int a = R + threadIdx.x; a < p2; a += blockDim.x) rkey[a] = ~0ull;
+        __syncthreads();
+        for (int kk = 2; kk <= p2; kk <<= 1)
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < p2; i += blockDim.x) {
                     int ixj = i ^ j;
                     if (ixj > i) {
-                        int a = sk[i], b = sk[ixj];
-                        bool up = (i & k) == 0;
-                        if ((a > b) == up) {
-                            sk[i] = b;
-                            sk[ixj] = a;
+                        unsigned long long a = rkey[i], b = rkey[ixj];
+                        if ((a > b) == ((i & kk) == 0)) {
+                            rkey[i] = b;
+                            rkey[ixj] = a;
                         }
                     }
                 }
@@ -99,12 +124,15 @@ __global__ void k_query_fv(GridDev g, int nq, const int32_t* q_len, const int64_
             }
         if (threadIdx.x == 0) {
             int w = 0;
-            for (int i = 0; i < L; i++) {
-                if (w > 0 && qfv_cell[(size_t)qi * stride + w - 1] == sk[i]) {
-                    qfv_cnt[(size_t)qi * stride + w - 1]++;
+            int32_t* oc = qfv_cell + (size_t)qi * stride;
+            int32_t* on = qfv_cnt + (size_t)qi * stride;
+            for (int a = 0; a < R; a++) {
+                int cell = (int)(rkey[a] >> 32), cnt = (int)(rkey[a] & 0xffffffffu);
+                if (w > 0 && oc[w - 1] == cell) {
+                    on[w - 1] += cnt;
                 } else {
-                    qfv_cell[(size_t)qi * stride + w] = sk[i];
-                    qfv_cnt[(size_t)qi * stride + w] = 1;
+                    oc[w] = cell;
+                    on[w] = cnt;
                     w++;
                 }
             }
@@ -115,6 +143,16 @@ __global__ void k_query_fv(GridDev g, int nq, const int32_t* q_len, const int64_
 }
 
 /* ---------------------------------------------------------------- 2. lower bounds */
+/* Virtual cells that can change a trajectory's bound: the query's cells (shared cells), the
+ * neighbour keys of the query's cells (pass 2 of FVTable.cpp:160-187 finds trajectory cells
+ * there) and the cells whose own neighbour keys hit a query cell (pass 1, FVTable.cpp:129-156).
+ * Away from the grid border the neighbour relation is symmetric, so the last set only needs
+ * checking for border cells. A trajectory with no cell in the set has bound
+ * max(its length, query length). */
+__global__ void k_near_bitmap(int nq, int vbits, const int32_t* qfv_cell, const int32_t* qfv_n, int stride, int words,
+                              uint32_t* near);
+
+/* ---------------------------------------------------------------- 2b. bound kernel */
 /* FVTable::findNeighbor (FVTable.cpp:53-75): x from even bits, y from odd bits of the
  * virtual cell id over log2(vcells) bits, neighbours in order xx = x-1..x+1, yy = y-1..y+1. */
 __device__ __forceinline__ void fv_neighbors(int cell, int bits, int nb[8]) {
@@ -145,6 +183,56 @@ __device__ __forceinline__ int find_key(const int* key, int n, int k) {
     return -1;
 }
 
+__device__ __forceinline__ bool in_qfv(const int32_t* qc, int qn, int c) {
+    int lo = 0, hi = qn - 1;
+    while (lo <= hi) {
+        int mid = (lo + hi) >> 1;
+        if (qc[mid] == c) return true;
+        if (qc[mid] < c)
+            lo = mid + 1;
+        else
+            hi = mid - 1;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void set_bit(uint32_t* bm, int words, int c) {
+    if (c >= 0 && (c >> 5) < words) atomicOr(&bm[c >> 5], 1u << (c & 31));
+}
+
+__global__ void k_near_bitmap(int nq, int vbits, const int32_t* qfv_cell, const int32_t* qfv_n, int stride, int words,
+                              uint32_t* near) {
+    int qi = blockIdx.x;
+    uint32_t* bm = near + (size_t)qi * words;
+    for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0;
+    __syncthreads();
+    const int qn = qfv_n[qi];
+    const int32_t* qc = qfv_cell + (size_t)qi * stride;
+    int nb[8];
+    for (int i = threadIdx.x; i < qn; i += blockDim.x) {
+        set_bit(bm, words, qc[i]);
+        fv_neighbors(qc[i], vbits, nb);
+        for (int k = 0; k < 8; k++) set_bit(bm, words, nb[k]);
+    }
+    /* border cells (virtual x or y equal to 0 or side - 1): at x == 0 / y == 0 findNeighbor's
+     * keys come from getIdxFromXY(-1, .); at the far border they can equal the id of a query
+     * point beyond the grid, whose own neighbours are decoded from its low bits only */
+    const int side = 1 << (vbits / 2);
+    for (int e = threadIdx.x; e < 4 * side; e += blockDim.x) {
+        int k4 = e / side, r = e % side;
+        int x = k4 == 0 ? 0 : k4 == 1 ? side - 1 : r;
+        int y = k4 == 0 || k4 == 1 ? r : (k4 == 2 ? 0 : side - 1);
+        int c = 0;
+        for (int bit = 0; bit < vbits / 2; bit++) c |= (((x >> bit) & 1) << (2 * bit)) | (((y >> bit) & 1) << (2 * bit + 1));
+        fv_neighbors(c, vbits, nb);
+        for (int k = 0; k < 8; k++)
+            if (in_qfv(qc, qn, nb[k])) {
+                set_bit(bm, words, c);
+                break;
+            }
+    }
+}
+
 /* one thread per (query, trajectory). The merged vector holds every cell of either vector
  * with value db - query (0 = absent). Pass 1 visits the positive cells in ascending order,
  * pass 2 the negative ones (FVTable.cpp:129-187); the reference increments a map iterator
@@ -153,10 +241,12 @@ __global__ void __launch_bounds__(kT) k_lower_bounds(int n, int nq, const int64_
                                                      const int32_t* __restrict__ fv_cell,
                                                      const int32_t* __restrict__ fv_cnt, const int32_t* qfv_cell,
                                                      const int32_t* qfv_cnt, const int32_t* qfv_n, int stride,
-                                                     int vbits, int32_t* lb, int32_t* flag) {
+                                                     int vbits, const uint32_t* __restrict__ near, int words,
+                                                     const int32_t* __restrict__ q_len, int32_t* lb, int32_t* flag) {
     extern __shared__ int sq[];
     int qi = blockIdx.y;
     int qn = qfv_n[qi];
+    const int qlen = q_len[qi];
     int* qc = sq;
     int* qv = sq + stride;
     for (int i = threadIdx.x; i < qn; i += blockDim.x) {
@@ -167,6 +257,20 @@ __global__ void __launch_bounds__(kT) k_lower_bounds(int n, int nq, const int64_
     int t = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (t > n) return;
     int64_t b = fv_off[t], e = fv_off[t + 1];
+    {
+        const uint32_t* bm = near + (size_t)qi * words;
+        bool touches = false;
+        int tlen = 0;
+        for (int64_t j = b; j < e; j++) {
+            int c = fv_cell[j];
+            tlen += fv_cnt[j];
+            if ((c >> 5) < words && ((__ldg(bm + (c >> 5)) >> (c & 31)) & 1u)) touches = true;
+        }
+        if (!touches) {
+            lb[(size_t)qi * (n + 1) + t] = max(tlen, qlen);
+            return;
+        }
+    }
     int key[kMaxFv], val[kMaxFv];
     int m = 0, i = 0;
     int64_t j = b;
@@ -254,182 +358,188 @@ __global__ void __launch_bounds__(kT) k_lower_bounds(int n, int nq, const int64_
     lb[(size_t)qi * (n + 1) + t] = max(sp, sn);
 }
 
-/* ---------------------------------------------------------------- 3. the walk */
-__device__ __forceinline__ unsigned lanemask_lt() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
+/* ---------------------------------------------------------------- 3. candidate order */
+/* Stable counting sort of every query's candidates by bound: tiles of kSortTile ids count
+ * their bounds (per-tile histograms laid out bound-major, tile-minor), one exclusive scan over
+ * all queries turns them into output positions, and one warp per tile scatters its ids in id
+ * order, so equal bounds keep ascending ids: the order is (bound, id). */
+constexpr int kSortTile = 2048;
+
+__global__ void k_sort_hist(int n, const int32_t* lb, int bins, int ntile, int64_t* H) {
+    extern __shared__ int hist[];
+    int tile = blockIdx.x, qi = blockIdx.y;
+    for (int i = threadIdx.x; i < bins; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const int32_t* row = lb + (size_t)qi * (n + 1);
+    int t0 = 1 + tile * kSortTile, t1 = min(n, (tile + 1) * kSortTile);
+    for (int t = t0 + threadIdx.x; t <= t1; t += blockDim.x) atomicAdd(&hist[min(row[t], bins - 1)], 1);
+    __syncthreads();
+    for (int v = threadIdx.x; v < bins; v += blockDim.x) H[((size_t)qi * bins + v) * ntile + tile] = hist[v];
 }
 
-__global__ void k_walk_init(int nq, int32_t* qs) {
+/* one warp per (tile, query); the tile's running output offset per bound lives in shared
+ * memory (loaded from the scanned histograms), the warp walks its ids in order 32 at a time */
+__global__ void __launch_bounds__(32) k_sort_scatter(int n, const int32_t* lb, int bins, int ntile, const int64_t* H,
+                                                     int32_t* cand, int32_t* slb) {
+    extern __shared__ long long run[];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x;
+    const int tile = blockIdx.x, qi = blockIdx.y;
+    for (int v = lane; v < bins; v += 32) run[v] = H[((size_t)qi * bins + v) * ntile + tile];
+    __syncwarp();
+    const int32_t* row = lb + (size_t)qi * (n + 1);
+    const int t0 = 1 + tile * kSortTile, t1 = min(n, (tile + 1) * kSortTile);
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    for (int b = t0; b <= t1; b += 32) {
+        const int t = b + lane;
+        const int raw = t <= t1 ? row[t] : -1;
+        const int v = raw < 0 ? -1 : min(raw, bins - 1);
+        const unsigned peers = __match_any_sync(FULL, v);
+        const int leader = __ffs(peers) - 1;
+        const int rank = __popc(peers & lt);
+        long long base = 0;
+        if (v >= 0 && lane == leader) {
+            base = run[v];
+            run[v] = base + __popc(peers);
+        }
+        base = __shfl_sync(FULL, base, leader);
+        if (v >= 0) {
+            const int64_t pos = base + rank; /* global position; query qi's slice starts at qi * n */
+            cand[pos] = t;
+            slb[pos] = raw;
+        }
+        __syncwarp();
+    }
+}
+
+/* ---------------------------------------------------------------- 4. the walk */
+/* per-query walk state */
+enum { WS_END = 0, WS_START, WS_CHUNK, WS_W, WS_DONE, WS_WORDS };
+
+__global__ void k_walk_init(int nq, int chunk, int32_t* ws) {
     int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= nq) return;
-    int32_t* s = qs + (size_t)qi * QS_WORDS;
-    s[QS_POS_LB] = -1;
-    s[QS_POS_ID] = 0;
-    s[QS_END_LB] = -1;
-    s[QS_END_ID] = 0;
-    s[QS_W] = INT_MAX;
-    s[QS_DONE] = 0;
-    s[QS_EVAL] = 0;
+    int32_t* s = ws + (size_t)qi * WS_WORDS;
+    s[WS_END] = 0;
+    s[WS_START] = 0;
+    s[WS_CHUNK] = chunk;
+    s[WS_W] = INT_MAX;
+    s[WS_DONE] = 0;
 }
 
-/* Chooses the end (elb, eid) of the next chunk: the `chunk` candidates that follow the walk
- * position in (bound, id) order, among bounds <= W (larger bounds can never be needed). A
- * histogram over bound values finds elb; an ordered scan of the ids with bound elb finds eid. */
-__global__ void k_walk_select(int n, const int32_t* lb, int chunk, int bins, int32_t* qs) {
+/* One CTA: each unfinished query extends its evaluated prefix [0, end) of the (bound, id)
+ * order by up to `chunk` candidates whose bound is at most W; the new slices are numbered
+ * consecutively over the queries (wprefix) for the EDR kernel. */
+__global__ void k_walk_plan(int n, int nq, const int32_t* slb, int32_t* ws, int* wprefix) {
+    __shared__ int warp_sum[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int q0 = 0; q0 < nq; q0 += blockDim.x) {
+        int qi = q0 + threadIdx.x;
+        int cnt = 0;
+        if (qi < nq) {
+            int32_t* s = ws + (size_t)qi * WS_WORDS;
+            int end = s[WS_END];
+            s[WS_START] = end;
+            if (!s[WS_DONE]) {
+                int e = (int)min((long long)n, (long long)end + s[WS_CHUNK]);
+                /* candidates with a bound above W can never be needed */
+                int W = s[WS_W];
+                const int32_t* row = slb + (size_t)qi * n;
+                if (e > end && row[e - 1] > W) {
+                    int lo = end, hi = e - 1; /* first index in [end, e) with bound > W */
+                    while (lo < hi) {
+                        int mid = (lo + hi) >> 1;
+                        if (row[mid] > W)
+                            hi = mid;
+                        else
+                            lo = mid + 1;
+                    }
+                    e = lo;
+                }
+                cnt = e - end;
+                s[WS_END] = e;
+            }
+        }
+        int x = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sum[warp] = x;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int run = 0;
+            for (int w = 0; w < nw; w++) {
+                int t = warp_sum[w];
+                warp_sum[w] = run;
+                run += t;
+            }
+        }
+        __syncthreads();
+        if (qi < nq) wprefix[qi] = carry + warp_sum[warp] + x - cnt;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += warp_sum[warp] + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) wprefix[nq] = carry;
+}
+
+/* EDR pairs of the current round: work item w belongs to the query whose wprefix range holds
+ * it, and is candidate start + (w - wprefix[q]) of that query's order. */
+struct WalkPairs {
+    int n, nq;
+    const int* wprefix;
+    const int32_t* ws;
+    const int32_t* cand;
+    const int32_t* q_len;
+    const int64_t* q_off;
+    const float2* Q;
+    const int32_t* db_len;
+    const int64_t* db_off;
+    const float2* DB;
+    int32_t* sdist;
+    __device__ int count() const { return wprefix[nq]; }
+    __device__ void get(int w, const float2*& a, int& la, const float2*& b, int& lb, int32_t*& o) const {
+        int lo = 0, hi = nq - 1; /* last q with wprefix[q] <= w */
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (wprefix[mid] <= w)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        int q = lo;
+        size_t idx = (size_t)q * n + ws[(size_t)q * WS_WORDS + WS_START] + (w - wprefix[q]);
+        int t = cand[idx];
+        a = Q + q_off[q];
+        la = q_len[q];
+        b = DB + db_off[t];
+        lb = db_len[t];
+        o = sdist + idx;
+    }
+};
+
+/* Per query: W = k-th smallest distance over the evaluated prefix, then the stop rule with
+ * (nlb, nid) the next candidate: done at the end of the order, when nlb > W, or when nlb == W
+ * and k evaluated pairs already sort before (W, nid). While nlb < W the walk goes on: a
+ * candidate with a smaller bound may still be closer. */
+__global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* slb, const int32_t* cand,
+                           const int32_t* sdist, int32_t* ws) {
     extern __shared__ int hist[];
-    __shared__ int sh_elb, sh_need, sh_eid, sh_seen;
-    __shared__ int wtot[kT / 32];
+    __shared__ int sh_W, cnt;
     int qi = blockIdx.x;
-    int32_t* s = qs + (size_t)qi * QS_WORDS;
-    if (s[QS_DONE]) return;
-    const int plb = s[QS_POS_LB], pid = s[QS_POS_ID], W = s[QS_W];
+    int32_t* s = ws + (size_t)qi * WS_WORDS;
+    if (s[WS_DONE]) return;
+    const int end = s[WS_END];
+    const int32_t* dist = sdist + (size_t)qi * n;
     for (int i = threadIdx.x; i < bins; i += blockDim.x) hist[i] = 0;
+    if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
-    const int32_t* row = lb + (size_t)qi * (n + 1);
-    for (int t = 1 + threadIdx.x; t <= n; t += blockDim.x) {
-        int v = row[t];
-        if (v <= W && after(v, t, plb, pid)) atomicAdd(&hist[min(v, bins - 1)], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0, v = -1, need = 0;
-        for (int i = max(plb, 0); i < bins; i++) {
-            if (hist[i] == 0) continue;
-            v = i;
-            if (run + hist[i] >= chunk) {
-                need = chunk - run;
-                break;
-            }
-            run += hist[i];
-            need = -1; /* the whole bucket fits */
-        }
-        sh_elb = v;
-        sh_need = need;
-        sh_eid = v < 0 ? 0 : n;
-        sh_seen = 0;
-    }
-    __syncthreads();
-    const int elb = sh_elb, need = sh_need;
-    if (elb >= 0 && need > 0) {
-        int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int t0 = 1; t0 <= n; t0 += blockDim.x) {
-            int t = t0 + threadIdx.x;
-            bool h = t <= n && row[t] == elb && after(elb, t, plb, pid);
-            unsigned bal = __ballot_sync(0xffffffffu, h);
-            if (lane == 0) wtot[warp] = __popc(bal);
-            __syncthreads();
-            int wb = 0, tt = 0;
-            for (int w = 0; w < kT / 32; w++) {
-                if (w < warp) wb += wtot[w];
-                tt += wtot[w];
-            }
-            int seen = sh_seen;
-            int rank = seen + wb + __popc(bal & lanemask_lt());
-            if (h && rank == need - 1) sh_eid = t;
-            __syncthreads();
-            if (threadIdx.x == 0) sh_seen = seen + tt;
-            __syncthreads();
-            if (sh_seen >= need) break;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        if (elb < 0) {
-            s[QS_DONE] = 1; /* nothing left below W */
-        } else {
-            s[QS_END_LB] = elb;
-            s[QS_END_ID] = sh_eid;
-        }
-    }
-}
-
-/* Appends the query's chunk (walk position, chunk end] as EDR pairs and advances the walk. */
-__global__ void __launch_bounds__(kT) k_walk_compact(int n, const int32_t* lb, int32_t* qs, const int32_t* q_len,
-                                                     const int64_t* q_off, const int32_t* db_len,
-                                                     const int64_t* db_off, int64_t cap, unsigned long long* cursor,
-                                                     int32_t* pq, int32_t* pt, int64_t* aoff, int32_t* alen,
-                                                     int64_t* boff, int32_t* blen, int64_t* seg_base, int64_t* seg_cnt) {
-    __shared__ int wtot[kT / 32];
-    __shared__ int sh_total;
-    __shared__ unsigned long long sh_base;
-    int qi = blockIdx.x;
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int32_t* s = qs + (size_t)qi * QS_WORDS;
-    const bool active = !s[QS_DONE];
-    const int plb = s[QS_POS_LB], pid = s[QS_POS_ID], elb = s[QS_END_LB], eid = s[QS_END_ID];
-    const int32_t* row = lb + (size_t)qi * (n + 1);
-    auto pick = [&](int t) -> bool {
-        int v = row[t];
-        return after(v, t, plb, pid) && upto(v, t, elb, eid);
-    };
-    int c = 0;
-    if (active)
-        for (int t = 1 + threadIdx.x; t <= n; t += blockDim.x) c += pick(t);
-    if (threadIdx.x == 0) sh_total = 0;
-    __syncthreads();
-    atomicAdd(&sh_total, c);
-    __syncthreads();
-    const int total = sh_total;
-    if (threadIdx.x == 0) sh_base = atomicAdd(cursor, (unsigned long long)total);
-    __syncthreads();
-    const int64_t base = (int64_t)sh_base;
-    const bool fits = base + total <= cap;
-    int written = 0;
-    if (active && fits && total > 0) {
-        for (int t0 = 1; t0 <= n; t0 += blockDim.x) {
-            int t = t0 + threadIdx.x;
-            bool h = t <= n && pick(t);
-            unsigned bal = __ballot_sync(0xffffffffu, h);
-            if (lane == 0) wtot[warp] = __popc(bal);
-            __syncthreads();
-            int wb = 0, tt = 0;
-            for (int w = 0; w < kT / 32; w++) {
-                if (w < warp) wb += wtot[w];
-                tt += wtot[w];
-            }
-            if (h) {
-                int64_t o = base + written + wb + __popc(bal & lanemask_lt());
-                pq[o] = qi;
-                pt[o] = t;
-                aoff[o] = q_off[qi];
-                alen[o] = q_len[qi];
-                boff[o] = db_off[t];
-                blen[o] = db_len[t];
-            }
-            written += tt;
-            __syncthreads();
-            if (written >= total) break;
-        }
-    }
-    if (threadIdx.x == 0) {
-        seg_base[qi] = base;
-        seg_cnt[qi] = active ? (fits ? total : -1) : 0;
-        if (active && fits) {
-            s[QS_POS_LB] = elb;
-            s[QS_POS_ID] = eid;
-        }
-    }
-}
-
-/* ---------------------------------------------------------------- 4. k-th distance, stop rule */
-/* W = k-th smallest evaluated distance (INT_MAX while fewer than k). */
-__global__ void k_kth(int nrounds, const int64_t* seg_base, const int64_t* seg_cnt, int nq, const int32_t* dist,
-                      int k, int bins, int32_t* qs) {
-    extern __shared__ int hist[];
-    int qi = blockIdx.x;
-    int32_t* s = qs + (size_t)qi * QS_WORDS;
-    if (s[QS_DONE]) return;
-    for (int i = threadIdx.x; i < bins; i += blockDim.x) hist[i] = 0;
-    __syncthreads();
-    int64_t nev = 0;
-    for (int r = 0; r < nrounds; r++) {
-        int64_t b = seg_base[(size_t)r * nq + qi], c = seg_cnt[(size_t)r * nq + qi];
-        if (c <= 0) continue;
-        nev += c;
-        for (int64_t i = threadIdx.x; i < c; i += blockDim.x) atomicAdd(&hist[min(dist[b + i], bins - 1)], 1);
-    }
+    for (int i = threadIdx.x; i < end; i += blockDim.x) atomicAdd(&hist[min(dist[i], bins - 1)], 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         int run = 0, W = INT_MAX;
@@ -440,96 +550,69 @@ __global__ void k_kth(int nrounds, const int64_t* seg_base, const int64_t* seg_c
             }
             run += hist[i];
         }
-        s[QS_W] = W;
-        s[QS_EVAL] = (int)nev;
-    }
-}
-
-/* Stop rule, with (nlb, nid) the first candidate after the walk position: done when there is
- * none with bound <= W, or when nlb == W and k evaluated pairs already sort before (W, nid).
- * While nlb < W the walk must go on: a candidate with a smaller bound may be closer. */
-__global__ void k_walk_check(int n, const int32_t* lb, int nrounds, const int64_t* seg_base, const int64_t* seg_cnt,
-                             int nq, const int32_t* dist, const int32_t* pt, int k, int32_t* qs, int* pending) {
-    __shared__ unsigned long long sh_next;
-    __shared__ int cnt;
-    int qi = blockIdx.x;
-    int32_t* s = qs + (size_t)qi * QS_WORDS;
-    if (s[QS_DONE]) return;
-    const int W = s[QS_W], plb = s[QS_POS_LB], pid = s[QS_POS_ID];
-    if (threadIdx.x == 0) {
-        sh_next = ~0ull;
-        cnt = 0;
+        sh_W = W;
     }
     __syncthreads();
-    const int32_t* row = lb + (size_t)qi * (n + 1);
-    unsigned long long best = ~0ull;
-    for (int t = 1 + threadIdx.x; t <= n; t += blockDim.x) {
-        int v = row[t];
-        if (v <= W && after(v, t, plb, pid)) {
-            unsigned long long key = ((unsigned long long)(unsigned)v << 32) | (unsigned)t;
-            if (key < best) best = key;
-        }
-    }
-    if (best != ~0ull) atomicMin(&sh_next, best);
-    __syncthreads();
-    const unsigned long long nx = sh_next;
+    const int W = sh_W;
     bool done;
-    if (nx == ~0ull) {
+    if (end >= n) {
         done = true;
     } else {
-        int nlb = (int)(nx >> 32), nid = (int)(nx & 0xffffffffu);
+        int nlb = slb[(size_t)qi * n + end];
         if (nlb < W) {
             done = false;
+        } else if (nlb > W) {
+            done = true;
         } else {
-            for (int r = 0; r < nrounds; r++) {
-                int64_t b = seg_base[(size_t)r * nq + qi], c = seg_cnt[(size_t)r * nq + qi];
-                for (int64_t i = threadIdx.x; i < c; i += blockDim.x) {
-                    int d = dist[b + i];
-                    if (d < W || (d == W && pt[b + i] < nid)) atomicAdd(&cnt, 1);
-                }
+            int nid = cand[(size_t)qi * n + end];
+            const int32_t* ids = cand + (size_t)qi * n;
+            int c = 0;
+            for (int i = threadIdx.x; i < end; i += blockDim.x) {
+                int d = dist[i];
+                c += (d < W || (d == W && ids[i] < nid));
             }
+            atomicAdd(&cnt, c);
             __syncthreads();
             done = cnt >= k;
         }
     }
     if (threadIdx.x == 0) {
-        s[QS_DONE] = done ? 1 : 0;
-        if (!done) atomicAdd(pending, 1);
+        s[WS_W] = W;
+        s[WS_DONE] = done ? 1 : 0;
+        s[WS_CHUNK] = (int)min((long long)growth * s[WS_CHUNK], 1LL << 30);
     }
 }
 
 /* ---------------------------------------------------------------- 5. selection */
-/* k smallest (distance, id): the LT pairs below W sorted, then the k - LT smallest ids at W
- * (a bitmap over ids in shared memory or a per-CTA global slice). */
-__global__ void k_final(int nrounds, const int64_t* seg_base, const int64_t* seg_cnt, int nq, const int32_t* dist,
-                        const int32_t* pt, int k, int words, uint32_t* gbitmap, const int32_t* qs, int32_t* out_ids,
-                        int32_t* out_dist) {
+/* k smallest (distance, id) over the evaluated prefix: the pairs below W sorted, then the
+ * smallest ids at W (a bitmap over ids in shared memory or a per-CTA global slice). */
+__global__ void k_final(int n, int k, int words, uint32_t* gbitmap, const int32_t* cand, const int32_t* sdist,
+                        const int32_t* ws, int32_t* out_ids, int32_t* out_dist, int32_t* flag) {
     extern __shared__ uint32_t bm_s[];
     __shared__ unsigned long long lt_keys[1024];
     __shared__ int lt_n;
     __shared__ int warp_cnt[kT / 32 + 1];
     int qi = blockIdx.x;
     uint32_t* bm = gbitmap ? gbitmap + (size_t)blockIdx.x * words : bm_s;
-    const int32_t* s = qs + (size_t)qi * QS_WORDS;
-    int W = s[QS_W];
+    const int32_t* s = ws + (size_t)qi * WS_WORDS;
+    if (threadIdx.x == 0 && !s[WS_DONE]) atomicCAS(flag, 0, GAT_ERR_STATE);
+    const int W = s[WS_W], end = s[WS_END];
+    const int32_t* dist = sdist + (size_t)qi * n;
+    const int32_t* ids = cand + (size_t)qi * n;
     for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0;
     if (threadIdx.x == 0) lt_n = 0;
     __syncthreads();
-    for (int r = 0; r < nrounds; r++) {
-        int64_t b = seg_base[(size_t)r * nq + qi], c = seg_cnt[(size_t)r * nq + qi];
-        for (int64_t i = threadIdx.x; i < c; i += blockDim.x) {
-            int d = dist[b + i], id = pt[b + i];
-            if (d < W) {
-                int slot = atomicAdd(&lt_n, 1);
-                if (slot < 1024) lt_keys[slot] = ((unsigned long long)(unsigned)d << 32) | (unsigned)id;
-            } else if (d == W) {
-                atomicOr(&bm[id >> 5], 1u << (id & 31));
-            }
+    for (int i = threadIdx.x; i < end; i += blockDim.x) {
+        int d = dist[i], id = ids[i];
+        if (d < W) {
+            int slot = atomicAdd(&lt_n, 1);
+            if (slot < 1024) lt_keys[slot] = ((unsigned long long)(unsigned)d << 32) | (unsigned)id;
+        } else if (d == W) {
+            atomicOr(&bm[id >> 5], 1u << (id & 31));
         }
     }
     __syncthreads();
     int nlt = min(lt_n, 1024);
-    /* sort the (few) pairs below W */
     int p2 = 1;
     while (p2 < nlt) p2 <<= 1;
     for (int i = nlt + threadIdx.x; i < p2; i += blockDim.x) lt_keys[i] = ~0ull;
@@ -554,13 +637,11 @@ __global__ void k_final(int nrounds, const int64_t* seg_base, const int64_t* seg
         out_ids[(size_t)qi * k + i] = (int32_t)(lt_keys[i] & 0xffffffffu);
         out_dist[(size_t)qi * k + i] = (int32_t)(lt_keys[i] >> 32);
     }
-    /* the k - emit smallest ids at distance W, in ascending order */
     int need = k - emit;
     int per = (words + kT - 1) / kT;
     int w0 = threadIdx.x * per, w1 = min(words, w0 + per);
     int c = 0;
     for (int w = w0; w < w1; w++) c += __popc(bm[w]);
-    /* exclusive scan over threads */
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int x = c;
     for (int o = 1; o < 32; o <<= 1) {
@@ -579,7 +660,6 @@ __global__ void k_final(int nrounds, const int64_t* seg_base, const int64_t* seg
         warp_cnt[kT / 32] = run;
     }
     __syncthreads();
-    const int last_warp_incl = warp_cnt[kT / 32] - warp_cnt[kT / 32 - 1];
     int pre = warp_cnt[warp] + x - c;
     for (int w = w0; w < w1 && pre < need; w++) {
         uint32_t v = bm[w];
@@ -591,10 +671,8 @@ __global__ void k_final(int nrounds, const int64_t* seg_base, const int64_t* seg
             pre++;
         }
     }
-    /* fewer than k candidates in the whole set: pad with -1 */
     if (threadIdx.x == 0) {
-        int ties = warp_cnt[kT / 32 - 1] + last_warp_incl;
-        int have = emit + min(ties, need);
+        int have = emit + min(warp_cnt[kT / 32], need);
         for (int i = have; i < k; i++) {
             out_ids[(size_t)qi * k + i] = -1;
             out_dist[(size_t)qi * k + i] = -1;
@@ -602,54 +680,32 @@ __global__ void k_final(int nrounds, const int64_t* seg_base, const int64_t* seg
     }
 }
 
-struct PairBufs {
-    int32_t *pq, *pt, *alen, *blen, *dist;
-    int64_t *aoff, *boff;
-    int64_t cap;
-};
-
-size_t pair_bytes(int64_t cap) { return (size_t)cap * (4 * 5 + 8 * 2) + 7 * 256; }
-int64_t pair_cap(size_t bytes) { return bytes < 7 * 256 ? 0 : (int64_t)((bytes - 7 * 256) / (4 * 5 + 8 * 2)); }
-
-void carve_pairs(char* base, int64_t c, PairBufs& o) {
-    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    char* p = base;
-    o.pq = (int32_t*)p; p += up((size_t)c * 4);
-    o.pt = (int32_t*)p; p += up((size_t)c * 4);
-    o.alen = (int32_t*)p; p += up((size_t)c * 4);
-    o.blen = (int32_t*)p; p += up((size_t)c * 4);
-    o.dist = (int32_t*)p; p += up((size_t)c * 4);
-    o.aoff = (int64_t*)p; p += up((size_t)c * 8);
-    o.boff = (int64_t*)p;
-    o.cap = c;
-}
-
-/* grows the pair arrays (scratch slot S_TOPK_PAIRS), preserving the first `keep` entries */
-int ensure_pairs(gat_ctx* ctx, PairBufs& P, int64_t need, int64_t keep) {
-    if (need <= P.cap) return GAT_OK;
-    int64_t cap = std::max<int64_t>(need, P.cap * 2);
-    void* nb = nullptr;
-    cudaError_t e = cudaMalloc(&nb, pair_bytes(cap));
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "top-k pair buffer");
-    PairBufs N;
-    carve_pairs((char*)nb, cap, N);
-    cudaStream_t s = ctx->stream;
-    if (P.cap > 0 && keep > 0) {
-        cudaMemcpyAsync(N.pq, P.pq, keep * 4, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(N.pt, P.pt, keep * 4, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(N.alen, P.alen, keep * 4, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(N.blen, P.blen, keep * 4, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(N.dist, P.dist, keep * 4, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(N.aoff, P.aoff, keep * 8, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(N.boff, P.boff, keep * 8, cudaMemcpyDeviceToDevice, s);
-    }
-    if (ctx->slot_ptr[S_TOPK_PAIRS]) {
-        cudaStreamSynchronize(s);
-        cudaFree(ctx->slot_ptr[S_TOPK_PAIRS]);
-    }
-    ctx->slot_ptr[S_TOPK_PAIRS] = nb;
-    ctx->slot_bytes[S_TOPK_PAIRS] = pair_bytes(cap);
-    P = N;
+/* persistent EDR launch over a device-counted pair source */
+template <class Src>
+int edr_launch_src(gat_ctx* ctx, const Src& src, int rows_hint, int max_cols, float u, unsigned long long* cells) {
+    using edr::k_edr;
+    using edr::kWarps;
+    int st = GAT_OK;
+    const int R = rows_hint <= 128 ? 4 : 8;
+    int per_sm = 0;
+    if (R == 4)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr<4, Src>, kWarps * 32, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr<8, Src>, kWarps * 32, 0);
+    int grid = ctx->sm_count * std::max(1, per_sm);
+    int stride = max_cols + 2;
+    int* carry = (int*)scratch(ctx, S_EDR_CARRY, (size_t)grid * kWarps * 2 * stride * sizeof(int), &st);
+    unsigned* work = (unsigned*)scratch(ctx, S_EDR_COUNTERS, 64, &st);
+    if (!carry || !work) return st;
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(work, 0, sizeof(unsigned), ctx->stream), "edr");
+    timed_begin(ctx, GAT_KERNEL_EDR);
+    if (R == 4)
+        k_edr<4, Src><<<grid, kWarps * 32, 0, ctx->stream>>>(src, u, carry, stride, work, cells);
+    else
+        k_edr<8, Src><<<grid, kWarps * 32, 0, ctx->stream>>>(src, u, carry, stride, work, cells);
+    timed_end(ctx, GAT_KERNEL_EDR, 0.0);
+    count_launch(ctx);
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "edr launch");
     return GAT_OK;
 }
 
@@ -658,6 +714,12 @@ int read_word(gat_ctx* ctx, const void* d, int64_t* v) {
     GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "top-k");
     *v = ctx->h_pinned[0];
     return GAT_OK;
+}
+
+/* device bytes topk_batch needs per query (sorted candidates, bounds, distances, histograms) */
+size_t topk_bytes_per_query(int n, int bins) {
+    int ntile = (n + kSortTile - 1) / kSortTile;
+    return (size_t)(n + 1) * 4 + (size_t)n * 12 + (size_t)bins * ntile * 8 + 64;
 }
 
 /* the whole pipeline for queries [0, nq) of the given device arrays */
@@ -677,7 +739,7 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     int32_t* qfv_cell = (int32_t*)qfv;
     int32_t* qfv_cnt = (int32_t*)(qfv + fvb);
     int32_t* qfv_n = (int32_t*)(qfv + 2 * fvb);
-    size_t smem_fv = (size_t)pow2 * 4;
+    size_t smem_fv = (size_t)pow2 * 12;
     if (smem_fv > 48 * 1024) cudaFuncSetAttribute(k_query_fv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fv);
     k_query_fv<<<std::min(nq, ctx->sm_count * 4), 512, smem_fv, s>>>(g->grid, nq, d_q_len, d_q_off, d_q_xy, stride, pow2,
                                                                       qfv_cell, qfv_cnt, qfv_n);
@@ -686,12 +748,17 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     int32_t* lb = (int32_t*)scratch(ctx, S_TOPK_LB, (size_t)nq * (n + 1) * 4, &st);
     if (!lb) return st;
     int vbits = (int)std::log2((double)(g->grid.cellnum >> 2));
+    int nwords = ((1 << vbits) + 31) / 32;
+    uint32_t* near = (uint32_t*)scratch(ctx, S_TOPK_NEAR, (size_t)nq * nwords * 4 + 64, &st);
+    if (!near) return st;
+    k_near_bitmap<<<nq, kT, 0, s>>>(nq, vbits, qfv_cell, qfv_n, stride, nwords, near);
+    count_launch(ctx);
     size_t smem_lb = (size_t)stride * 8;
     if (smem_lb > 48 * 1024) cudaFuncSetAttribute(k_lower_bounds, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_lb);
     dim3 lgrid((n + kT - 1) / kT, nq);
     timed_begin(ctx, GAT_KERNEL_BOUNDS);
     k_lower_bounds<<<lgrid, kT, smem_lb, s>>>(n, nq, g->d_fv_off, g->d_fv_cell, g->d_fv_cnt, qfv_cell, qfv_cnt, qfv_n, stride,
-                                             vbits, lb, ctx->d_flag);
+                                             vbits, near, nwords, d_q_len, lb, ctx->d_flag);
     /* algorithmic bytes: every trajectory's FV (8 B per entry + 8 B offset) and its bound (4 B)
      * per query */
     timed_end(ctx, GAT_KERNEL_BOUNDS, (double)nq * ((double)g->fv_entries * 8.0 + (double)n * 12.0));
@@ -699,78 +766,58 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     if (stats && stats[3] == -1) { /* bounds only */
         return check_device_flag(ctx, "frequency-vector bounds");
     }
-    /* per-query state + segments */
-    int32_t* qs = (int32_t*)scratch(ctx, S_TOPK_QSTATE, (size_t)nq * QS_WORDS * 4 + 256, &st);
-    int64_t* seg = (int64_t*)scratch(ctx, S_TOPK_SEG, (size_t)kMaxRounds * nq * 2 * 8 + 256, &st);
-    unsigned long long* cursor = (unsigned long long*)scratch(ctx, S_TOPK_IO, 256, &st);
-    if (!qs || !seg || !cursor) return st;
-    int64_t* seg_base = seg;
-    int64_t* seg_cnt = seg + (size_t)kMaxRounds * nq;
-    unsigned long long* cells = cursor + 1;
-    int* pending = (int*)(cursor + 2);
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 64, s), "top-k");
+    /* candidate order */
     int bins_lb = std::max(max_q_len, db->maxlen) + 2;
-    int bins_d = max_q_len + db->maxlen + 2;
-    size_t smem_lbh = (size_t)bins_lb * 4, smem_dh = (size_t)bins_d * 4;
-    if (smem_dh > 48 * 1024) cudaFuncSetAttribute(k_kth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dh);
-    k_walk_init<<<(nq + 127) / 128, 128, 0, s>>>(nq, qs);
+    int ntile = (n + kSortTile - 1) / kSortTile;
+    int64_t* H = (int64_t*)scratch(ctx, S_TOPK_SEG, (size_t)nq * bins_lb * ntile * 8 + 64, &st);
+    char* sorted = (char*)scratch(ctx, S_TOPK_PAIRS, (size_t)nq * n * 12 + 1024, &st);
+    int32_t* ws = (int32_t*)scratch(ctx, S_TOPK_QSTATE, (size_t)nq * WS_WORDS * 4 + (size_t)(nq + 1) * 4 + 256, &st);
+    unsigned long long* cells = (unsigned long long*)scratch(ctx, S_TOPK_IO, 256, &st);
+    if (!H || !sorted || !ws || !cells) return st;
+    int32_t* cand = (int32_t*)sorted;
+    int32_t* slb = cand + (size_t)nq * n;
+    int32_t* sdist = slb + (size_t)nq * n;
+    int* wprefix = (int*)(ws + (size_t)nq * WS_WORDS);
+    size_t smem_h = (size_t)bins_lb * 4;
+    if (smem_h > 48 * 1024) cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_h);
+    k_sort_hist<<<dim3(ntile, nq), kT, smem_h, s>>>(n, lb, bins_lb, ntile, H);
     count_launch(ctx);
-    if (smem_lbh > 48 * 1024) cudaFuncSetAttribute(k_walk_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_lbh);
-
-    PairBufs P{};
-    if (ctx->slot_ptr[S_TOPK_PAIRS]) carve_pairs((char*)ctx->slot_ptr[S_TOPK_PAIRS], pair_cap(ctx->slot_bytes[S_TOPK_PAIRS]), P);
-    int chunk = std::max(4 * k, 128);
-    if ((st = ensure_pairs(ctx, P, std::max<int64_t>((int64_t)nq * chunk * 2, 1 << 16), 0)) != GAT_OK) return st;
-
-    int rounds = 0;
-    int64_t used = 0;
+    if ((st = scan_i64(ctx, H, H, (int64_t)nq * bins_lb * ntile)) != GAT_OK) return st;
+    size_t smem_run = (size_t)bins_lb * 8;
+    if (smem_run > 48 * 1024) cudaFuncSetAttribute(k_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_run);
+    k_sort_scatter<<<dim3(ntile, nq), 32, smem_run, s>>>(n, lb, bins_lb, ntile, H, cand, slb);
+    count_launch(ctx);
+    /* the walk: rounds need no host round trip; a finished query costs nothing in later
+     * rounds, and `rounds` covers the whole order with doubling chunks */
+    /* a lone query leaves most of the GPU idle in a small round, so it starts with a larger
+     * chunk and grows faster; a batch keeps rounds tight to limit surplus evaluations */
+    const bool lone = nq <= 4;
+    int chunk0 = lone ? std::max(8 * k, 1024) : std::max(4 * k, 128);
+    int growth = lone ? 4 : 2;
+    int rounds = 1;
+    for (int64_t cover = chunk0, c = chunk0; cover < n; rounds++) {
+        c *= growth;
+        cover += c;
+    }
+    rounds += 1;
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(cells, 0, 8, s), "top-k");
+    k_walk_init<<<(nq + 127) / 128, 128, 0, s>>>(nq, chunk0, ws);
+    count_launch(ctx);
+    int bins_d = max_q_len + db->maxlen + 2;
+    size_t smem_d = (size_t)bins_d * 4;
+    if (smem_d > 48 * 1024) cudaFuncSetAttribute(k_walk_kth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_d);
     int rows_hint = std::min(max_q_len, db->maxlen);
     int max_cols = std::max(max_q_len, db->maxlen);
-    int words = (n + 1 + 31) / 32;
-    /* the walk: each round takes the next `chunk` candidates of every unfinished query in
-     * (bound, id) order, evaluates them, updates W and applies the stop rule; chunks grow
-     * geometrically so a query needs O(log) rounds */
-    for (;;) {
-        if (rounds >= kMaxRounds) return fail(ctx, GAT_ERR_STATE, "top-k: candidate walk did not finish");
-        k_walk_select<<<nq, kT, smem_lbh, s>>>(n, lb, chunk, bins_lb, qs);
+    WalkPairs src{n, nq, wprefix, ws, cand, d_q_len, d_q_off, d_q_xy, db->d_len, db->d_off, db->d_xy, sdist};
+    for (int r = 0; r < rounds; r++) {
+        k_walk_plan<<<1, 1024, 0, s>>>(n, nq, slb, ws, wprefix);
         count_launch(ctx);
-        bool done_round = false;
-        for (int attempt = 0; attempt < 2 && !done_round; attempt++) {
-            k_walk_compact<<<nq, kT, 0, s>>>(n, lb, qs, d_q_len, d_q_off, db->d_len, db->d_off, P.cap, cursor, P.pq, P.pt,
-                                             P.aoff, P.alen, P.boff, P.blen, seg_base + (size_t)rounds * nq,
-                                             seg_cnt + (size_t)rounds * nq);
-            count_launch(ctx);
-            int64_t cur = 0;
-            if ((st = read_word(ctx, cursor, &cur)) != GAT_OK) return st;
-            if (cur <= P.cap) {
-                int np = (int)(cur - used);
-                if (np > 0 && (st = edr_launch_soa(ctx, np, nullptr, P.aoff + used, P.alen + used, P.boff + used,
-                                                   P.blen + used, rows_hint, max_cols, d_q_xy, db->d_xy, u,
-                                                   P.dist + used, cells)) != GAT_OK)
-                    return st;
-                used = cur;
-                done_round = true;
-            } else {
-                /* overflow: grow, rewind the cursor, redo the compaction (the walk position only
-                 * advances when a query's chunk fitted) */
-                if ((st = ensure_pairs(ctx, P, cur, used)) != GAT_OK) return st;
-                ctx->h_pinned[2] = used;
-                GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cursor, ctx->h_pinned + 2, 8, cudaMemcpyHostToDevice, s), "top-k");
-            }
-        }
-        if (!done_round) return fail(ctx, GAT_ERR_OOM, "top-k: pair buffer overflow");
-        rounds++;
-        k_kth<<<nq, kT, smem_dh, s>>>(rounds, seg_base, seg_cnt, nq, P.dist, k, bins_d, qs);
+        if ((st = edr_launch_src(ctx, src, rows_hint, max_cols, u, cells)) != GAT_OK) return st;
+        k_walk_kth<<<nq, kT, smem_d, s>>>(n, k, bins_d, growth, slb, cand, sdist, ws);
         count_launch(ctx);
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(pending, 0, 4, s), "top-k");
-        k_walk_check<<<nq, kT, 0, s>>>(n, lb, rounds, seg_base, seg_cnt, nq, P.dist, P.pt, k, qs, pending);
-        count_launch(ctx);
-        int64_t pend = 0;
-        if ((st = read_word(ctx, cursor + 2, &pend)) != GAT_OK) return st;
-        if ((pend & 0xffffffff) == 0) break;
-        chunk = (int)std::min<int64_t>((int64_t)chunk * 2, 1 << 20);
     }
     /* selection */
+    int words = (n + 1 + 31) / 32;
     uint32_t* gbm = nullptr;
     size_t smem_final = (size_t)words * 4;
     if (smem_final > 160 * 1024) {
@@ -780,20 +827,22 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     } else if (smem_final > 32 * 1024) {
         cudaFuncSetAttribute(k_final, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_final);
     }
-    k_final<<<nq, kT, smem_final, s>>>(rounds, seg_base, seg_cnt, nq, P.dist, P.pt, k, words, gbm, qs, d_ids, d_dist);
+    k_final<<<nq, kT, smem_final, s>>>(n, k, words, gbm, cand, sdist, ws, d_ids, d_dist, ctx->d_flag);
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "top-k launch");
-    if ((st = check_device_flag(ctx, "top-k")) != GAT_OK) return st;
     if (stats || ctx->timing) {
+        /* pairs evaluated = sum of the evaluated prefixes */
+        std::vector<int32_t> h((size_t)nq * WS_WORDS);
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), ws, h.size() * 4, cudaMemcpyDeviceToHost, s), "top-k");
         int64_t c = 0;
         if ((st = read_word(ctx, cells, &c)) != GAT_OK) return st;
         timed_add_work(ctx, GAT_KERNEL_EDR, (double)c);
         if (stats) {
-            stats[0] += used;
+            for (int q = 0; q < nq; q++) stats[0] += h[(size_t)q * WS_WORDS + WS_END];
             stats[1] += c;
         }
     }
-    return GAT_OK;
+    return check_device_flag(ctx, "top-k");
 }
 
 int topk_dev(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, const int64_t* d_q_off,
@@ -804,8 +853,9 @@ int topk_dev(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
     int64_t local[4] = {0, 0, 0, 0};
     int st = GAT_OK;
     if (exec == GAT_EXEC_BATCHED) {
-        /* batches bounded so the bound matrix stays below ~4 GiB */
-        int64_t per = std::max<int64_t>(1, ((int64_t)1 << 30) / std::max(1, g->db->n + 1));
+        /* query batches sized so the per-batch candidate arrays stay below ~8 GiB */
+        int bins = std::max(max_q_len, g->db->maxlen) + 2;
+        int64_t per = std::max<int64_t>(1, ((int64_t)8 << 30) / (int64_t)topk_bytes_per_query(g->db->n, bins));
         for (int q0 = 0; q0 < nq && st == GAT_OK; q0 += (int)per) {
             int c = (int)std::min<int64_t>(per, nq - q0);
             st = topk_batch(ctx, g, c, d_q_len + q0, d_q_off + q0, d_q_xy, max_q_len, k, u, d_ids + (size_t)q0 * k,
