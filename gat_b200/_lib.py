@@ -35,6 +35,7 @@ GAT_EXEC_PLAIN, GAT_EXEC_BATCHED = 0, 1
 GAT_LEN_UNIFORM, GAT_LEN_LOGNORMAL, GAT_LEN_LOGUNIFORM = 0, 1, 2
 GAT_SIDE_FIXED, GAT_SIDE_LOGUNIFORM = 0, 1
 GAT_EDR_MAX_LEN = 16384
+GAT_EDR_NOALLOC_MAX_LEN = 4096
 GAT_KERNEL_EDR, GAT_KERNEL_BOUNDS, GAT_KERNEL_RANGE_SCAN = 0, 1, 2
 
 # (name, restype, argtypes) for every symbol of include/gat_b200.h
@@ -61,6 +62,7 @@ SIGNATURES = [
     ("gat_range_query_dev", c_int, [c_p, c_p, c_p, c_int, c_int, c_int, c_p, c_p, c_p, c_i64, P_i64]),
     ("gat_edr_pairs", c_int, [c_p, c_int, P_i32, P_i64, P_f32, c_i64, P_i32, P_i64, P_f32, c_i64, c_d, P_i32]),
     ("gat_edr_pairs_dev", c_int, [c_p, c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_d, c_p]),
+    ("gat_edr_pairs_dev_noalloc", c_int, [c_p, c_int, c_int, c_p, c_p, c_p, c_p, c_p, c_p, c_d, c_p]),
     ("gat_fv_lower_bounds", c_int, [c_p, c_p, c_int, P_i32, P_f32, P_f32, P_i32]),
     ("gat_topk", c_int, [c_p, c_p, c_int, P_i32, P_f32, P_f32, c_int, c_d, c_int, P_i32, P_i32, P_i64]),
     ("gat_topk_dev", c_int, [c_p, c_p, c_int, c_p, c_p, c_p, c_int, c_int, c_d, c_int, c_p, c_p, P_i64]),

@@ -138,6 +138,21 @@ int gat_edr_pairs(gat_ctx* ctx, int npairs, const int32_t* q_len, const int64_t*
 int gat_edr_pairs_dev(gat_ctx* ctx, int npairs, const int32_t* d_q_len, const int64_t* d_q_off,
                       const float* d_q_xy, const int32_t* d_c_len, const int64_t* d_c_off,
                       const float* d_c_xy, double eps, int32_t* d_out);
+/* gat_edr_pairs_dev without any allocation (no counterpart in the reference). For callers that
+ * cannot call cudaMalloc (inside someone else's graph capture, under a no-allocation policy, or
+ * with a fixed device footprint): no context, only the caller's stream and device arrays. The
+ * kernel's working memory is a file-scope device array of fixed size (16.8 MB, held by every GPU
+ * that loads the library until exit), which bounds every trajectory side to
+ * GAT_EDR_NOALLOC_MAX_LEN points: max_len (the longest side the caller passes, host value) above
+ * it returns GAT_ERR_ARG, and a pair whose side exceeds max_len gets -1. The first call on a
+ * device looks the array up (cudaGetSymbolAddress) and should come before any stream capture.
+ * Asynchronous on `stream`; calls that overlap on the GPU share the array and race, so the
+ * caller serialises them. */
+#define GAT_EDR_NOALLOC_MAX_LEN 4096
+int gat_edr_pairs_dev_noalloc(void* stream, int npairs, int max_len, const int32_t* d_q_len,
+                              const int64_t* d_q_off, const float* d_q_xy, const int32_t* d_c_len,
+                              const int64_t* d_c_off, const float* d_c_xy, double eps,
+                              int32_t* d_out);
 
 /* ---------------------------------------------------------------- top-k similarity */
 /* FVTable::formPriorityQueue lower bounds (FVTable.cpp:77-207) of every trajectory of the
