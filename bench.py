@@ -382,26 +382,452 @@ def run_reference_c2(args, world, rank):
     }
 
 
+# ---------------------------------------------------------------- shared GPU harness
+class Harness:
+    """CUDA-event timing on the library's stream, L2 flush between timed steps, clocks."""
+
+    def __init__(self, ctx, dev):
+        import torch
+
+        self.torch = torch
+        self.ctx = ctx
+        self.dev = dev
+        self.stream = torch.cuda.ExternalStream(ctx.stream)
+        self.flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def time(self, fn) -> float:
+        torch = self.torch
+        self.flush_buf.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        fn()
+        e1.record(self.stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+
+def hbm_peak():
+    p = measured_peaks()
+    return float(p.get("hbm_gbs", 6650.0)), ("measured" if "hbm_gbs" in p else "fallback")
+
+
+def range_roofline(st, name):
+    gbs, src = hbm_peak()
+    if st["launches"] == 0 or st["ms"] <= 0:
+        return None
+    per_bytes = st["work"] / st["launches"]
+    per_s = st["ms"] / st["launches"] / 1e3
+    ach = per_bytes / per_s / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": round(ach, 1), "peak": gbs, "unit": "GB/s",
+            "frac": round(ach / gbs, 4), "traffic": None, "work_per_launch": per_bytes,
+            "note": f"algorithmic bytes: 8 B (x, y) per candidate point + 4 B per hit; peak of {src}"}
+
+
+def edr_roofline(st, clk):
+    if st["launches"] == 0 or st["ms"] <= 0:
+        return None
+    per_cells = st["work"] / st["launches"]
+    per_s = st["ms"] / st["launches"] / 1e3
+    ach = per_cells / per_s / 1e9
+    mhz = clk.get("sm_mhz") or 1965.0
+    peak = 148 * 128 * mhz * 1e6 / OPS_PER_CELL / 1e9
+    return {"kernel": "k_edr", "bound": "alu", "achieved": round(ach, 2), "peak": round(peak, 1), "unit": "Gcell/s",
+            "frac": round(ach / peak, 4), "traffic": None, "work_per_launch": per_cells,
+            "note": f"peak = 148 SM x 128 int32 lanes x sampled SM clock / {OPS_PER_CELL} ops per cell (nominal issue rate)"}
+
+
+def base_line(args, world, metric, unit, value, ms_total, config, dtype="fp32-compare/int32"):
+    return {"metric": metric, "value": round(value, 3), "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_total / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded random walks; no dataset)",
+            "config": config}
+
+
+# ---------------------------------------------------------------- workload: config 1
+C1 = dict(n=10_000, nq=1_000, cell=0.01, leaf_cap=512)
+
+
+def run_c1(args, world, rank, local, td):
+    """Plain GT-quadtree range queries: 10k walks, 1k squares of 0.01 deg, leaf cap 512; id sets."""
+    import torch
+
+    import gat_b200 as G
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t, q = D.config1(seed=0, n=C1["n"], nq=C1["nq"])
+    if rank > 0:
+        q = D.boxes(C1["nq"], L.GAT_SIDE_FIXED, 0.01, 0.01, 1000 + rank)
+    ctx = G.Context(local)
+    db = G.TrajectorySet(ctx, t)
+    g = G.Grid(ctx, db, G.BOX, C1["cell"], 2, C1["leaf_cap"])
+    H = Harness(ctx, dev)
+    nq = q.shape[0]
+    cap = nq * 512
+    d_q = torch.from_numpy(q).to(dev)
+    d_off = torch.empty(nq + 1, dtype=torch.int64, device=dev)
+    d_tid = torch.empty(cap, dtype=torch.int32, device=dev)
+    import ctypes as C
+
+    need = C.c_int64(0)
+
+    def call(execution):
+        ctx.check(L.lib.gat_range_query_dev(ctx.h, g.h, d_q.data_ptr(), nq, L.GAT_RESULT_IDS, execution, d_off.data_ptr(),
+                                            d_tid.data_ptr(), None, cap, C.byref(need)), "gat_range_query_dev")
+
+    h_q = torch.from_numpy(q).pin_memory()
+    h_off = torch.empty(nq + 1, dtype=torch.int64).pin_memory()
+    h_tid = torch.empty(cap, dtype=torch.int32).pin_memory()
+
+    def call_e2e(execution):
+        ctx.check(L.lib.gat_range_query(ctx.h, g.h, h_q.data_ptr(), nq, L.GAT_RESULT_IDS, execution,
+                                        h_off.numpy().ctypes.data_as(L.P_i64), h_tid.numpy().ctypes.data_as(L.P_i32), None,
+                                        cap, C.byref(need)), "gat_range_query")
+
+    plain, batched = L.GAT_EXEC_PLAIN, L.GAT_EXEC_BATCHED
+    for _ in range(args.warmup):
+        H.time(lambda: call(plain))
+    ctx.set_timing(True)
+    l0 = ctx.launches
+    clocks = ClockSampler(local)
+    barrier(td, dev)
+    clocks.start()
+    ms = [H.time(lambda: call(plain)) for _ in range(args.steps)]
+    clk = clocks.stop()
+    launches = ctx.launches - l0
+    scan = ctx.kernel_stats(L.GAT_KERNEL_RANGE_SCAN)
+    ctx.set_timing(False)
+    tot = max_over_ranks(td, sum(ms), dev)
+    for _ in range(args.warmup):
+        H.time(lambda: call(batched))
+    ctx.set_timing(True)
+    bms = [H.time(lambda: call(batched)) for _ in range(args.steps)]
+    bscan = ctx.kernel_stats(L.GAT_KERNEL_RANGE_SCAN)
+    ctx.set_timing(False)
+    btot = max_over_ranks(td, sum(bms), dev)
+    for _ in range(args.warmup):
+        H.time(lambda: call_e2e(plain))
+    ems = [H.time(lambda: call_e2e(plain)) for _ in range(args.steps)]
+    etot = max_over_ranks(td, sum(ems), dev)
+    total_ids = int(need.value)
+    if rank != 0:
+        ctx.close()
+        return None
+    line = base_line(args, world, "range queries/s (plain: one query per launch sequence)", "queries/s",
+                     nq * world * args.steps / (tot / 1e3), tot,
+                     {"workload": "C1 plain GT-quadtree range: 10k walks U[20,200], 1k squares 0.01 deg, leaf cap 512, "
+                                  "cell 0.01 deg, trajectory-id sets", "l2": "flushed between steps (256 MiB write)",
+                      "parallelism": f"replicas x{world}"})
+    line.update({
+        "e2e": {"value": round(nq * world * args.steps / (etot / 1e3), 3), "unit": "queries/s",
+                "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int((nq + 1) * 8 + total_ids * 4)},
+        "gpu_launches": int(launches),
+        "batched": {"value": round(nq * world * args.steps / (btot / 1e3), 3), "unit": "queries/s",
+                    "speedup_vs_plain": round(tot / btot, 2), "roofline": range_roofline(bscan, "k_range_ids")},
+        "roofline": range_roofline(scan, "k_range_ids"),
+        "clocks": clk,
+        "result_ids": total_ids,
+    })
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import pyoracle as po
+
+        if po.ref_available():
+            r = po.RefRunner().gtq(t, q, (121.0, 30.7, 122.0, 31.7), C1["cell"], C1["leaf_cap"], layout=False, threads=0)
+            line["cpu_baseline"] = {"value": round(nq / float(r["t_query"][0]), 1), "unit": "queries/s", "cores": 1,
+                                    "kind": "reference", "sample": "all 1k queries, Grid::rangeQueryBatch on one core"}
+    ctx.close()
+    return line
+
+
+def run_reference_c1(args, world, rank):
+    if rank != 0:
+        return None
+    from gat_b200 import data as D
+    from oracle import pyoracle as po
+
+    t, q = D.config1(seed=0, n=C1["n"], nq=C1["nq"])
+    threads = os.cpu_count() or 1
+    times = []
+    R = po.RefRunner()
+    for s in range(args.warmup + args.steps):
+        r = R.gtq(t, q, (121.0, 30.7, 122.0, 31.7), C1["cell"], C1["leaf_cap"], layout=False, threads=threads)
+        if s >= args.warmup:
+            times.append(float(r["t_query"][0]))
+    sec = sum(times)
+    v = len(q) * args.steps / sec
+    line = base_line(args, world, "range queries/s (plain: one query per launch sequence)", "queries/s", v, sec * 1e3,
+                     {"workload": "C1 plain GT-quadtree range: 10k walks U[20,200], 1k squares 0.01 deg, leaf cap 512"})
+    line.update({"impl": "reference",
+                 "cpu_baseline": {"value": round(v, 3), "unit": "queries/s", "cores": threads, "kind": "reference",
+                                  "sample": f"all 1k queries per step, Grid::rangeQueryBatch on {threads} threads (query slices)"},
+                 "e2e": {"value": round(v, 3), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return line
+
+
+# ---------------------------------------------------------------- workload: config 3
+C3 = dict(n=1_000_000, nq=100_000, cell=0.001, leaf_cap=512, stig_block=10240)
+
+
+def run_c3(args, world, rank, local, td):
+    """Batched range queries over the three indexes: 1M walks U[50,350], 100k rectangles with
+    log-uniform sides in [0.001, 0.05] deg; trajectory-id sets."""
+    import ctypes as C
+
+    import torch
+
+    import gat_b200 as G
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    t, q = D.config3(seed=0, n=args.c3_n, nq=C3["nq"])
+    log("c3 data", t.n, len(t.lon), round(time.time() - t0, 1))
+    ctx = G.Context(local)
+    db = G.TrajectorySet(ctx, t)
+    idx = {}
+    t0 = time.time()
+    idx["grid"] = G.Grid(ctx, db, G.BOX, C3["cell"], 2, C3["leaf_cap"])
+    log("grid built", round(time.time() - t0, 1), idx["grid"].info())
+    t0 = time.time()
+    idx["fsg"] = G.FSG(ctx, db, G.BOX, C3["cell"])
+    log("fsg built", round(time.time() - t0, 1))
+    if "stig" in args.c3_indexes:
+        t0 = time.time()
+        idx["stig"] = G.STIG(ctx, db, C3["stig_block"])
+        log("stig built", round(time.time() - t0, 1))
+    H = Harness(ctx, dev)
+    nq = q.shape[0]
+    cap = 64 * 1024 * 1024
+    d_q = torch.from_numpy(q).to(dev)
+    d_off = torch.empty(nq + 1, dtype=torch.int64, device=dev)
+    d_tid = torch.empty(cap, dtype=torch.int32, device=dev)
+    need = C.c_int64(0)
+
+    def call(ix, n=nq, execution=L.GAT_EXEC_BATCHED):
+        ctx.check(L.lib.gat_range_query_dev(ctx.h, ix.h, d_q.data_ptr(), n, L.GAT_RESULT_IDS, execution, d_off.data_ptr(),
+                                            d_tid.data_ptr(), None, cap, C.byref(need)), "gat_range_query_dev")
+
+    res = {}
+    for name, ix in idx.items():
+        for _ in range(args.warmup):
+            H.time(lambda: call(ix))
+        ctx.set_timing(True)
+        l0 = ctx.launches
+        clocks = ClockSampler(local)
+        clocks.start()
+        ms = [H.time(lambda: call(ix)) for _ in range(args.steps)]
+        clk = clocks.stop()
+        st = ctx.kernel_stats(L.GAT_KERNEL_RANGE_SCAN)
+        ctx.set_timing(False)
+        res[name] = dict(ms=max_over_ranks(td, sum(ms), dev), launches=ctx.launches - l0, ids=int(need.value), scan=st, clk=clk)
+        log(name, ms, res[name]["ids"])
+    # plain form on a sample of queries, for the batched-vs-plain ratio
+    ns = min(nq, args.c3_plain_sample)
+    pms = [H.time(lambda: call(idx["grid"], ns, L.GAT_EXEC_PLAIN)) for _ in range(max(1, args.steps // 2))]
+    plain_qps = ns * len(pms) / (sum(pms) / 1e3)
+    # end to end (host buffers) on the Grid
+    h_q = torch.from_numpy(q).pin_memory()
+    h_off = torch.empty(nq + 1, dtype=torch.int64).pin_memory()
+    h_tid = torch.empty(cap, dtype=torch.int32).pin_memory()
+
+    def call_e2e():
+        ctx.check(L.lib.gat_range_query(ctx.h, idx["grid"].h, h_q.data_ptr(), nq, L.GAT_RESULT_IDS, L.GAT_EXEC_BATCHED,
+                                        h_off.numpy().ctypes.data_as(L.P_i64), h_tid.numpy().ctypes.data_as(L.P_i32), None,
+                                        cap, C.byref(need)), "gat_range_query")
+
+    H.time(call_e2e)
+    ems = [H.time(call_e2e) for _ in range(args.steps)]
+    etot = max_over_ranks(td, sum(ems), dev)
+    if rank != 0:
+        ctx.close()
+        return None
+    g = res["grid"]
+    line = base_line(args, world, "range queries/s (batched, GT-quadtree, trajectory-id sets)", "queries/s",
+                     nq * world * args.steps / (g["ms"] / 1e3), g["ms"],
+                     {"workload": f"C3 batched range: {t.n} walks U[50,350] ({len(t.lon)} points), 100k rectangles "
+                                  "log-U[0.001,0.05] deg, cell 0.001 deg, leaf cap 512, STIG block 10240",
+                      "l2": "flushed between steps (256 MiB write); point arrays 3.2 GB per index",
+                      "parallelism": f"replicas x{world}"})
+    line.update({
+        "e2e": {"value": round(nq * world * args.steps / (etot / 1e3), 3), "unit": "queries/s",
+                "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int((nq + 1) * 8 + g["ids"] * 4)},
+        "gpu_launches": int(g["launches"]),
+        "indexes": {k: {"queries_per_s": round(nq * world * args.steps / (v["ms"] / 1e3), 1), "result_ids": v["ids"],
+                        "roofline": range_roofline(v["scan"], "k_range_ids")} for k, v in res.items()},
+        "plain_sample": {"queries": ns, "queries_per_s": round(plain_qps, 1),
+                         "batched_speedup": round(nq * world * args.steps / (g["ms"] / 1e3) / plain_qps, 1)},
+        "roofline": range_roofline(g["scan"], "k_range_ids"),
+        "clocks": g["clk"],
+    })
+    ctx.close()
+    return line
+
+
+# ---------------------------------------------------------------- workload: config 4
+def run_c4(args, world, rank, local, td):
+    """Batched EDR: 4096 pairs, both lengths log-uniform in [16, 4096], eps 5e-4."""
+    import torch
+
+    import gat_b200 as G
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    la, a, lb, b = D.config4_pairs(seed=rank, npairs=4096)
+    n = len(la)
+    cells = float(np.sum(la.astype(np.float64) * lb.astype(np.float64)))
+    ctx = G.Context(local)
+    H = Harness(ctx, dev)
+    oa = np.zeros(n, np.int64)
+    ob = np.zeros(n, np.int64)
+    oa[1:] = np.cumsum(la)[:-1]
+    ob[1:] = np.cumsum(lb)[:-1]
+    T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    d_la, d_oa, d_a, d_lb, d_ob, d_b = T(la.astype(np.int32)), T(oa), T(a), T(lb.astype(np.int32)), T(ob), T(b)
+    d_out = torch.empty(n, dtype=torch.int32, device=dev)
+
+    def call(lo=0, hi=n):
+        ctx.check(L.lib.gat_edr_pairs_dev(ctx.h, hi - lo, d_la.data_ptr() + 4 * lo, d_oa.data_ptr() + 8 * lo, d_a.data_ptr(),
+                                          d_lb.data_ptr() + 4 * lo, d_ob.data_ptr() + 8 * lo, d_b.data_ptr(), 5e-4,
+                                          d_out.data_ptr() + 4 * lo), "gat_edr_pairs_dev")
+
+    for _ in range(args.warmup):
+        H.time(call)
+    ctx.set_timing(True)
+    l0 = ctx.launches
+    clocks = ClockSampler(local)
+    barrier(td, dev)
+    clocks.start()
+    ms = [H.time(call) for _ in range(args.steps)]
+    clk = clocks.stop()
+    st = ctx.kernel_stats(L.GAT_KERNEL_EDR)
+    st["work"] = cells * args.steps
+    ctx.set_timing(False)
+    launches = ctx.launches - l0
+    tot = max_over_ranks(td, sum(ms), dev)
+    # plain: one pair per launch
+    def plain():
+        for i in range(n):
+            call(i, i + 1)
+
+    pms = [H.time(plain) for _ in range(1)]
+    ptot = max_over_ranks(td, sum(pms), dev)
+    # end to end through the host-buffer call
+    import gat_b200.api as A
+
+    ems = []
+    for _ in range(args.steps):
+        t0 = time.time()
+        A.edr_pairs(ctx, la, a, lb, b, 5e-4)
+        ems.append((time.time() - t0) * 1e3)
+    etot = max_over_ranks(td, sum(ems), dev)
+    if rank != 0:
+        ctx.close()
+        return None
+    g = cells * world * args.steps / (tot / 1e3) / 1e9
+    line = base_line(args, world, "EDR GCUPS (batched pairs)", "GCUPS", g, tot,
+                     {"workload": "C4 batched EDR: 4096 pairs, lengths log-U[16,4096] both sides, eps 5e-4 deg, "
+                                  f"{cells:.3g} DP cells per step", "l2": "flushed between steps (256 MiB write)",
+                      "parallelism": f"replicas x{world}"}, dtype="int32")
+    line.update({
+        "e2e": {"value": round(cells * world * args.steps / (etot / 1e3) / 1e9, 3), "unit": "GCUPS",
+                "h2d_bytes_per_step": int(a.nbytes + b.nbytes + 24 * n), "d2h_bytes_per_step": int(4 * n),
+                "timer": "host wall clock around gat_edr_pairs (synchronous call)"},
+        "gpu_launches": int(launches),
+        "plain": {"value": round(cells * world / (ptot / 1e3) / 1e9, 3), "unit": "GCUPS", "note": "one pair per launch",
+                  "batched_speedup": round(ptot / (tot / args.steps), 2)},
+        "roofline": edr_roofline(st, clk),
+        "clocks": clk,
+    })
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import pyoracle as po
+
+        idx = np.arange(0, n, 64)
+        sa = np.concatenate([a[oa[i]:oa[i] + la[i]] for i in idx])
+        sb = np.concatenate([b[ob[i]:ob[i] + lb[i]] for i in idx])
+        sc = float(np.sum(la[idx].astype(np.float64) * lb[idx]))
+        thr = os.cpu_count() or 1
+        if po.ref_available():
+            r = po.RefRunner().edr(la[idx], sa, lb[idx], sb, 5e-4, threads=thr)
+            line["cpu_baseline"] = {"value": round(sc / float(r["t_query"][0]) / 1e9, 4), "unit": "GCUPS", "cores": thr,
+                                    "kind": "reference", "sample": f"{len(idx)} of the 4096 pairs, Grid::SimilarityExecuter"}
+    ctx.close()
+    return line
+
+
+def run_reference_c4(args, world, rank):
+    if rank != 0:
+        return None
+    from gat_b200 import data as D
+    from oracle import pyoracle as po
+
+    la, a, lb, b = D.config4_pairs(seed=0, npairs=4096)
+    n = len(la)
+    oa = np.zeros(n, np.int64)
+    ob = np.zeros(n, np.int64)
+    oa[1:] = np.cumsum(la)[:-1]
+    ob[1:] = np.cumsum(lb)[:-1]
+    idx = np.arange(0, n, 32)
+    sa = np.concatenate([a[oa[i]:oa[i] + la[i]] for i in idx])
+    sb = np.concatenate([b[ob[i]:ob[i] + lb[i]] for i in idx])
+    sc = float(np.sum(la[idx].astype(np.float64) * lb[idx]))
+    thr = os.cpu_count() or 1
+    R = po.RefRunner()
+    times = []
+    for s in range(args.warmup + args.steps):
+        r = R.edr(la[idx], sa, lb[idx], sb, 5e-4, threads=thr)
+        if s >= args.warmup:
+            times.append(float(r["t_query"][0]))
+    sec = sum(times)
+    v = sc * args.steps / sec / 1e9
+    line = base_line(args, world, "EDR GCUPS (batched pairs)", "GCUPS", v, sec * 1e3,
+                     {"workload": "C4 batched EDR: 4096 pairs log-U[16,4096] (every 32nd pair per step)"}, dtype="int32")
+    line.update({"impl": "reference",
+                 "cpu_baseline": {"value": round(v, 4), "unit": "GCUPS", "cores": thr, "kind": "reference",
+                                  "sample": f"{len(idx)} of 4096 pairs per step, Grid::SimilarityExecuter on {thr} threads"},
+                 "e2e": {"value": round(v, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return line
+
+
+WORKLOADS = {"c1": run_c1, "c2": None, "c3": run_c3, "c4": run_c4}
+REFERENCE = {"c1": run_reference_c1, "c2": None, "c4": run_reference_c4}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2"])
-    ap.add_argument("--cpu-sample", type=int, default=32)
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--cpu-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--c3-indexes", default="grid,fsg,stig")
+    ap.add_argument("--c3-n", type=int, default=C3["n"])
+    ap.add_argument("--c3-plain-sample", type=int, default=2000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_env()
     if args.impl == "reference":
-        line = run_reference_c2(args, world, rank)
+        fn = REFERENCE.get(args.workload) or run_reference_c2
+        if args.workload == "c3":
+            line = {"impl": "reference", "unavailable": "the reference's Grid build is O(trajectories x cells) in memset "
+                    "(Grid.cpp:268-269); at 1M trajectories and 1M cells it does not finish in minutes"}
+        else:
+            line = fn(args, world, rank)
         if line is not None:
             print(json.dumps(line), flush=True)
         return
     td = init_dist(world)
     try:
-        line = run_c2(args, world, rank, local, td)
+        fn = WORKLOADS.get(args.workload) or run_c2
+        line = fn(args, world, rank, local, td)
         if line is not None:
             print(json.dumps(line), flush=True)
     finally:

@@ -6,41 +6,16 @@
 #include "internal.h"
 
 namespace gat {
-using edr::kWarps;
 using edr::SoaPairs;
-using edr::k_edr;
 
-/* Launch over pairs given as (a_off, a_len, b_off, b_len) arrays. max_cols bounds the longer
- * side of every pair (sizes the carry rows); rows_hint picks the tile height. */
+/* Launch over pairs given as (a_off, a_len, b_off, b_len) arrays. max_rows / max_cols bound
+ * the shorter / longer side of every pair. */
 int edr_launch_soa(gat_ctx* ctx, int npairs, const int* d_npairs, const int64_t* a_off, const int32_t* a_len,
-                   const int64_t* b_off, const int32_t* b_len, int rows_hint, int max_cols, const float2* A,
+                   const int64_t* b_off, const int32_t* b_len, int max_rows, int max_cols, const float2* A,
                    const float2* B, float u, int32_t* d_out, unsigned long long* d_cells) {
-    if (npairs <= 0 && !d_npairs) return GAT_OK;
-    int st = GAT_OK;
-    const int R = rows_hint <= 128 ? 4 : 8;
-    int per_sm = 0;
-    if (R == 4)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr<4, SoaPairs>, kWarps * 32, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr<8, SoaPairs>, kWarps * 32, 0);
-    per_sm = std::max(1, per_sm);
-    int grid = ctx->sm_count * per_sm;
-    if (!d_npairs) grid = std::max(1, std::min(grid, (npairs + kWarps - 1) / kWarps));
-    int stride = max_cols + 2;
-    int* carry = (int*)scratch(ctx, S_EDR_CARRY, (size_t)grid * kWarps * 2 * stride * sizeof(int), &st);
-    unsigned* work = (unsigned*)scratch(ctx, S_EDR_COUNTERS, 64, &st);
-    if (!carry || !work) return st;
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(work, 0, sizeof(unsigned), ctx->stream), "edr");
-    timed_begin(ctx, GAT_KERNEL_EDR);
+    if (npairs <= 0) return GAT_OK;
     SoaPairs src{npairs, d_npairs, a_off, a_len, b_off, b_len, A, B, d_out};
-    if (R == 4)
-        k_edr<4><<<grid, kWarps * 32, 0, ctx->stream>>>(src, u, carry, stride, work, d_cells);
-    else
-        k_edr<8><<<grid, kWarps * 32, 0, ctx->stream>>>(src, u, carry, stride, work, d_cells);
-    timed_end(ctx, GAT_KERNEL_EDR, 0.0);
-    count_launch(ctx);
-    GAT_CUDA_TRY(ctx, cudaGetLastError(), "edr launch");
-    return GAT_OK;
+    return edr::edr_launch(ctx, src, npairs, max_rows, max_cols, u, d_cells);
 }
 
 }  // namespace gat
@@ -104,6 +79,7 @@ int gat_edr_pairs(gat_ctx* ctx, int npairs, const int32_t* q_len, const int64_t*
     if ((st = edr_launch_soa(ctx, npairs, nullptr, d_aoff, d_alen, d_boff, d_blen, mr, mc, d_a, d_b,
                              match_threshold(eps), d_out, nullptr)) != GAT_OK)
         return st;
+    if ((st = check_device_flag(ctx, "edr")) != GAT_OK) return st;
     double cells = 0;
     for (int i = 0; i < npairs; i++) cells += (double)q_len[i] * (double)c_len[i];
     timed_add_work(ctx, GAT_KERNEL_EDR, cells);
@@ -125,8 +101,7 @@ int gat_edr_pairs_dev(gat_ctx* ctx, int npairs, const int32_t* d_q_len, const in
     int st = edr_launch_soa(ctx, npairs, nullptr, d_q_off, d_q_len, d_c_off, d_c_len, GAT_EDR_MAX_LEN, GAT_EDR_MAX_LEN,
                             (const float2*)d_q_xy, (const float2*)d_c_xy, match_threshold(eps), d_out, nullptr);
     if (st != GAT_OK) return st;
-    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "edr");
-    return GAT_OK;
+    return check_device_flag(ctx, "edr");
 }
 
 }  // extern "C"

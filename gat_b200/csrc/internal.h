@@ -187,6 +187,9 @@ enum Slot {
     S_EDR_CARRY,
     S_EDR_COUNTERS,
     S_EDR_IO,
+    S_EDR_ITEMS,
+    S_EDR_PROG,
+    S_EDR_PCARRY,
     S_TOPK_QFV,
     S_TOPK_LB,
     S_TOPK_PAIRS,

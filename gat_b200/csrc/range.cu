@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
                                                         const int2* items, const float* X, const float* Y,
                                                         const int32_t* tid, int words, uint32_t* gbitmap,
                                                         uint32_t* arena, int64_t cap, unsigned long long* cursor,
-                                                        int64_t* segbase, int64_t* segcnt) {
+                                                        int64_t* segbase, int64_t* segcnt, unsigned long long* work) {
     extern __shared__ uint32_t smem_bm[];
     __shared__ int sh[kThreads / 32 + 1];
     __shared__ unsigned long long base_sh;
@@ -236,12 +236,20 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
         for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
         __syncthreads();
         Box q = load_box(queries, qi);
+        unsigned long long cand = 0, hits = 0;
         for (int64_t it = ioff[qi]; it < ioff[qi + 1]; it++) {
             int2 r = items[it];
+            cand += (unsigned long long)(r.y - r.x);
             scan_range(X, Y, r.x, r.y, q, [&](int i) {
                 int t = __ldg(tid + i);
                 atomicOr(&bm[t >> 5], 1u << (t & 31));
+                hits++;
             });
+        }
+        /* algorithmic bytes: x and y of every candidate point, the id of every hit */
+        if (work) {
+            if (threadIdx.x == 0) atomicAdd(work, 8ull * cand);
+            if (hits) atomicAdd(work, 4ull * hits);
         }
         __syncthreads();
         int w0 = threadIdx.x * per, w1 = min(words, w0 + per);
@@ -489,11 +497,12 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         uint32_t* arena = (uint32_t*)scratch(ctx, S_RANGE_ARENA, (size_t)cap * 4, &st);
         if (!arena) return st;
         cap = (int64_t)(ctx->slot_bytes[S_RANGE_ARENA] / 4);
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s), "range");
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 2 * sizeof(unsigned long long), s), "range");
         timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
         if (mode == GAT_RESULT_IDS)
             k_range_ids<<<grid, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid,
-                                                                       words, gbm, arena, cap, cursor, segbase, segcnt);
+                                                                       words, gbm, arena, cap, cursor, segbase, segcnt,
+                                                                       ctx->timing ? cursor + 1 : nullptr);
         else
             k_range_points<<<grid, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits, arena,
                                                      cap, cursor, segbase, segcnt);
@@ -503,7 +512,14 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
         GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
         int64_t used = ctx->h_pinned[0];
-        if (used <= cap) break;
+        if (used <= cap) {
+            if (ctx->timing) {
+                GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 3, cursor + 1, 8, cudaMemcpyDeviceToHost, s), "range");
+                GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
+                timed_add_work(ctx, GAT_KERNEL_RANGE_SCAN, (double)ctx->h_pinned[3]);
+            }
+            break;
+        }
         if (attempt == 1) return fail(ctx, GAT_ERR_OOM, "range: result arena overflow");
         cap = used;
     }

@@ -528,7 +528,7 @@ struct WalkPairs {
  * and k evaluated pairs already sort before (W, nid). While nlb < W the walk goes on: a
  * candidate with a smaller bound may still be closer. */
 __global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* slb, const int32_t* cand,
-                           const int32_t* sdist, int32_t* ws) {
+                           const int32_t* sdist, int32_t* ws, int* pending) {
     extern __shared__ int hist[];
     __shared__ int sh_W, cnt;
     int qi = blockIdx.x;
@@ -580,6 +580,7 @@ __global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* sl
         s[WS_W] = W;
         s[WS_DONE] = done ? 1 : 0;
         s[WS_CHUNK] = (int)min((long long)growth * s[WS_CHUNK], 1LL << 30);
+        if (!done) atomicAdd(pending, 1);
     }
 }
 
@@ -680,35 +681,6 @@ __global__ void k_final(int n, int k, int words, uint32_t* gbitmap, const int32_
     }
 }
 
-/* persistent EDR launch over a device-counted pair source */
-template <class Src>
-int edr_launch_src(gat_ctx* ctx, const Src& src, int rows_hint, int max_cols, float u, unsigned long long* cells) {
-    using edr::k_edr;
-    using edr::kWarps;
-    int st = GAT_OK;
-    const int R = rows_hint <= 128 ? 4 : 8;
-    int per_sm = 0;
-    if (R == 4)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr<4, Src>, kWarps * 32, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr<8, Src>, kWarps * 32, 0);
-    int grid = ctx->sm_count * std::max(1, per_sm);
-    int stride = max_cols + 2;
-    int* carry = (int*)scratch(ctx, S_EDR_CARRY, (size_t)grid * kWarps * 2 * stride * sizeof(int), &st);
-    unsigned* work = (unsigned*)scratch(ctx, S_EDR_COUNTERS, 64, &st);
-    if (!carry || !work) return st;
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(work, 0, sizeof(unsigned), ctx->stream), "edr");
-    timed_begin(ctx, GAT_KERNEL_EDR);
-    if (R == 4)
-        k_edr<4, Src><<<grid, kWarps * 32, 0, ctx->stream>>>(src, u, carry, stride, work, cells);
-    else
-        k_edr<8, Src><<<grid, kWarps * 32, 0, ctx->stream>>>(src, u, carry, stride, work, cells);
-    timed_end(ctx, GAT_KERNEL_EDR, 0.0);
-    count_launch(ctx);
-    GAT_CUDA_TRY(ctx, cudaGetLastError(), "edr launch");
-    return GAT_OK;
-}
-
 int read_word(gat_ctx* ctx, const void* d, int64_t* v) {
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, d, 8, cudaMemcpyDeviceToHost, ctx->stream), "top-k");
     GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "top-k");
@@ -787,8 +759,8 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     if (smem_run > 48 * 1024) cudaFuncSetAttribute(k_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_run);
     k_sort_scatter<<<dim3(ntile, nq), 32, smem_run, s>>>(n, lb, bins_lb, ntile, H, cand, slb);
     count_launch(ctx);
-    /* the walk: rounds need no host round trip; a finished query costs nothing in later
-     * rounds, and `rounds` covers the whole order with doubling chunks */
+    /* the walk: a finished query costs nothing in later rounds, `rounds` covers the whole
+     * order with growing chunks, and the loop ends early once no query is pending */
     /* a lone query leaves most of the GPU idle in a small round, so it starts with a larger
      * chunk and grows faster; a batch keeps rounds tight to limit surplus evaluations */
     const bool lone = nq <= 4;
@@ -809,12 +781,22 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     int rows_hint = std::min(max_q_len, db->maxlen);
     int max_cols = std::max(max_q_len, db->maxlen);
     WalkPairs src{n, nq, wprefix, ws, cand, d_q_len, d_q_off, d_q_xy, db->d_len, db->d_off, db->d_xy, sdist};
+    int64_t chunk_r = chunk0;
     for (int r = 0; r < rounds; r++) {
         k_walk_plan<<<1, 1024, 0, s>>>(n, nq, slb, ws, wprefix);
         count_launch(ctx);
-        if ((st = edr_launch_src(ctx, src, rows_hint, max_cols, u, cells)) != GAT_OK) return st;
-        k_walk_kth<<<nq, kT, smem_d, s>>>(n, k, bins_d, growth, slb, cand, sdist, ws);
+        /* upper bound of this round's pairs: every query extends by at most its chunk */
+        int64_t cap = std::min<int64_t>((int64_t)nq * chunk_r, (int64_t)nq * n);
+        if ((st = edr::edr_launch(ctx, src, cap, rows_hint, max_cols, u, cells)) != GAT_OK) return st;
+        chunk_r = std::min<int64_t>(chunk_r * growth, (int64_t)1 << 30);
+        int* pending = reinterpret_cast<int*>(cells + 1);
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(pending, 0, sizeof(int), s), "top-k");
+        k_walk_kth<<<nq, kT, smem_d, s>>>(n, k, bins_d, growth, slb, cand, sdist, ws, pending);
         count_launch(ctx);
+        /* stop as soon as every query is done: one small read per round */
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 4, pending, sizeof(int), cudaMemcpyDeviceToHost, s), "top-k");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "top-k");
+        if ((int)(ctx->h_pinned[4] & 0xffffffff) == 0) break;
     }
     /* selection */
     int words = (n + 1 + 31) / 32;
