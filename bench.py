@@ -155,6 +155,9 @@ def run_c2(args, world, rank, local, td):
         from gat_b200 import data as D
 
         qids = D.sample_ids(C2["nq"], C2["n"], 1000 + rank)
+    if args.queries:
+        # a prefix of the query sample, for launch-list captures under a profiler
+        qids = qids[:args.queries]
     ctx = G.Context(local)
     db = G.TrajectorySet(ctx, t)
     g = G.Grid(ctx, db, G.BOX, C2["cell"], C2["vparam"], C2["leaf_cap"])
@@ -273,7 +276,7 @@ def run_c2(args, world, rank, local, td):
         "vs_baseline": None,
         "dtype": "int32",
         "data": "synthetic (seeded random walks; no dataset)",
-        "config": {"workload": "C2 plain EDR top-k: 100k trajectories, lognormal(ln200,0.6) lengths 32..1024, 256 queries "
+        "config": {"workload": f"C2 plain EDR top-k: 100k trajectories, lognormal(ln200,0.6) lengths 32..1024, {nq} queries "
                                "from the set, k=32, eps=5e-4 deg, FV grid 256x256 (cell 0.0025, shift 2), one query per launch",
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
         "e2e": {"value": round(nqs / (ems_max / 1e3), 2), "unit": "queries/s",
@@ -679,7 +682,7 @@ def run_c4(args, world, rank, local, td):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    la, a, lb, b = D.config4_pairs(seed=rank, npairs=4096)
+    la, a, lb, b = D.config4_pairs(seed=rank, npairs=args.pairs)
     n = len(la)
     cells = float(np.sum(la.astype(np.float64) * lb.astype(np.float64)))
     ctx = G.Context(local)
@@ -732,7 +735,7 @@ def run_c4(args, world, rank, local, td):
         return None
     g = cells * world * args.steps / (tot / 1e3) / 1e9
     line = base_line(args, world, "EDR GCUPS (batched pairs)", "GCUPS", g, tot,
-                     {"workload": "C4 batched EDR: 4096 pairs, lengths log-U[16,4096] both sides, eps 5e-4 deg, "
+                     {"workload": f"C4 batched EDR: {n} pairs, lengths log-U[16,4096] both sides, eps 5e-4 deg, "
                                   f"{cells:.3g} DP cells per step", "l2": "flushed between steps (256 MiB write)",
                       "parallelism": f"replicas x{world}"}, dtype="int32")
     line.update({
@@ -756,7 +759,7 @@ def run_c4(args, world, rank, local, td):
         if po.ref_available():
             r = po.RefRunner().edr(la[idx], sa, lb[idx], sb, 5e-4, threads=thr)
             line["cpu_baseline"] = {"value": round(sc / float(r["t_query"][0]) / 1e9, 4), "unit": "GCUPS", "cores": thr,
-                                    "kind": "reference", "sample": f"{len(idx)} of the 4096 pairs, Grid::SimilarityExecuter"}
+                                    "kind": "reference", "sample": f"{len(idx)} of the {n} pairs, Grid::SimilarityExecuter"}
     ctx.close()
     return line
 
@@ -808,6 +811,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--cpu-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--queries", type=int, default=0, help="C2: use only the first N of the 256 queries")
+    ap.add_argument("--pairs", type=int, default=4096, help="C4: pairs per launch")
     ap.add_argument("--c3-indexes", default="grid,fsg,stig")
     ap.add_argument("--c3-n", type=int, default=C3["n"])
     ap.add_argument("--c3-plain-sample", type=int, default=2000)
