@@ -37,6 +37,7 @@ GAT_SIDE_FIXED, GAT_SIDE_LOGUNIFORM = 0, 1
 GAT_EDR_MAX_LEN = 16384
 GAT_EDR_NOALLOC_MAX_LEN = 4096
 GAT_KERNEL_EDR, GAT_KERNEL_BOUNDS, GAT_KERNEL_RANGE_SCAN = 0, 1, 2
+GAT_TUNE_EDR_ROWS, GAT_TUNE_EDR_TUNED = 1, 2
 
 # (name, restype, argtypes) for every symbol of include/gat_b200.h
 SIGNATURES = [
@@ -49,6 +50,8 @@ SIGNATURES = [
     ("gat_ctx_scratch_bytes", c_i64, [c_p]),
     ("gat_ctx_set_timing", c_int, [c_p, c_int]),
     ("gat_ctx_kernel_stats", c_int, [c_p, c_int, C.POINTER(c_d), P_i64, C.POINTER(c_d)]),
+    ("gat_ctx_set_tuning", c_int, [c_p, c_int, c_int]),
+    ("gat_ctx_get_tuning", c_int, [c_p, c_int, P_i32]),
     ("gat_db_create", c_int, [c_p, c_int, P_i32, P_f32, P_f32, C.POINTER(c_p)]),
     ("gat_db_destroy", None, [c_p]),
     ("gat_db_info", c_int, [c_p, P_i64]),

@@ -77,6 +77,15 @@ class Context:
         self.check(lib.gat_ctx_kernel_stats(self.h, cls, C.byref(ms), C.byref(n), C.byref(w)), "gat_ctx_kernel_stats")
         return dict(ms=ms.value, launches=int(n.value), work=w.value)
 
+    def set_edr_rows(self, rows: int) -> None:
+        """Rows per lane of the EDR wavefront: 0 = autotune (default), 2, 4 or 8."""
+        self.check(lib.gat_ctx_set_tuning(self.h, L.GAT_TUNE_EDR_ROWS, int(rows)), "gat_ctx_set_tuning")
+
+    def tuning(self, knob: int) -> int:
+        v = C.c_int32(0)
+        self.check(lib.gat_ctx_get_tuning(self.h, knob, C.byref(v)), "gat_ctx_get_tuning")
+        return int(v.value)
+
     @property
     def scratch_bytes(self) -> int:
         return int(lib.gat_ctx_scratch_bytes(self.h))

@@ -41,6 +41,20 @@ void* scratch(gat_ctx* ctx, int slot, size_t bytes, int* status) {
     }
     ctx->slot_ptr[slot] = p;
     ctx->slot_bytes[slot] = grow;
+    ctx->slot_fresh[slot] = 1;
+    return p;
+}
+
+void* scratch_zeroed(gat_ctx* ctx, int slot, size_t bytes, int* status) {
+    void* p = scratch(ctx, slot, bytes, status);
+    if (p && ctx->slot_fresh[slot]) {
+        cudaError_t e = cudaMemsetAsync(p, 0, ctx->slot_bytes[slot], ctx->stream);
+        if (e != cudaSuccess) {
+            *status = cuda_fail(ctx, e, "scratch clear");
+            return nullptr;
+        }
+        ctx->slot_fresh[slot] = 0;
+    }
     return p;
 }
 
@@ -136,6 +150,7 @@ int gat_ctx_create(int device, gat_ctx** out) {
         c->device = -1;
         c->slot_ptr.assign(S_COUNT, nullptr);
         c->slot_bytes.assign(S_COUNT, 0);
+    c->slot_fresh.assign(S_COUNT, 0);
         *out = c;
         return GAT_OK;
     }
@@ -149,11 +164,12 @@ int gat_ctx_create(int device, gat_ctx** out) {
     c->device = device;
     c->slot_ptr.assign(S_COUNT, nullptr);
     c->slot_bytes.assign(S_COUNT, 0);
+    c->slot_fresh.assign(S_COUNT, 0);
     if ((e = cudaSetDevice(device)) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaMalloc(&c->d_flag, sizeof(int32_t))) != cudaSuccess ||
-        (e = cudaMemset(c->d_flag, 0, sizeof(int32_t))) != cudaSuccess ||
+        (e = cudaMalloc(&c->d_flag, 16 * sizeof(int32_t))) != cudaSuccess ||
+        (e = cudaMemset(c->d_flag, 0, 16 * sizeof(int32_t))) != cudaSuccess ||
         (e = cudaMallocHost(&c->h_pinned, 64 * sizeof(int64_t))) != cudaSuccess) {
         cudaGetLastError();
         gat_ctx_destroy(c);
@@ -217,6 +233,29 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int cls, double* ms, int64_t* launches, d
     if (ms) *ms = ctx->t_ms[cls];
     if (launches) *launches = ctx->t_launches[cls];
     if (work) *work = ctx->t_work[cls];
+    return GAT_OK;
+}
+
+int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
+    if (!ctx) return GAT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (knob != GAT_TUNE_EDR_ROWS) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: unknown knob");
+    if (value != 0 && value != 2 && value != 4 && value != 8)
+        return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR rows per lane must be 0 (autotune), 2, 4 or 8");
+    ctx->edr_rows = value;
+    ctx->edr_tune.clear();
+    return GAT_OK;
+}
+
+int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
+    if (!ctx || !value) return GAT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (knob == GAT_TUNE_EDR_ROWS)
+        *value = ctx->edr_rows;
+    else if (knob == GAT_TUNE_EDR_TUNED)
+        *value = (int)ctx->edr_tune.size();
+    else
+        return fail(ctx, GAT_ERR_ARG, "gat_ctx_get_tuning: unknown knob");
     return GAT_OK;
 }
 

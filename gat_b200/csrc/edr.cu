@@ -14,7 +14,7 @@ int edr_launch_soa(gat_ctx* ctx, int npairs, const int* d_npairs, const int64_t*
                    const int64_t* b_off, const int32_t* b_len, int max_rows, int max_cols, const float2* A,
                    const float2* B, float u, int32_t* d_out, unsigned long long* d_cells) {
     if (npairs <= 0) return GAT_OK;
-    SoaPairs src{npairs, d_npairs, a_off, a_len, b_off, b_len, A, B, d_out};
+    SoaPairs src{npairs, d_npairs, a_off, a_len, b_off, b_len, A, B, d_out, std::max(max_rows, max_cols), ctx->d_flag};
     return edr::edr_launch(ctx, src, npairs, max_rows, max_cols, u, d_cells);
 }
 

@@ -9,13 +9,16 @@
  * not below eps, which is the same predicate. Orientation: rows are the query when the
  * candidate is at least as long, else the candidate (Grid.cpp:1234-1247).
  *
- * Mapping: one warp per pair (persistent, pairs taken from an atomic counter). Lane L owns R
- * consecutive rows of a 32*R-row tile and handles column j = s - L at step s, so a step
- * advances 32*R cells of one anti-diagonal band. The value below a lane's last row moves to
- * the next lane with one shuffle per step; columns are staged 32 at a time in a per-warp
- * shared-memory ring that every lane reads; tiles of 32*R rows run one after another and
- * hand their bottom row to the next tile through a double-buffered carry row in global
- * memory (L2-resident). Everything is int32 arithmetic plus two float subtractions per cell.
+ * Mapping: a warp works on row tiles of 32*R rows. Lane L owns R consecutive rows of the tile
+ * and handles column j = s - L at step s, so a step advances 32*R cells of one anti-diagonal
+ * band. The value below a lane's last row moves to the next lane with one shuffle per step;
+ * columns are staged 32 at a time in per-warp shared memory that every lane reads; a tile hands
+ * its bottom row to the next tile through a carry row in global memory (L2-resident).
+ * Everything is int32 arithmetic plus two float subtractions and two compares per cell.
+ *
+ * Two kernels: k_edr (one warp per pair, its tiles in sequence; used by the allocation-free
+ * entry point) and k_edr_tiles (row tiles as work items, longest pairs first, consecutive
+ * tiles of a pair pipelined across warps; every other caller).
  */
 #pragma once
 #include <algorithm>
@@ -28,7 +31,9 @@ namespace edr {
 constexpr int kWarps = 8;
 constexpr int kBig = 1 << 29; /* above any distance; up + 1 never overflows against it */
 
-/* Pair source over (a_off, a_len, b_off, b_len) arrays; results to out[p]. */
+/* Pair source over (a_off, a_len, b_off, b_len) arrays; results to out[p]. A pair with a side
+ * outside 1..lim gets -1, raises GAT_ERR_ARG in the status word and runs as an empty problem
+ * whose result goes to the sink word (flag + 1). */
 struct SoaPairs {
     int npairs;
     const int* d_npairs;
@@ -39,12 +44,24 @@ struct SoaPairs {
     const float2* A;
     const float2* B;
     int32_t* out;
+    int lim;
+    int32_t* flag;
+    static constexpr int kKind = 0;
     __device__ int count() const { return d_npairs ? *d_npairs : npairs; }
     __device__ void get(int p, const float2*& a, int& la, const float2*& b, int& lb, int32_t*& o) const {
-        a = A + a_off[p];
         la = a_len[p];
-        b = B + b_off[p];
         lb = b_len[p];
+        if (la < 1 || lb < 1 || la > lim || lb > lim) {
+            out[p] = -1;
+            atomicCAS(flag, 0, GAT_ERR_ARG);
+            a = A;
+            b = B;
+            la = lb = 0;
+            o = flag + 1;
+            return;
+        }
+        a = A + a_off[p];
+        b = B + b_off[p];
         o = out + p;
     }
 };
@@ -176,178 +193,317 @@ __global__ void __launch_bounds__(kWarps * 32) k_edr(Src src, float u, int* __re
 /* ================================================================ tiled, load-balanced form
  * Work items are row tiles. A pair whose rows span T >= 2 tiles contributes T items and its
  * tiles run on different warps, pipelined: tile t consumes the bottom row of tile t-1 through a
- * carry row in L2 as tile t-1 publishes it, 32 columns at a time (release/acquire on a
- * per-tile progress word). Pairs with one tile, and pairs beyond the cooperative pool, are one
- * item that a single warp walks tile by tile with its own carry rows. Waits are bounded:
- * after kSpinLimit polls the warp raises GAT_ERR_TIMEOUT in the status word and abandons the
- * pair (its result becomes -1). Every warp of the persistent grid is resident and items are
- * taken in increasing order, so the producer of any tile a warp waits for is already running. */
+ * carry row in L2 while tile t-1 is still producing it. Pairs with one tile, and multi-tile
+ * pairs beyond the cooperative pool, are one item that a single warp walks tile by tile with
+ * its own carry rows.
+ *
+ * Carry words: each column's carry value is one 64-bit word, tag << 16 | (uint16) value, with
+ * tag = launch epoch << 8 | producing tile (mod 256). The consumer polls the words it needs and
+ * accepts a word whose tag is the one it expects, so the hand-over needs neither a progress
+ * flag nor a memory fence: a 64-bit store is seen whole or not at all. Values are the
+ * column-shifted distances E = D - c, which lie in [-16384, 16384] and fit 16 bits; epochs
+ * only grow (2^40 launches before a repeat), and carry buffers are zeroed when allocated, so a
+ * stale word never carries the expected tag. A tile rewrites the buffer its predecessor read
+ * (double buffering per pair) only for columns that predecessor has already consumed.
+ *
+ * Schedule (longest first): a count pass puts every pair in one of kClasses duration classes
+ * (half-octaves of the pair's critical path in column steps: len2 + 32 (T - 1) when its tiles
+ * are pipelined, T (len2 + 31) on one warp) and a write pass lays the items out class by
+ * class, longest class first, a pair's tiles consecutive. Warps take items in that order from
+ * one counter, so the long pairs start first and the short ones fill in behind them.
+ *
+ * Waits are bounded: after kSpinLimit polls the warp raises GAT_ERR_TIMEOUT in the status word
+ * and abandons the pair (its result becomes -1). The producer of the tile a warp waits for
+ * took the preceding item from the same counter, so it is already running. */
 constexpr int kSpinLimit = 1 << 22;
+constexpr int kClasses = 48;
+/* counter block: [0] item counter, [1] cooperative slots taken, [2] total items,
+ * [4, 4 + kClasses) items per class, [4 + kClasses, 4 + 2 kClasses) class cursors */
+constexpr int kCtrWords = 4 + 2 * kClasses;
+typedef unsigned long long carry_t;
 
 struct TileCtl {
-    const int64_t* item_pre; /* exclusive prefix of items per pair, item_pre[count] = total */
-    int* prog;               /* progress word per cooperative item (zeroed per launch) */
-    int* pair_carry;         /* cooperative pair p: rows pair_carry + p * 2 * stride */
-    int coop_cap;            /* pairs with index >= coop_cap run on one warp */
-    int* warp_carry;         /* per-warp double carry rows for single-warp pairs */
+    const int4* items; /* (pair, tile or -1 for a whole pair on one warp, cooperative slot, tiles) */
+    const int* total;
+    carry_t* pair_carry; /* cooperative slot s: rows pair_carry + s * 2 * stride */
+    carry_t* warp_carry; /* per-warp double carry rows for single-warp pairs */
     int stride;
+    unsigned long long epoch;
     int32_t* flag;
 };
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+/* The carry word is the only datum exchanged, so neither access needs to order other memory
+ * operations (no "memory" clobber: the step loop's shared-memory loads may move across them);
+ * volatile keeps every poll a fresh load. */
+__device__ __forceinline__ carry_t ld_carry(const carry_t* p) {
+    carry_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
     return v;
 }
-__device__ __forceinline__ void st_release(int* p, int v) {
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_carry(carry_t* p, carry_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v));
+}
+
+/* floor(2 log2(d)) for d >= 1, clamped to the class range */
+__device__ __forceinline__ int duration_class(long long d) {
+    if (d < 1) d = 1;
+    const int e = 63 - __clzll(d);
+    const int half = (d * d >= (1LL << (2 * e + 1))) ? 1 : 0;
+    return min(2 * e + half, kClasses - 1);
 }
 
 template <int R, class Src>
-__global__ void k_edr_prep(Src src, int cap, int coop_cap, int64_t* items) {
-    const int n = src.count();
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < cap; p += gridDim.x * blockDim.x) {
-        int64_t it = 0;
-        if (p < n) {
-            const float2 *a, *b;
-            int la, lb;
-            int32_t* o;
-            src.get(p, a, la, b, lb, o);
-            int len1 = min(la, lb);
-            int T = len1 <= 0 ? 1 : (len1 + 32 * R - 1) / (32 * R);
-            it = (T >= 2 && p < coop_cap) ? T : 1;
+__global__ void k_sched_count(Src src, int cap, int coop_cap, int* __restrict__ ctr, int2* __restrict__ meta) {
+    __shared__ int hist[kClasses];
+    for (int i = threadIdx.x; i < kClasses; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const int n = min(src.count(), cap);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const float2 *a, *b;
+        int la, lb;
+        int32_t* o;
+        src.get(p, a, la, b, lb, o);
+        const int len1 = min(la, lb), len2 = max(la, lb);
+        const int T = len1 <= 0 ? 1 : (len1 + 32 * R - 1) / (32 * R);
+        int slot = -1, items = 1;
+        if (T >= 2) {
+            const int sl = atomicAdd(&ctr[1], 1);
+            if (sl < coop_cap) {
+                slot = sl;
+                items = T;
+            }
         }
-        items[p] = it;
+        const long long dur = slot >= 0 ? (long long)len2 + 32LL * (T - 1) : (long long)T * (len2 + 31);
+        const int c = duration_class(dur);
+        atomicAdd(&hist[c], items);
+        meta[p] = make_int2(slot, (c << 16) | items);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kClasses; i += blockDim.x)
+        if (hist[i]) atomicAdd(&ctr[4 + i], hist[i]);
+}
+
+template <class Src>
+__global__ void k_sched_write(Src src, int cap, int* __restrict__ ctr, const int2* __restrict__ meta,
+                              int4* __restrict__ items) {
+    __shared__ int off[kClasses];
+    __shared__ int lcnt[kClasses];
+    __shared__ int lbase[kClasses];
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int c = kClasses - 1; c >= 0; c--) {
+            off[c] = acc;
+            acc += ctr[4 + c];
+        }
+        if (blockIdx.x == 0) ctr[2] = acc;
+    }
+    const int n = min(src.count(), cap);
+    /* block-sized chunks (uniform trip count over the block) so the local counters reset */
+    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        for (int i = threadIdx.x; i < kClasses; i += blockDim.x) lcnt[i] = 0;
+        __syncthreads();
+        const int p = base + threadIdx.x;
+        int c = 0, nit = 0, loc = 0, slot = -1;
+        if (p < n) {
+            const int2 m = meta[p];
+            slot = m.x;
+            c = m.y >> 16;
+            nit = m.y & 0xffff;
+            loc = atomicAdd(&lcnt[c], nit);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kClasses; i += blockDim.x)
+            if (lcnt[i]) lbase[i] = atomicAdd(&ctr[4 + kClasses + i], lcnt[i]);
+        __syncthreads();
+        if (p < n) {
+            const int pos = off[c] + lbase[c] + loc;
+            if (slot < 0)
+                items[pos] = make_int4(p, -1, -1, 1);
+            else
+                for (int t = 0; t < nit; t++) items[pos + t] = make_int4(p, t, slot, nit);
+        }
+        __syncthreads();
     }
 }
 
-/* One row tile of one pair (rows r0 = t * 32R ...). cin: the bottom row of tile t-1
- * (nullptr for t == 0), cout: this tile's bottom row for tile t+1 (nullptr for the last tile);
- * prog_in/prog_out: progress words when the neighbouring tile runs on another warp. Returns
- * false when a wait gave up. The owner lane of the pair's last row leaves the distance in
- * `result`. */
+/* Match mask of one cell: -1 when |x1 - x2| < u and |y1 - y2| < u (float differences, no
+ * contraction), else 0. */
+__device__ __forceinline__ int match_mask(float ax, float ay, float2 b, float u) {
+    const float dx = __fsub_rn(ax, b.x), dy = __fsub_rn(ay, b.y);
+    int m;
+    asm("{\n\t.reg .pred p;\n\t.reg .f32 t0, t1;\n\t"
+        "abs.f32 t0, %1;\n\tabs.f32 t1, %2;\n\t"
+        "setp.lt.f32 p, t0, %3;\n\t"
+        "set.lt.and.s32.f32 %0, t1, %3, p;\n\t}"
+        : "=r"(m)
+        : "f"(dx), "f"(dy), "f"(u));
+    return m;
+}
+
+/* One wavefront step of a lane's R rows at column c (DP column index). Values are held shifted
+ * by their column: E[r][c] = D[r][c] - c. The reference's three operands at (r, c) become, in
+ * column c's shift, m = E[r-1][c-1] + (match ? -1 : 0), l = E[r][c-1] and u = E[r-1][c] + 1;
+ * a common shift keeps every comparison, so the choice min(u, mml), mml = min(m, l) or +inf
+ * when m == l, is taken on shifted values unchanged. State per row i: Lp[i] = E[r0+i+1][c-1];
+ * diag0 = E[r0][c-1]; up0 = E[r0][c] (the value above the lane's first row). */
 template <int R>
-__device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const float2* __restrict__ cols, int len1,
-                                         int len2, int t, const int* cin, int* cout, const int* prog_in,
-                                         int* prog_out, float u, float2* bring, int* cring, int& result) {
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    constexpr int kTile = 32 * R;
-    const int last_row = len1 - 1;
-    const int r0 = t * kTile + lane * R;
-    float ax[R], ay[R];
-    int left[R];
+__device__ __forceinline__ int wf_step(const float (&ax)[R], const float (&ay)[R], int (&Lp)[R], int& diag0, float2 b,
+                                       int up0, float u) {
+    int mml[R];
 #pragma unroll
     for (int i = 0; i < R; i++) {
-        int r = r0 + i;
+        const int m = (i == 0 ? diag0 : Lp[i - 1]) + match_mask(ax[i], ay[i], b, u);
+        mml[i] = (m == Lp[i]) ? kBig : min(m, Lp[i]);
+    }
+    int up = up0;
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+        up = __viaddmin_s32(up, 1, mml[i]);
+        Lp[i] = up;
+    }
+    diag0 = up0;
+    return up;
+}
+
+/* One row tile of one pair (rows r0 = t * 32R ...). cin: the carry words of tile t-1's bottom
+ * row (nullptr for t == 0), accepted with tag tag_in; cout: this tile's bottom row for tile t+1
+ * (nullptr for the last tile), written with tag tag_out. Returns false when a wait gave up.
+ * The owner lane of the pair's last row leaves the distance in `result`.
+ *
+ * Columns move through a per-warp window of 64 points in shared memory: at the start of the
+ * chunk of columns [s0, s0 + 32) the window holds columns s0 - 32 .. s0 + 31, so lane L reads
+ * column s0 + k - L of step k at window index 32 + k - L (a per-lane base plus a constant).
+ * The next chunk's points and carry words are loaded one chunk early. Chunks where every
+ * lane's column is inside the pair skip the bounds test. */
+template <int R>
+__device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const float2* __restrict__ cols, int len1,
+                                         int len2, int t, const carry_t* cin, carry_t* cout, carry_t tag_in,
+                                         carry_t tag_out, float u, float2* sb, int* sc, int& result) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool lane0 = lane == 0;
+    const bool writer = cout != nullptr && lane == 31;
+    constexpr int kTile = 32 * R;
+    const int r0 = t * kTile + lane * R;
+    float ax[R], ay[R];
+    int Lp[R];
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+        const int r = r0 + i;
         if (r < len1) {
-            float2 v = rows[r];
+            const float2 v = rows[r];
             ax[i] = v.x;
             ay[i] = v.y;
         } else {
             ax[i] = __int_as_float(0x7f800000); /* +inf never matches */
             ay[i] = ax[i];
         }
-        left[i] = r + 1; /* D[r+1][0] */
+        Lp[i] = r + 1; /* E[r+1][0] = D[r+1][0] */
     }
-    const bool owns_last = (last_row >= r0) && (last_row < r0 + R);
-    const int last_i = last_row - r0;
-    int diag_in = r0; /* D[r0][0] */
+    int diag0 = r0; /* E[r0][0] */
     int bottom = 0;
+    const float2* pb = sb + 32 - lane;
     const int steps = len2 + 31;
-    for (int s = 0; s < steps; s++) {
-        if ((s & 31) == 0) {
-            __syncwarp();
-            if (prog_in && s < len2) {
-                int ok = 1;
-                if (lane == 0) {
-                    const int need = min(s + 32, len2);
-                    int polls = 0;
-                    while (ld_acquire(prog_in) < need) {
-                        if (++polls > kSpinLimit) {
-                            ok = 0;
-                            break;
-                        }
-                        __nanosleep(64);
+    const carry_t tag_hi = tag_out << 16;
+    /* prefetched inputs of the next chunk: column point and carry word of column s0 + lane */
+    float2 nb = make_float2(0.f, 0.f);
+    carry_t nw = 0;
+    bool nw_ok = false;
+    if (lane < len2) {
+        nb = cols[lane];
+        if (cin) {
+            nw = ld_carry(cin + lane + 1);
+            nw_ok = (nw >> 16) == tag_in;
+        }
+    }
+    for (int s0 = 0; s0 < steps; s0 += 32) {
+        const int c = s0 + lane;
+        if (s0 < len2) {
+            int cv = 0; /* E[0][c+1] = D[0][c+1] - (c+1) for the first tile */
+            if (cin) {
+                bool ok = c >= len2 || nw_ok;
+                for (int polls = 0;; polls++) {
+                    if (!ok) {
+                        nw = ld_carry(cin + c + 1);
+                        ok = (nw >> 16) == tag_in;
                     }
+                    if (__all_sync(FULL, ok)) break;
+                    if (polls >= kSpinLimit) return false;
+                    if (polls >= 16) __nanosleep(64); /* each poll is an L2 round trip already */
                 }
-                if (!__shfl_sync(FULL, ok, 0)) return false;
-            }
-            int c = s + lane;
-            if (c < len2) {
-                bring[c & 63] = cols[c];
-                cring[c & 63] = cin ? __ldcg(cin + c + 1) : c + 1;
+                cv = (int)(short)(nw & 0xffffu);
             }
             __syncwarp();
+            sb[lane] = sb[32 + lane];
+            sb[32 + lane] = nb;
+            sc[lane] = cv;
+            __syncwarp();
+            /* next chunk */
+            const int cn = c + 32;
+            nw_ok = false;
+            if (cn < len2) {
+                nb = cols[cn];
+                if (cin) {
+                    nw = ld_carry(cin + cn + 1);
+                    nw_ok = (nw >> 16) == tag_in;
+                }
+            }
+        } else {
+            __syncwarp();
+            sb[lane] = sb[32 + lane];
+            __syncwarp();
         }
-        const int from_above = __shfl_up_sync(FULL, bottom, 1);
-        const int j = s - lane;
-        if (j >= 0 && j < len2) {
-            const float2 b = bring[j & 63];
-            const int upf = lane == 0 ? cring[j & 63] : from_above;
-            int mml[R];
-#pragma unroll
-            for (int i = 0; i < R; i++) {
-                const bool match = (fabsf(__fsub_rn(ax[i], b.x)) < u) & (fabsf(__fsub_rn(ay[i], b.y)) < u);
-                const int m = (i == 0 ? diag_in : left[i - 1]) + (match ? 0 : 1);
-                const int l = left[i] + 1;
-                mml[i] = (m == l) ? kBig : min(m, l);
+        if (s0 >= 32 && s0 + 32 <= len2) {
+            /* every lane's column s0 + k - lane lies in [1, len2) */
+#pragma unroll 8
+            for (int k = 0; k < 32; k++) {
+                const int from_above = __shfl_up_sync(FULL, bottom, 1);
+                const int up0 = lane0 ? sc[k] : from_above;
+                bottom = wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u);
+                if (writer) st_carry(cout + (s0 + k - 30), tag_hi | (carry_t)(unsigned short)bottom);
             }
-            int up = upf;
-#pragma unroll
-            for (int i = 0; i < R; i++) {
-                up = __viaddmin_s32(up, 1, mml[i]);
-                left[i] = up;
-            }
-            bottom = up;
-            diag_in = upf;
-            if (cout && lane == 31) {
-                cout[j + 1] = bottom;
-                if (prog_out && (((j + 1) & 31) == 0 || j + 1 == len2)) st_release(prog_out, j + 1);
-            }
-            if (owns_last && j == len2 - 1) {
-#pragma unroll
-                for (int i = 0; i < R; i++)
-                    if (i == last_i) result = left[i];
+        } else {
+            const int kend = min(32, steps - s0);
+            for (int k = 0; k < kend; k++) {
+                const int from_above = __shfl_up_sync(FULL, bottom, 1);
+                const int j = s0 + k - lane;
+                if (j >= 0 && j < len2) {
+                    const int up0 = lane0 ? sc[k] : from_above;
+                    bottom = wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u);
+                    if (writer) st_carry(cout + (j + 1), tag_hi | (carry_t)(unsigned short)bottom);
+                }
             }
         }
+    }
+    const int last_i = len1 - 1 - r0;
+    if (last_i >= 0 && last_i < R) {
+#pragma unroll
+        for (int i = 0; i < R; i++)
+            if (i == last_i) result = Lp[i] + len2; /* D = E + column */
     }
     __syncwarp();
     return true;
 }
 
 template <int R, class Src>
-__global__ void __launch_bounds__(kWarps * 32) k_edr_tiles(Src src, float u, TileCtl ctl, unsigned* __restrict__ work,
+__global__ void __launch_bounds__(kWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(Src src, float u, TileCtl ctl, unsigned* __restrict__ work,
                                                            unsigned long long* __restrict__ cells) {
     __shared__ float2 bring[kWarps][64];
-    __shared__ int cring[kWarps][64];
+    __shared__ int cring[kWarps][32];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int gw = blockIdx.x * kWarps + wib;
-    int* wc0 = ctl.warp_carry + (size_t)gw * 2 * ctl.stride;
-    int* wc1 = wc0 + ctl.stride;
-    const int n = src.count();
-    /* without an item prefix every pair is one item (no pair spans two tiles) */
-    const int64_t total = ctl.item_pre ? ctl.item_pre[n] : (int64_t)n;
+    carry_t* wc0 = ctl.warp_carry + (size_t)gw * 2 * ctl.stride;
+    carry_t* wc1 = wc0 + ctl.stride;
+    const carry_t ep = ctl.epoch << 8;
+    const unsigned total = (unsigned)*ctl.total;
     for (;;) {
-        unsigned item = 0;
-        if (lane == 0) item = atomicAdd(work, 1u);
-        item = __shfl_sync(FULL, item, 0);
-        if ((int64_t)item >= total) break;
-        int p = (int)item, t0 = 0, nitems = 1;
-        if (ctl.item_pre) {
-            int lo = 0, hi = n - 1; /* last pair whose first item is <= item */
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (ctl.item_pre[mid] <= (int64_t)item)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            p = lo;
-            t0 = (int)((int64_t)item - ctl.item_pre[p]);
-            nitems = (int)(ctl.item_pre[p + 1] - ctl.item_pre[p]);
-        }
+        unsigned idx = 0;
+        if (lane == 0) idx = atomicAdd(work, 1u);
+        idx = __shfl_sync(FULL, idx, 0);
+        if (idx >= total) break;
+        const int4 it = ctl.items[idx];
+        const int p = it.x, t = it.y;
         const float2 *pa, *pb;
         int la, lb;
         int32_t* outp;
@@ -373,19 +529,17 @@ __global__ void __launch_bounds__(kWarps * 32) k_edr_tiles(Src src, float u, Til
         const int T = (len1 + kTile - 1) / kTile;
         int result = 0;
         bool ok = true, finished = false;
-        if (nitems == 1) {
-            for (int t = 0; t < T && ok; t++)
-                ok = edr_tile<R>(rows, cols, len1, len2, t, t > 0 ? ((t - 1) & 1 ? wc1 : wc0) : nullptr,
-                                 t + 1 < T ? ((t & 1) ? wc1 : wc0) : nullptr, nullptr, nullptr, u, bring[wib], cring[wib],
-                                 result);
+        if (t < 0) {
+            for (int tt = 0; tt < T && ok; tt++)
+                ok = edr_tile<R>(rows, cols, len1, len2, tt, tt > 0 ? ((tt - 1) & 1 ? wc1 : wc0) : nullptr,
+                                 tt + 1 < T ? ((tt & 1) ? wc1 : wc0) : nullptr, ep | ((tt - 1) & 0xff),
+                                 ep | (tt & 0xff), u, bring[wib], cring[wib], result);
             finished = true;
         } else {
-            const int t = t0;
-            int* pc = ctl.pair_carry + (size_t)p * 2 * ctl.stride;
-            const int64_t base = ctl.item_pre ? ctl.item_pre[p] : p;
+            carry_t* pc = ctl.pair_carry + (size_t)it.z * 2 * ctl.stride;
             ok = edr_tile<R>(rows, cols, len1, len2, t, t > 0 ? pc + ((t - 1) & 1) * ctl.stride : nullptr,
-                             t + 1 < T ? pc + (t & 1) * ctl.stride : nullptr, t > 0 ? ctl.prog + base + t - 1 : nullptr,
-                             t + 1 < T ? ctl.prog + base + t : nullptr, u, bring[wib], cring[wib], result);
+                             t + 1 < T ? pc + (t & 1) * ctl.stride : nullptr, ep | ((t - 1) & 0xff), ep | (t & 0xff),
+                             u, bring[wib], cring[wib], result);
             finished = t == T - 1;
         }
         if (!ok) {
@@ -406,12 +560,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_edr_tiles(Src src, float u, Til
     }
 }
 
-/* Host side: prep (items per pair) -> scan -> tiled kernel. cap bounds the pair count (exact
- * for host-known lists, an upper bound for device-counted ones); max_rows / max_cols bound the
- * shorter / longer side of every pair. */
+/* Host side: schedule (count, write) -> tiled kernel. cap is the number of pairs (exact for
+ * host-known lists, an upper bound for device-counted ones); max_rows / max_cols bound the
+ * shorter / longer side of every pair. ev0/ev1, when given, bracket the tile kernel. */
 template <int R, class Src>
 int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
-                 unsigned long long* cells) {
+                 unsigned long long* cells, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
     int st = GAT_OK;
     cudaStream_t s = ctx->stream;
     int per_sm = 0;
@@ -420,27 +574,30 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     const int stride = max_cols + 2;
     const int maxT = max_rows <= 0 ? 1 : (max_rows + 32 * R - 1) / (32 * R);
     const size_t budget = (size_t)512 << 20; /* cooperative carry rows */
-    int64_t coop = (int64_t)(budget / ((size_t)2 * stride * sizeof(int)));
+    int64_t coop = (int64_t)(budget / ((size_t)2 * stride * sizeof(carry_t)));
     if (coop > cap) coop = cap;
     if (maxT < 2) coop = 0;
-    int64_t* items = coop > 0 ? (int64_t*)scratch(ctx, S_EDR_ITEMS, (size_t)(cap + 1) * 8, &st) : nullptr;
-    int* prog = coop > 0 ? (int*)scratch(ctx, S_EDR_PROG, (size_t)coop * maxT * 4, &st) : nullptr;
-    int* pcarry = coop > 0 ? (int*)scratch(ctx, S_EDR_PCARRY, (size_t)coop * 2 * stride * 4, &st) : nullptr;
-    int* wcarry = (int*)scratch(ctx, S_EDR_CARRY, (size_t)grid * kWarps * 2 * stride * 4, &st);
-    unsigned* work = (unsigned*)scratch(ctx, S_EDR_COUNTERS, 64, &st);
-    if (!wcarry || !work || (coop > 0 && (!items || !prog || !pcarry))) return st;
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(work, 0, sizeof(unsigned), s), "edr");
-    if (coop > 0) {
-        /* items per pair and their prefix; skipped when no pair spans two tiles */
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(prog, 0, (size_t)coop * maxT * 4, s), "edr");
-        int pgrid = (int)std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->sm_count * 16);
-        k_edr_prep<R, Src><<<pgrid > 0 ? pgrid : 1, 256, 0, s>>>(src, (int)cap, (int)coop, items);
-        count_launch(ctx);
-        if ((st = scan_i64(ctx, items, items, cap)) != GAT_OK) return st;
-    }
-    TileCtl ctl{items, prog, pcarry, (int)coop, wcarry, stride, ctx->d_flag};
+    const int64_t item_cap = cap + coop * (maxT - 1);
+    if (item_cap >= (int64_t)1 << 31) return fail(ctx, GAT_ERR_ARG, "edr: too many work items in one launch");
+    int* ctr = (int*)scratch(ctx, S_EDR_COUNTERS, kCtrWords * sizeof(int), &st);
+    int2* meta = (int2*)scratch(ctx, S_EDR_META, (size_t)cap * sizeof(int2), &st);
+    int4* items = (int4*)scratch(ctx, S_EDR_ITEMS, (size_t)item_cap * sizeof(int4), &st);
+    carry_t* pcarry =
+        coop > 0 ? (carry_t*)scratch_zeroed(ctx, S_EDR_PCARRY, (size_t)coop * 2 * stride * sizeof(carry_t), &st) : nullptr;
+    carry_t* wcarry = (carry_t*)scratch_zeroed(ctx, S_EDR_CARRY, (size_t)grid * kWarps * 2 * stride * sizeof(carry_t), &st);
+    if (!ctr || !meta || !items || !wcarry || (coop > 0 && !pcarry)) return st;
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(ctr, 0, kCtrWords * sizeof(int), s), "edr");
+    const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->sm_count * 8));
+    k_sched_count<R, Src><<<pgrid, 256, 0, s>>>(src, (int)cap, (int)coop, ctr, meta);
+    count_launch(ctx);
+    k_sched_write<Src><<<pgrid, 256, 0, s>>>(src, (int)cap, ctr, meta, items);
+    count_launch(ctx);
+    ctx->edr_epoch++;
+    TileCtl ctl{items, ctr + 2, pcarry, wcarry, stride, (unsigned long long)ctx->edr_epoch, ctx->d_flag};
     timed_begin(ctx, GAT_KERNEL_EDR);
-    k_edr_tiles<R, Src><<<grid, kWarps * 32, 0, s>>>(src, u, ctl, work, cells);
+    if (ev0) cudaEventRecord(ev0, s);
+    k_edr_tiles<R, Src><<<grid, kWarps * 32, 0, s>>>(src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
+    if (ev1) cudaEventRecord(ev1, s);
     timed_end(ctx, GAT_KERNEL_EDR, 0.0);
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "edr launch");
@@ -448,11 +605,60 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
 }
 
 template <class Src>
+int launch_rows(gat_ctx* ctx, int R, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
+                unsigned long long* cells, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
+    switch (R) {
+        case 2: return launch_tiles<2, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 4: return launch_tiles<4, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        default: return launch_tiles<8, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+    }
+}
+
+inline uint64_t ceil_log2(int64_t v) {
+    uint64_t e = 0;
+    while (e < 62 && ((int64_t)1 << e) < v) e++;
+    return e;
+}
+
+/* EDR over a pair source with the context's rows-per-lane choice. Autotune (edr_rows == 0):
+ * the first launch of a shape class times 8, 4 and 2 rows per lane on this launch's own
+ * pairs (every candidate writes the same results; the cell counter is fed once) and records
+ * the fastest; later launches of the class use it. */
+template <class Src>
 int edr_launch(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
                unsigned long long* cells) {
     if (cap <= 0) return GAT_OK;
-    return max_rows <= 128 ? launch_tiles<4, Src>(ctx, src, cap, max_rows, max_cols, u, cells)
-                           : launch_tiles<8, Src>(ctx, src, cap, max_rows, max_cols, u, cells);
+    if (ctx->edr_rows != 0) return launch_rows(ctx, ctx->edr_rows, src, cap, max_rows, max_cols, u, cells);
+    const uint64_t key = ((uint64_t)Src::kKind << 60) | (ceil_log2(cap) << 40) | (ceil_log2(max_rows) << 20) |
+                         ceil_log2(max_cols);
+    auto hit = ctx->edr_tune.find(key);
+    if (hit != ctx->edr_tune.end()) return launch_rows(ctx, hit->second, src, cap, max_rows, max_cols, u, cells);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        cudaGetLastError();
+        return launch_rows(ctx, 8, src, cap, max_rows, max_cols, u, cells);
+    }
+    int best = 8, st = GAT_OK;
+    float best_ms = 0.f;
+    const int cand[3] = {8, 4, 2};
+    for (int i = 0; i < 3 && st == GAT_OK; i++) {
+        st = launch_rows(ctx, cand[i], src, cap, max_rows, max_cols, u, i == 0 ? cells : nullptr, e0, e1);
+        if (st != GAT_OK) break;
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            st = cuda_fail(ctx, cudaGetLastError(), "edr autotune");
+            break;
+        }
+        if (i == 0 || ms < best_ms) {
+            best_ms = ms;
+            best = cand[i];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st == GAT_OK) ctx->edr_tune[key] = best;
+    return st;
 }
 
 }  // namespace edr

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -78,7 +79,8 @@ struct gat_ctx {
     /* scratch arena: slot -> device buffer, grown on demand, freed with the context */
     std::vector<void*> slot_ptr;
     std::vector<size_t> slot_bytes;
-    int32_t* d_flag = nullptr; /* device status word written by kernels (0 = ok) */
+    std::vector<char> slot_fresh; /* allocated since the last scratch_zeroed clear */
+    int32_t* d_flag = nullptr; /* [0] device status written by kernels (0 = ok), [1] sink word */
     /* optional per-kernel-class event timing (gat_ctx_set_timing) */
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[GAT_KERNEL_CLASSES];
@@ -87,6 +89,10 @@ struct gat_ctx {
     int64_t t_launches[GAT_KERNEL_CLASSES] = {0, 0, 0};
     double t_work[GAT_KERNEL_CLASSES] = {0, 0, 0};
     int64_t* h_pinned = nullptr; /* pinned host words for small D2H reads */
+    /* EDR rows per lane: 0 = autotune per shape class (edr_tune), else fixed */
+    int edr_rows = 0;
+    std::map<uint64_t, int> edr_tune;
+    uint64_t edr_epoch = 0; /* launches of the tiled EDR kernel; tags its carry words */
 };
 
 struct gat_db {
@@ -137,6 +143,8 @@ int fail(gat_ctx* ctx, int code, const std::string& msg);
 int cuda_fail(gat_ctx* ctx, cudaError_t e, const char* what);
 /* device scratch slot of at least `bytes` bytes; contents undefined */
 void* scratch(gat_ctx* ctx, int slot, size_t bytes, int* status);
+/* same, but a slot that was (re)allocated is cleared to zero (on the context stream) first */
+void* scratch_zeroed(gat_ctx* ctx, int slot, size_t bytes, int* status);
 /* cudaMalloc tracked by an index (freed by gat_index_destroy) */
 void* index_alloc(gat_index* ix, size_t bytes, int* status);
 template <class T>
@@ -188,8 +196,8 @@ enum Slot {
     S_EDR_COUNTERS,
     S_EDR_IO,
     S_EDR_ITEMS,
-    S_EDR_PROG,
     S_EDR_PCARRY,
+    S_EDR_META,
     S_TOPK_QFV,
     S_TOPK_LB,
     S_TOPK_PAIRS,

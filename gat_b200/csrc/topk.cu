@@ -502,6 +502,7 @@ struct WalkPairs {
     const int64_t* db_off;
     const float2* DB;
     int32_t* sdist;
+    static constexpr int kKind = 1;
     __device__ int count() const { return wprefix[nq]; }
     __device__ void get(int w, const float2*& a, int& la, const float2*& b, int& lb, int32_t*& o) const {
         int lo = 0, hi = nq - 1; /* last q with wprefix[q] <= w */
@@ -528,7 +529,7 @@ struct WalkPairs {
  * and k evaluated pairs already sort before (W, nid). While nlb < W the walk goes on: a
  * candidate with a smaller bound may still be closer. */
 __global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* slb, const int32_t* cand,
-                           const int32_t* sdist, int32_t* ws, int* pending) {
+                           const int32_t* sdist, int32_t* ws) {
     extern __shared__ int hist[];
     __shared__ int sh_W, cnt;
     int qi = blockIdx.x;
@@ -580,7 +581,6 @@ __global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* sl
         s[WS_W] = W;
         s[WS_DONE] = done ? 1 : 0;
         s[WS_CHUNK] = (int)min((long long)growth * s[WS_CHUNK], 1LL << 30);
-        if (!done) atomicAdd(pending, 1);
     }
 }
 
@@ -760,7 +760,7 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     k_sort_scatter<<<dim3(ntile, nq), 32, smem_run, s>>>(n, lb, bins_lb, ntile, H, cand, slb);
     count_launch(ctx);
     /* the walk: a finished query costs nothing in later rounds, `rounds` covers the whole
-     * order with growing chunks, and the loop ends early once no query is pending */
+     * order with growing chunks, and the loop ends early once no query extends */
     /* a lone query leaves most of the GPU idle in a small round, so it starts with a larger
      * chunk and grows faster; a batch keeps rounds tight to limit surplus evaluations */
     const bool lone = nq <= 4;
@@ -781,22 +781,19 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     int rows_hint = std::min(max_q_len, db->maxlen);
     int max_cols = std::max(max_q_len, db->maxlen);
     WalkPairs src{n, nq, wprefix, ws, cand, d_q_len, d_q_off, d_q_xy, db->d_len, db->d_off, db->d_xy, sdist};
-    int64_t chunk_r = chunk0;
     for (int r = 0; r < rounds; r++) {
         k_walk_plan<<<1, 1024, 0, s>>>(n, nq, slb, ws, wprefix);
         count_launch(ctx);
-        /* upper bound of this round's pairs: every query extends by at most its chunk */
-        int64_t cap = std::min<int64_t>((int64_t)nq * chunk_r, (int64_t)nq * n);
-        if ((st = edr::edr_launch(ctx, src, cap, rows_hint, max_cols, u, cells)) != GAT_OK) return st;
-        chunk_r = std::min<int64_t>(chunk_r * growth, (int64_t)1 << 30);
-        int* pending = reinterpret_cast<int*>(cells + 1);
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(pending, 0, sizeof(int), s), "top-k");
-        k_walk_kth<<<nq, kT, smem_d, s>>>(n, k, bins_d, growth, slb, cand, sdist, ws, pending);
-        count_launch(ctx);
-        /* stop as soon as every query is done: one small read per round */
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 4, pending, sizeof(int), cudaMemcpyDeviceToHost, s), "top-k");
+        /* the round's pair count sizes the EDR launch exactly; it is zero once no query can
+         * extend (every query at the end of its order or with its next bound above W) */
+        int32_t* cnt = reinterpret_cast<int32_t*>(ctx->h_pinned + 4);
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, wprefix + nq, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "top-k");
         GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "top-k");
-        if ((int)(ctx->h_pinned[4] & 0xffffffff) == 0) break;
+        const int64_t npairs = *cnt;
+        if (npairs == 0) break;
+        if ((st = edr::edr_launch(ctx, src, npairs, rows_hint, max_cols, u, cells)) != GAT_OK) return st;
+        k_walk_kth<<<nq, kT, smem_d, s>>>(n, k, bins_d, growth, slb, cand, sdist, ws);
+        count_launch(ctx);
     }
     /* selection */
     int words = (n + 1 + 31) / 32;

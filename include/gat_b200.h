@@ -81,6 +81,17 @@ int64_t gat_ctx_scratch_bytes(const gat_ctx* ctx);
 enum { GAT_KERNEL_EDR = 0, GAT_KERNEL_BOUNDS = 1, GAT_KERNEL_RANGE_SCAN = 2, GAT_KERNEL_CLASSES = 3 };
 int gat_ctx_set_timing(gat_ctx* ctx, int on);
 int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* launches, double* work);
+/* Tuning knobs (no counterpart in the reference, which has fixed launch shapes).
+ * GAT_TUNE_EDR_ROWS: rows each lane of the EDR wavefront owns (tile height = 32 x rows).
+ *   0 (default) = autotune: the first launch of each shape class (pair count, longest shorter
+ *   side and longest longer side, each rounded up to a power of two) times 2, 4 and 8 rows
+ *   per lane on the caller's own data and keeps the fastest for that class; results are the
+ *   same for every choice. 2, 4 or 8 fixes the value. Setting the knob clears the tuned table.
+ * gat_ctx_get_tuning(GAT_TUNE_EDR_ROWS) returns the knob; GAT_TUNE_EDR_TUNED returns the
+ * number of tuned shape classes. */
+enum { GAT_TUNE_EDR_ROWS = 1, GAT_TUNE_EDR_TUNED = 2 };
+int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value);
+int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value);
 
 /* ---------------------------------------------------------------- trajectory set */
 int gat_db_create(gat_ctx* ctx, int n, const int32_t* lengths, const float* lon, const float* lat,
@@ -134,7 +145,8 @@ int gat_edr_pairs(gat_ctx* ctx, int npairs, const int32_t* q_len, const int64_t*
                   const float* q_xy, int64_t q_points, const int32_t* c_len,
                   const int64_t* c_off, const float* c_xy, int64_t c_points, double eps,
                   int32_t* out);
-/* Same, device arrays. */
+/* Same, device arrays. A pair with a side outside 1..GAT_EDR_MAX_LEN gets -1 and the call
+ * returns GAT_ERR_ARG. */
 int gat_edr_pairs_dev(gat_ctx* ctx, int npairs, const int32_t* d_q_len, const int64_t* d_q_off,
                       const float* d_q_xy, const int32_t* d_c_len, const int64_t* d_c_off,
                       const float* d_c_xy, double eps, int32_t* d_out);

@@ -68,3 +68,103 @@ def test_full_config4_properties(gpu_ctx):
     eq = la == lb
     # with unequal lengths the shorter side is always the row side, so swapping is invariant
     assert np.array_equal(d[~eq], d2[~eq])
+
+
+def _mixed_pairs():
+    la = np.concatenate([D.lengths(600, 2, 0, 0, 1, 900, 51), [1, 64, 65, 128, 129, 256, 257, 512, 513]]).astype(np.int32)
+    lb = np.concatenate([D.lengths(600, 2, 0, 0, 1, 900, 52), [700, 64, 66, 900, 129, 257, 256, 1024, 2000]]).astype(np.int32)
+    a, b = D.pairs(la, lb, 53)
+    return la, a, lb, b
+
+
+@pytest.mark.parametrize("rows", [2, 4, 8])
+def test_rows_per_lane_variants(gpu_ctx, rows):
+    """Every tile height (64, 128, 256 rows) gives the oracle's distances, across single-tile
+    pairs, pipelined multi-tile pairs and the tile boundaries."""
+    la, a, lb, b = _mixed_pairs()
+    want = po.edr_batch(la, a, lb, b, 5e-4)
+    gpu_ctx.set_edr_rows(rows)
+    try:
+        got = G.edr_pairs(gpu_ctx, la, a, lb, b, 5e-4)
+    finally:
+        gpu_ctx.set_edr_rows(0)
+    assert np.array_equal(got, want)
+
+
+def test_autotune_classes(gpu_ctx):
+    """Autotune (the default) records the shape class on first use; both the tuning launch
+    and the tuned launch give the oracle's distances."""
+    from gat_b200 import _lib as L
+
+    gpu_ctx.set_edr_rows(0)  # clears the table
+    assert gpu_ctx.tuning(L.GAT_TUNE_EDR_TUNED) == 0
+    la, a, lb, b = _mixed_pairs()
+    want = po.edr_batch(la, a, lb, b, 5e-4)
+    assert np.array_equal(G.edr_pairs(gpu_ctx, la, a, lb, b, 5e-4), want)
+    assert gpu_ctx.tuning(L.GAT_TUNE_EDR_TUNED) >= 1
+    assert np.array_equal(G.edr_pairs(gpu_ctx, la, a, lb, b, 5e-4), want)
+    with pytest.raises(G.GatError):
+        gpu_ctx.set_edr_rows(3)
+
+
+def test_device_api_beyond_cooperative_pool(gpu_ctx):
+    """gat_edr_pairs_dev sizes carry rows for the longest allowed side, which caps the
+    cooperative pool at a few thousand pairs; more multi-tile pairs than that run tile by
+    tile on one warp each. Both kinds must agree with the oracle."""
+    import torch
+
+    from gat_b200 import _lib as L
+
+    la = D.lengths(5000, 0, 0, 0, 65, 300, 61)
+    lb = D.lengths(5000, 0, 0, 0, 65, 300, 62)
+    a, b = D.pairs(la, lb, 63)
+    oa = np.zeros(len(la), np.int64); oa[1:] = np.cumsum(la)[:-1]
+    ob = np.zeros(len(lb), np.int64); ob[1:] = np.cumsum(lb)[:-1]
+    dev = torch.device("cuda", 0)
+    T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    d = [T(la.astype(np.int32)), T(oa), T(a), T(lb.astype(np.int32)), T(ob), T(b)]
+    out = torch.full((len(la),), -7, dtype=torch.int32, device=dev)
+    want = po.edr_batch(la, a, lb, b, 5e-4)
+    gpu_ctx.set_edr_rows(2)
+    try:
+        torch.cuda.synchronize()
+        gpu_ctx.check(L.lib.gat_edr_pairs_dev(gpu_ctx.h, len(la), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                              d[3].data_ptr(), d[4].data_ptr(), d[5].data_ptr(), 5e-4, out.data_ptr()),
+                      "gat_edr_pairs_dev")
+        gpu_ctx.check(L.lib.gat_ctx_sync(gpu_ctx.h), "gat_ctx_sync")
+    finally:
+        gpu_ctx.set_edr_rows(0)
+    assert np.array_equal(out.cpu().numpy(), want)
+
+
+def test_device_api_rejects_bad_lengths(gpu_ctx):
+    """gat_edr_pairs_dev reads lengths on the device: a side outside 1..GAT_EDR_MAX_LEN gets
+    -1 (its points are never read) and the call returns GAT_ERR_ARG; other pairs are exact."""
+    import torch
+
+    from gat_b200 import _lib as L
+
+    la = np.array([10, 0, 40, 20000, 7], np.int32)
+    lb = np.array([12, 5, 33, 9, 7], np.int32)
+    ra, rb = np.maximum(la, 0), lb.copy()
+    ra[3] = 0  # no points stored for the oversize side
+    a, b = D.pairs(np.where(ra > 0, ra, 1), rb, 71)
+    oa = np.zeros(5, np.int64); oa[1:] = np.cumsum(np.where(ra > 0, ra, 1))[:-1]
+    ob = np.zeros(5, np.int64); ob[1:] = np.cumsum(rb)[:-1]
+    dev = torch.device("cuda", 0)
+    T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    d = [T(la), T(oa), T(a), T(lb), T(ob), T(b)]
+    out = torch.full((5,), -7, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    rc = L.lib.gat_edr_pairs_dev(gpu_ctx.h, 5, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(),
+                                 d[4].data_ptr(), d[5].data_ptr(), 5e-4, out.data_ptr())
+    assert rc == L.GAT_ERR_ARG
+    got = out.cpu().numpy()
+    assert got[1] == -1 and got[3] == -1
+    ok = np.array([0, 2, 4])
+    la_ok = la[ok]
+    sa = np.concatenate([a[oa[i]:oa[i] + la[i]] for i in ok])
+    sb = np.concatenate([b[ob[i]:ob[i] + lb[i]] for i in ok])
+    assert np.array_equal(got[ok], po.edr_batch(la_ok, sa, lb[ok], sb, 5e-4))
+    # the context stays usable
+    assert np.array_equal(G.edr_pairs(gpu_ctx, la_ok, sa, lb[ok], sb, 5e-4), got[ok])

@@ -107,3 +107,17 @@ def test_argument_errors(host_ctx):
     with pytest.raises(G.GatError) as e:
         g.range_query(np.zeros((1, 4), np.float32))
     assert e.value.status == L.GAT_ERR_STATE  # host-only context has no device
+
+
+def test_tuning_knob(host_ctx):
+    """GAT_TUNE_EDR_ROWS accepts 0 (autotune), 2, 4 and 8 and nothing else."""
+    for v in (2, 4, 8, 0):
+        host_ctx.set_edr_rows(v)
+        assert host_ctx.tuning(L.GAT_TUNE_EDR_ROWS) == v
+    assert host_ctx.tuning(L.GAT_TUNE_EDR_TUNED) == 0
+    for bad in (1, 3, 16, -1):
+        with pytest.raises(G.GatError) as e:
+            host_ctx.set_edr_rows(bad)
+        assert e.value.status == L.GAT_ERR_ARG
+    with pytest.raises(G.GatError):
+        host_ctx.tuning(99)
