@@ -5,7 +5,8 @@ Default workload (config 2 of the reference's benchmark set): plain EDR top-k si
 256 query trajectories drawn from the set, k = 32, eps = 5e-4 deg, frequency vectors on the
 256 x 256 virtual grid (cell 0.0025 deg, virtual-cell shift 2), one query per launch sequence.
 A step is one pass over the 256 queries. Other workloads: --workload c1 (plain GT-quadtree range
-queries), c3 (batched range queries over the three indexes), c4 (batched EDR pairs).
+queries), c3 (batched range queries over the three indexes), c4 (batched EDR pairs), c5 (served
+mix of range and top-k requests through the serving loop at three offered loads).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
 
@@ -798,7 +799,161 @@ def run_reference_c4(args, world, rank):
     return line
 
 
-WORKLOADS = {"c1": run_c1, "c2": None, "c3": run_c3, "c4": run_c4}
+# ---------------------------------------------------------------- workload: config 5
+C5 = dict(requests=4000, range_frac=0.7, loads=(0.25, 0.5, 0.8), lanes=4, budget=40 << 30, eps=5e-4)
+
+
+def run_c5(args, world, rank, local, td):
+    """Served mix over the C3 set and its three indexes, resident on the device: open-loop
+    Poisson arrivals of 70% range requests (rectangles log-U[0.001, 0.05] deg, spread over the
+    GT-quadtree, STIG and FSG; trajectory-id sets) and 30% top-k requests (query walks with
+    lengths log-U[16, 2048], k uniform in [8, 64], eps 5e-4) through the serving loop
+    (continuous batching, 4 lanes, 40 GiB budget). First a burst of all requests gives the
+    saturation throughput; then three offered loads (fractions of it) give the achieved
+    throughput and p50/p99 latency (arrival to completion, host clock)."""
+    import threading
+
+    import torch
+
+    import gat_b200 as G
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    t, _ = D.config3(seed=0, n=args.c3_n, nq=1)
+    ctx = G.Context(local)
+    db = G.TrajectorySet(ctx, t)
+    grid = G.Grid(ctx, db, G.BOX, C3["cell"], 2, C3["leaf_cap"])
+    stig = G.STIG(ctx, db, C3["stig_block"])
+    fsg = G.FSG(ctx, db, G.BOX, C3["cell"])
+    log("c5 set and indexes", t.n, round(time.time() - t0, 1))
+    n = args.c5_requests
+    rng = np.random.default_rng(500 + rank)
+    is_range = rng.random(n) < C5["range_frac"]
+    ikind = rng.integers(0, 3, n)
+    boxes = D.boxes(n, L.GAT_SIDE_LOGUNIFORM, 0.001, 0.05, 501 + rank)
+    qlen = D.lengths(n, L.GAT_LEN_LOGUNIFORM, 0, 0, 16, 2048, 502 + rank)
+    qs = D.walks(qlen, 503 + rank)
+    ks = rng.integers(8, 65, n)
+    qoff = np.zeros(n + 1, np.int64)
+    qoff[1:] = np.cumsum(qlen)
+    srv = G.Server(ctx, grid, stig, fsg, lanes=C5["lanes"], budget_bytes=C5["budget"])
+
+    def submit(i):
+        if is_range[i]:
+            return srv.submit_range(boxes[i], int(ikind[i]), "ids")
+        a, b = qoff[i], qoff[i + 1]
+        return srv.submit_topk(qs.lon[a:b], qs.lat[a:b], int(ks[i]), C5["eps"])
+
+    def run(idx, rate=None):
+        """Submits requests idx (open loop at `rate` per second, or all at once), waits for all;
+        returns per-request (arrival, completion) ns and the result entries returned."""
+        ids = [None] * len(idx)
+        gaps = rng.exponential(1.0 / rate, len(idx)) if rate else np.zeros(len(idx))
+        due = np.cumsum(gaps)
+
+        def producer():
+            start = time.perf_counter()
+            for j, i in enumerate(idx):
+                while True:
+                    wait = start + due[j] - time.perf_counter()
+                    if wait <= 0:
+                        break
+                    time.sleep(min(wait, 0.0005) if wait > 0.0002 else 0)
+                ids[j] = submit(i)
+
+        th = threading.Thread(target=producer)
+        th.start()
+        th.join()
+        times = np.zeros((len(idx), 3), np.int64)
+        entries = 0
+        for j, r in enumerate(ids):
+            st = srv.wait(r)
+            if st != L.GAT_OK:
+                raise RuntimeError(f"request {idx[j]} failed with status {st}")
+            times[j] = srv.times(r)
+            if is_range[idx[j]]:
+                entries += len(srv.range_result(r))
+            else:
+                entries += int(ks[idx[j]])
+            srv.release(r)
+        return times, entries
+
+    def summary(idx, times, entries):
+        lat = (times[:, 2] - times[:, 0]) / 1e6
+        span = (times[:, 2].max() - times[:, 0].min()) / 1e9
+        rg = np.array([is_range[i] for i in idx])
+        pct = lambda a, p: round(float(np.percentile(a, p)), 3) if len(a) else None
+        return {"requests": len(idx), "achieved_per_s": round(len(idx) / span, 1), "p50_ms": pct(lat, 50),
+                "p99_ms": pct(lat, 99), "range_p50_ms": pct(lat[rg], 50), "range_p99_ms": pct(lat[rg], 99),
+                "topk_p50_ms": pct(lat[~rg], 50), "topk_p99_ms": pct(lat[~rg], 99), "result_entries": entries}
+
+    # warm-up: every lane sees both request kinds (first launches tune the EDR tiles)
+    for _ in range(args.warmup):
+        run(np.arange(0, min(n, 400)))
+    clocks = ClockSampler(local)
+    clocks.start()
+    allidx = np.arange(n)
+    times, entries = run(allidx)
+    sat = summary(allidx, times, entries)
+    loads = []
+    for f in C5["loads"]:
+        rate = f * sat["achieved_per_s"]
+        times, entries = run(allidx, rate)
+        s = summary(allidx, times, entries)
+        s["offered_per_s"] = round(rate, 1)
+        loads.append(s)
+        log("load", f, s)
+    clk = clocks.stop()
+    st = srv.stats()
+    # a sample of requests against the direct calls (each result must equal the request alone)
+    ok = True
+    chk = rng.choice(n, size=min(n, 24), replace=False)
+    for i in chk:
+        r = submit(i)
+        srv.wait(r)
+        if is_range[i]:
+            got = srv.range_result(r)
+            want = {0: grid, 1: stig, 2: fsg}[int(ikind[i])].range_query(boxes[i:i + 1]).tids
+            ok &= bool(np.array_equal(got, want))
+        else:
+            got = srv.topk_result(r, int(ks[i]))
+            a, b = qoff[i], qoff[i + 1]
+            wi, wd, _ = grid.topk(D.Trajectories(np.array([b - a], np.int32), qs.lon[a:b], qs.lat[a:b]), int(ks[i]), C5["eps"])
+            ok &= bool(np.array_equal(got[0], wi[0]) and np.array_equal(got[1], wd[0]))
+        srv.release(r)
+    srv.close()
+    if rank != 0:
+        ctx.close()
+        return None
+    top = loads[-1]
+    h2d = int(sum(32 if is_range[i] else 8 * qlen[i] + 16 for i in range(n)))
+    line = base_line(args, world, "served mixed requests/s (continuous batching; 70% range / 30% top-k)", "requests/s",
+                     top["achieved_per_s"] * world, 1e3 * n / max(top["achieved_per_s"], 1e-9) * args.steps,
+                     {"workload": f"C5 served mix: {t.n} walks U[50,350] resident with GT-quadtree (cell 0.001, leaf 512), "
+                                  f"STIG (block 10240) and FSG (cell 0.001); {n} requests per load: 70% range "
+                                  "(log-U[0.001,0.05] deg rectangles over the three indexes, id sets), 30% top-k "
+                                  "(query lengths log-U[16,2048], k U[8,64], eps 5e-4); open-loop Poisson arrivals",
+                      "server": {"lanes": C5["lanes"], "budget_bytes": C5["budget"], "max_range_batch": 4096,
+                                 "max_topk_batch": 32},
+                      "l2": "inputs (3.2 GB per index) larger than L2", "parallelism": f"replicas x{world}"})
+    line.update({
+        "e2e": {"value": round(top["achieved_per_s"] * world, 1), "unit": "requests/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(top["result_entries"] * 4 * 2),
+                "timer": "host clock from each request's submission to its completion (the serving path is end to end)"},
+        "saturation": sat,
+        "loads": loads,
+        "server_stats": st,
+        "results_equal_direct_calls": ok,
+        "clocks": clk,
+    })
+    ctx.close()
+    return line
+
+
+WORKLOADS = {"c1": run_c1, "c2": None, "c3": run_c3, "c4": run_c4, "c5": run_c5}
 REFERENCE = {"c1": run_reference_c1, "c2": None, "c4": run_reference_c4}
 
 
@@ -808,7 +963,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--cpu-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=0, help="C2: use only the first N of the 256 queries")
@@ -816,6 +971,7 @@ def main():
     ap.add_argument("--c3-indexes", default="grid,fsg,stig")
     ap.add_argument("--c3-n", type=int, default=C3["n"])
     ap.add_argument("--c3-plain-sample", type=int, default=2000)
+    ap.add_argument("--c5-requests", type=int, default=C5["requests"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_env()
@@ -824,6 +980,9 @@ def main():
         if args.workload == "c3":
             line = {"impl": "reference", "unavailable": "the reference's Grid build is O(trajectories x cells) in memset "
                     "(Grid.cpp:268-269); at 1M trajectories and 1M cells it does not finish in minutes"}
+        elif args.workload == "c5":
+            line = {"impl": "reference", "unavailable": "the reference has no serving loop, and its Grid build over the "
+                    "1M-trajectory set does not finish in minutes (Grid.cpp:268-269)"}
         else:
             line = fn(args, world, rank)
         if line is not None:

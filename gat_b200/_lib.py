@@ -37,6 +37,12 @@ GAT_SIDE_FIXED, GAT_SIDE_LOGUNIFORM = 0, 1
 GAT_EDR_MAX_LEN = 16384
 GAT_EDR_NOALLOC_MAX_LEN = 4096
 GAT_KERNEL_EDR, GAT_KERNEL_BOUNDS, GAT_KERNEL_RANGE_SCAN = 0, 1, 2
+class ServerConfig(C.Structure):
+    """gat_server_config."""
+
+    _fields_ = [("lanes", c_int), ("budget_bytes", c_i64), ("max_range_batch", c_int), ("max_topk_batch", c_int)]
+
+
 GAT_TUNE_EDR_ROWS, GAT_TUNE_EDR_TUNED = 1, 2
 
 # (name, restype, argtypes) for every symbol of include/gat_b200.h
@@ -50,6 +56,8 @@ SIGNATURES = [
     ("gat_ctx_scratch_bytes", c_i64, [c_p]),
     ("gat_ctx_set_timing", c_int, [c_p, c_int]),
     ("gat_ctx_kernel_stats", c_int, [c_p, c_int, C.POINTER(c_d), P_i64, C.POINTER(c_d)]),
+    ("gat_ctx_create_worker", c_int, [c_p, C.POINTER(c_p)]),
+    ("gat_ctx_trim", c_int, [c_p]),
     ("gat_ctx_set_tuning", c_int, [c_p, c_int, c_int]),
     ("gat_ctx_get_tuning", c_int, [c_p, c_int, P_i32]),
     ("gat_db_create", c_int, [c_p, c_int, P_i32, P_f32, P_f32, C.POINTER(c_p)]),
@@ -69,6 +77,16 @@ SIGNATURES = [
     ("gat_fv_lower_bounds", c_int, [c_p, c_p, c_int, P_i32, P_f32, P_f32, P_i32]),
     ("gat_topk", c_int, [c_p, c_p, c_int, P_i32, P_f32, P_f32, c_int, c_d, c_int, P_i32, P_i32, P_i64]),
     ("gat_topk_dev", c_int, [c_p, c_p, c_int, c_p, c_p, c_p, c_int, c_int, c_d, c_int, c_p, c_p, P_i64]),
+    ("gat_server_create", c_int, [c_p, c_p, c_p, c_p, C.POINTER(ServerConfig), C.POINTER(c_p)]),
+    ("gat_server_destroy", None, [c_p]),
+    ("gat_server_submit_range", c_int, [c_p, c_int, MBB, c_int, P_i64]),
+    ("gat_server_submit_topk", c_int, [c_p, c_int, P_f32, P_f32, c_int, c_d, P_i64]),
+    ("gat_server_wait", c_int, [c_p, c_i64, c_int, P_i32]),
+    ("gat_server_range_result", c_int, [c_p, c_i64, P_i32, P_i32, c_i64, P_i64]),
+    ("gat_server_topk_result", c_int, [c_p, c_i64, P_i32, P_i32, c_int]),
+    ("gat_server_request_times", c_int, [c_p, c_i64, P_i64]),
+    ("gat_server_release", c_int, [c_p, c_i64]),
+    ("gat_server_stats", c_int, [c_p, P_i64]),
     ("gat_gen_lengths", c_int, [c_int, c_int, c_d, c_d, c_int, c_int, c_u64, P_i32]),
     ("gat_gen_walks", c_int, [c_int, P_i32, P_f32, c_d, c_u64, P_f32, P_f32]),
     ("gat_gen_boxes", c_int, [c_int, c_int, c_d, c_d, P_f32, c_u64, P_f32]),

@@ -95,6 +95,9 @@ class Context:
             # indexes first, then trajectory sets: native handles must not outlive the context
             kids = list(self._children)
             for o in kids:
+                if isinstance(o, Server):
+                    o.close()
+            for o in kids:
                 if isinstance(o, Index):
                     o.close()
             for o in kids:
@@ -270,6 +273,95 @@ def edr_pairs(ctx: Context, q_len, q_xy, c_len, c_xy, eps: float) -> np.ndarray:
                                 _p(cl, L.P_i32), _p(co, L.P_i64), _p(ca, L.P_f32), ca.shape[0], eps, _p(out, L.P_i32)),
               "gat_edr_pairs")
     return out
+
+
+class Server:
+    """The serving loop (gat_server_*): continuous batching of range and top-k requests over the
+    given device-resident indexes, admitted by a device-memory budget."""
+
+    def __init__(self, ctx: Context, grid: Index | None = None, stig: Index | None = None, fsg: Index | None = None,
+                 lanes: int = 4, budget_bytes: int = 40 << 30, max_range_batch: int = 4096, max_topk_batch: int = 32):
+        self.ctx = ctx
+        self.h = None
+        cfg = L.ServerConfig(lanes, budget_bytes, max_range_batch, max_topk_batch)
+        h = C.c_void_p()
+        hs = [x.h if x is not None else None for x in (grid, stig, fsg)]
+        ctx.check(lib.gat_server_create(ctx.h, hs[0], hs[1], hs[2], C.byref(cfg), C.byref(h)), "gat_server_create")
+        self.h = h
+        self._keep = (grid, stig, fsg)
+        ctx.adopt(self)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib.gat_server_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit_range(self, box, index_kind: int = L.GAT_INDEX_GRID, result: str = "ids") -> int:
+        b = np.asarray(box, np.float32).reshape(4)
+        rid = C.c_int64(0)
+        kind = L.GAT_RESULT_IDS if result == "ids" else L.GAT_RESULT_POINTS
+        rc = lib.gat_server_submit_range(self.h, index_kind, L.MBB(*[float(v) for v in b]), kind, C.byref(rid))
+        if rc != L.GAT_OK:
+            raise GatError(rc, "gat_server_submit_range")
+        return int(rid.value)
+
+    def submit_topk(self, lon, lat, k: int, eps: float) -> int:
+        x, y = _c(lon, np.float32), _c(lat, np.float32)
+        rid = C.c_int64(0)
+        rc = lib.gat_server_submit_topk(self.h, len(x), _p(x, L.P_f32), _p(y, L.P_f32), k, eps, C.byref(rid))
+        if rc != L.GAT_OK:
+            raise GatError(rc, "gat_server_submit_topk")
+        return int(rid.value)
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> int:
+        """The request's own status (GAT_OK, GAT_ERR_OOM, ...)."""
+        st = C.c_int32(0)
+        rc = lib.gat_server_wait(self.h, rid, timeout_ms, C.byref(st))
+        if rc != L.GAT_OK:
+            raise GatError(rc, "gat_server_wait")
+        return int(st.value)
+
+    def range_result(self, rid: int, points: bool = False):
+        n = C.c_int64(0)
+        rc = lib.gat_server_range_result(self.h, rid, None, None, 0, C.byref(n))
+        if rc not in (L.GAT_OK, L.GAT_ERR_TRUNCATED):
+            raise GatError(rc, "gat_server_range_result")
+        t = np.zeros(max(1, n.value), np.int32)
+        p = np.zeros(max(1, n.value), np.int32)
+        rc = lib.gat_server_range_result(self.h, rid, _p(t, L.P_i32), _p(p, L.P_i32), n.value, C.byref(n))
+        if rc != L.GAT_OK:
+            raise GatError(rc, "gat_server_range_result")
+        return (t[:n.value], p[:n.value]) if points else t[:n.value]
+
+    def topk_result(self, rid: int, k: int):
+        ids, dist = np.zeros(k, np.int32), np.zeros(k, np.int32)
+        rc = lib.gat_server_topk_result(self.h, rid, _p(ids, L.P_i32), _p(dist, L.P_i32), k)
+        if rc != L.GAT_OK:
+            raise GatError(rc, "gat_server_topk_result")
+        return ids, dist
+
+    def times(self, rid: int) -> np.ndarray:
+        """(arrival, admission, completion) in ns since the server started."""
+        t = np.zeros(3, np.int64)
+        rc = lib.gat_server_request_times(self.h, rid, _p(t, L.P_i64))
+        if rc != L.GAT_OK:
+            raise GatError(rc, "gat_server_request_times")
+        return t
+
+    def release(self, rid: int) -> None:
+        rc = lib.gat_server_release(self.h, rid)
+        if rc != L.GAT_OK:
+            raise GatError(rc, "gat_server_release")
+
+    def stats(self) -> dict:
+        a = np.zeros(8, np.int64)
+        lib.gat_server_stats(self.h, _p(a, L.P_i64))
+        keys = ["submitted", "completed", "batches", "range_batches", "topk_batches", "peak_admitted_bytes",
+                "largest_batch", "failed"]
+        return dict(zip(keys, (int(v) for v in a)))
 
 
 class SystemTest:

@@ -80,6 +80,12 @@ int check_device_flag(gat_ctx* ctx, const char* what) {
     return fail(ctx, flag, std::string(what) + ": device reported status " + std::to_string(flag));
 }
 
+bool same_owner(const gat_ctx* owner, const gat_ctx* user) {
+    const gat_ctx* a = owner->root ? owner->root : owner;
+    const gat_ctx* b = user->root ? user->root : user;
+    return a == b;
+}
+
 int require_device(gat_ctx* ctx, const char* what) {
     if (ctx && ctx->device < 0) return fail(ctx, GAT_ERR_STATE, std::string(what) + ": host-only context has no device");
     return GAT_OK;
@@ -176,6 +182,28 @@ int gat_ctx_create(int device, gat_ctx** out) {
         return e == cudaErrorMemoryAllocation ? GAT_ERR_OOM : GAT_ERR_CUDA;
     }
     *out = c;
+    return GAT_OK;
+}
+
+int gat_ctx_create_worker(gat_ctx* parent, gat_ctx** out) {
+    if (!parent || !out) return GAT_ERR_ARG;
+    int rc = gat_ctx_create(parent->device < 0 ? -1 : parent->device, out);
+    if (rc != GAT_OK) return rc;
+    (*out)->root = parent->root ? parent->root : parent;
+    return GAT_OK;
+}
+
+int gat_ctx_trim(gat_ctx* ctx) {
+    if (!ctx) return GAT_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (ctx->device < 0) return GAT_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (size_t i = 0; i < ctx->slot_ptr.size(); i++) {
+        if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
+        ctx->slot_ptr[i] = nullptr;
+        ctx->slot_bytes[i] = 0;
+    }
     return GAT_OK;
 }
 

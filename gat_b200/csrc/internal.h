@@ -90,6 +90,7 @@ struct gat_ctx {
     double t_work[GAT_KERNEL_CLASSES] = {0, 0, 0};
     int64_t* h_pinned = nullptr; /* pinned host words for small D2H reads */
     /* EDR rows per lane: 0 = autotune per shape class (edr_tune), else fixed */
+    gat_ctx* root = nullptr; /* worker contexts: the context whose indexes they may use */
     int edr_rows = 0;
     std::map<uint64_t, int> edr_tune;
     uint64_t edr_epoch = 0; /* launches of the tiled EDR kernel; tags its carry words */
@@ -171,6 +172,9 @@ void timed_add_work(gat_ctx* ctx, int cls, double work);
 
 /* GAT_ERR_STATE for a host-only context (device -1) */
 int require_device(gat_ctx* ctx, const char* what);
+/* true when `user` may run queries on objects created through `owner` (the same context, or
+ * worker contexts of one parent) */
+bool same_owner(const gat_ctx* owner, const gat_ctx* user);
 
 /* smallest float >= eps (the reference compares |float diff| < (double)EPSILON) */
 float match_threshold(double eps);

@@ -602,7 +602,7 @@ int gat_range_query_dev(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_quer
         (result_kind != GAT_RESULT_IDS && result_kind != GAT_RESULT_POINTS) ||
         (exec != GAT_EXEC_PLAIN && exec != GAT_EXEC_BATCHED))
         return fail(ctx, GAT_ERR_ARG, "gat_range_query_dev: bad arguments");
-    if (ix->ctx != ctx) return fail(ctx, GAT_ERR_STATE, "gat_range_query_dev: index from another context");
+    if (!same_owner(ix->ctx, ctx)) return fail(ctx, GAT_ERR_STATE, "gat_range_query_dev: index from another context");
     if (int rq = require_device(ctx, "gat_range_query_dev")) return rq;
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
@@ -616,7 +616,7 @@ int gat_range_query(gat_ctx* ctx, const gat_index* ix, const gat_mbb* queries, i
         (result_kind != GAT_RESULT_IDS && result_kind != GAT_RESULT_POINTS) ||
         (exec != GAT_EXEC_PLAIN && exec != GAT_EXEC_BATCHED))
         return fail(ctx, GAT_ERR_ARG, "gat_range_query: bad arguments");
-    if (ix->ctx != ctx) return fail(ctx, GAT_ERR_STATE, "gat_range_query: index from another context");
+    if (!same_owner(ix->ctx, ctx)) return fail(ctx, GAT_ERR_STATE, "gat_range_query: index from another context");
     if (int rq = require_device(ctx, "gat_range_query")) return rq;
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);

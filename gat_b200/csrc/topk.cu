@@ -857,7 +857,7 @@ int topk_dev(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
 
 int check_grid(gat_ctx* ctx, const gat_index* g) {
     if (!g || g->kind != GAT_INDEX_GRID) return fail(ctx, GAT_ERR_STATE, "top-k needs a Grid index (it holds the FVTable)");
-    if (g->ctx != ctx) return fail(ctx, GAT_ERR_STATE, "index from another context");
+    if (!same_owner(g->ctx, ctx)) return fail(ctx, GAT_ERR_STATE, "index from another context");
     return GAT_OK;
 }
 

@@ -67,6 +67,13 @@ enum { GAT_EXEC_PLAIN = 0, GAT_EXEC_BATCHED = 1 };
 int gat_ctx_create(int device, gat_ctx** out);
 void gat_ctx_destroy(gat_ctx* ctx);
 const char* gat_last_error(const gat_ctx* ctx);
+/* A worker context (no counterpart in the reference): same device as parent, its own stream,
+ * scratch arena and lock, and it may run queries on the trajectory sets and indexes created
+ * through the parent, so several host threads can drive one device concurrently. Destroy
+ * workers before their parent. */
+int gat_ctx_create_worker(gat_ctx* parent, gat_ctx** out);
+/* Frees the context's scratch arena (it grows again on demand). */
+int gat_ctx_trim(gat_ctx* ctx);
 /* The cudaStream_t all work of the context is issued on (for event timing by callers). */
 void* gat_ctx_stream(gat_ctx* ctx);
 int gat_ctx_sync(gat_ctx* ctx);
@@ -183,6 +190,46 @@ int gat_topk(gat_ctx* ctx, const gat_index* grid, int nq, const int32_t* q_len,
 int gat_topk_dev(gat_ctx* ctx, const gat_index* grid, int nq, const int32_t* d_q_len,
                  const int64_t* d_q_off, const float* d_q_xy, int max_q_len, int k, double eps,
                  int exec, int32_t* d_ids, int32_t* d_dist, int64_t* stats);
+
+/* ---------------------------------------------------------------- serving (no counterpart in the reference) */
+/* A request loop over device-resident indexes with continuous batching: requests are submitted
+ * one at a time from any thread; a scheduler thread forms a batch whenever one of `lanes`
+ * worker contexts is free, from the queue whose head request is oldest (range requests grouped
+ * by index and result kind, top-k requests by eps), and admits it only while the estimated
+ * device bytes of all admitted batches stay within budget_bytes. Batches of different lanes
+ * overlap on the device. Results equal those of the same request run alone. */
+typedef struct gat_server gat_server;
+typedef struct {
+    int lanes;            /* worker contexts (streams) running batches concurrently; default 4 */
+    int64_t budget_bytes; /* device bytes for admitted batches' results and scratch; default 40 GiB */
+    int max_range_batch;  /* range requests per batch; default 4096 */
+    int max_topk_batch;   /* top-k requests per batch; default 32 */
+} gat_server_config;
+/* cfg may be NULL (defaults). Any index may be NULL except that range requests need the index
+ * they name and top-k requests need the grid. */
+int gat_server_create(gat_ctx* ctx, const gat_index* grid, const gat_index* stig, const gat_index* fsg,
+                      const gat_server_config* cfg, gat_server** out);
+/* Finishes every submitted request, then stops the threads and frees everything. */
+void gat_server_destroy(gat_server* server);
+int gat_server_submit_range(gat_server* server, int index_kind, gat_mbb box, int result_kind, int64_t* id);
+int gat_server_submit_topk(gat_server* server, int q_len, const float* lon, const float* lat, int k,
+                           double eps, int64_t* id);
+/* Waits for a request (timeout_ms < 0: no limit; GAT_ERR_TIMEOUT when it runs out); the
+ * request's own status goes to *req_status (GAT_ERR_OOM when it can never fit the budget). */
+int gat_server_wait(gat_server* server, int64_t id, int timeout_ms, int* req_status);
+/* Result of a finished range request: *count entries (GAT_ERR_TRUNCATED when capacity is
+ * smaller); pidx only for GAT_RESULT_POINTS requests. */
+int gat_server_range_result(gat_server* server, int64_t id, int32_t* tids, int32_t* pidx, int64_t capacity,
+                            int64_t* count);
+/* Result of a finished top-k request: k ids and distances sorted by (distance, id). */
+int gat_server_topk_result(gat_server* server, int64_t id, int32_t* ids, int32_t* dist, int capacity);
+/* Arrival, admission and completion times of a request, ns since the server started. */
+int gat_server_request_times(gat_server* server, int64_t id, int64_t t[3]);
+/* Forgets a finished request and its result. */
+int gat_server_release(gat_server* server, int64_t id);
+/* [0] submitted, [1] completed, [2] batches, [3] range batches, [4] top-k batches,
+ * [5] peak admitted bytes, [6] largest batch, [7] failed requests */
+int gat_server_stats(gat_server* server, int64_t stats[8]);
 
 /* ---------------------------------------------------------------- synthetic inputs */
 enum { GAT_LEN_UNIFORM = 0, GAT_LEN_LOGNORMAL = 1, GAT_LEN_LOGUNIFORM = 2 };
