@@ -6,7 +6,8 @@ Default workload (config 2 of the reference's benchmark set): plain EDR top-k si
 256 x 256 virtual grid (cell 0.0025 deg, virtual-cell shift 2), one query per launch sequence.
 A step is one pass over the 256 queries. Other workloads: --workload c1 (plain GT-quadtree range
 queries), c3 (batched range queries over the three indexes), c4 (batched EDR pairs), c5 (served
-mix of range and top-k requests through the serving loop at three offered loads).
+mix of range and top-k requests through the serving loop at three offered loads), c4k (batched
+top-k of 1024 long queries against the 1M-trajectory set).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
 
@@ -799,6 +800,106 @@ def run_reference_c4(args, world, rank):
     return line
 
 
+# ---------------------------------------------------------------- workload: config 4, top-k part
+C4K = dict(nq=1024, k=64, eps=5e-4, cell=0.0025, vparam=2, leaf_cap=512, check=8)
+
+
+def run_c4k(args, world, rank, local, td):
+    """Batched top-k: 1024 query walks with lengths log-U[16, 4096] (the pair length
+    distribution of config 4), k = 64, eps 5e-4, against the 1M-trajectory set of config 3 with
+    frequency-vector pruning (FV on 256 x 256 virtual cells: cell 0.0025, shift 2). A sample of
+    queries is checked against exhaustive EDR over the whole set (every pair on the GPU)."""
+    import torch
+
+    import gat_b200 as G
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    t, _ = D.config3(seed=0, n=args.c3_n, nq=1)
+    ctx = G.Context(local)
+    db = G.TrajectorySet(ctx, t)
+    grid = G.Grid(ctx, db, G.BOX, C4K["cell"], C4K["vparam"], C4K["leaf_cap"])
+    log("c4k set and grid", t.n, round(time.time() - t0, 1))
+    nq, k = args.c4k_queries, C4K["k"]
+    qlen = D.lengths(nq, L.GAT_LEN_LOGUNIFORM, 0, 0, 16, 4096, 41 + rank)
+    qs = D.walks(qlen, 42 + rank)
+    qoff = np.zeros(nq + 1, np.int64)
+    qoff[1:] = np.cumsum(qlen)
+    T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    d_len, d_off, d_xy = T(qlen.astype(np.int32)), T(qoff), T(np.stack([qs.lon, qs.lat], 1).astype(np.float32))
+    d_ids = torch.empty(nq * k, dtype=torch.int32, device=dev)
+    d_dist = torch.empty(nq * k, dtype=torch.int32, device=dev)
+    stats = np.zeros(4, np.int64)
+    H = Harness(ctx, dev)
+
+    def call():
+        stats[:] = 0
+        ctx.check(L.lib.gat_topk_dev(ctx.h, grid.h, nq, d_len.data_ptr(), d_off.data_ptr(), d_xy.data_ptr(), int(qlen.max()), k,
+                                     C4K["eps"], L.GAT_EXEC_BATCHED, d_ids.data_ptr(), d_dist.data_ptr(),
+                                     stats.ctypes.data_as(L.P_i64)), "gat_topk_dev")
+
+    for _ in range(args.warmup):
+        log("warmup", H.time(call))
+    ctx.set_timing(True)
+    l0 = ctx.launches
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = []
+    for _ in range(args.steps):
+        ms.append(H.time(call))
+        log("step", ms[-1], stats.tolist())
+    clk = clocks.stop()
+    edr = ctx.kernel_stats(L.GAT_KERNEL_EDR)
+    bnd = ctx.kernel_stats(L.GAT_KERNEL_BOUNDS)
+    ctx.set_timing(False)
+    launches = ctx.launches - l0
+    tot = max_over_ranks(td, sum(ms), dev)
+    ids = d_ids.cpu().numpy().reshape(nq, k)
+    dist = d_dist.cpu().numpy().reshape(nq, k)
+    # exhaustive check of a sample: EDR of the query against every trajectory of the set
+    d_B = T(np.stack([t.lon, t.lat], 1).astype(np.float32))
+    d_blen = T(t.lengths.astype(np.int32))
+    d_boff = T(t.offsets[:-1].astype(np.int64))
+    out = torch.empty(t.n, dtype=torch.int32, device=dev)
+    chk = np.random.default_rng(43).choice(nq, size=min(nq, args.c4k_check), replace=False)
+    ok = True
+    for i in chk:
+        a_len = torch.full((t.n,), int(qlen[i]), dtype=torch.int32, device=dev)
+        a_off = torch.full((t.n,), int(qoff[i]), dtype=torch.int64, device=dev)
+        ctx.check(L.lib.gat_edr_pairs_dev(ctx.h, t.n, a_len.data_ptr(), a_off.data_ptr(), d_xy.data_ptr(), d_blen.data_ptr(),
+                                          d_boff.data_ptr(), d_B.data_ptr(), C4K["eps"], out.data_ptr()), "gat_edr_pairs_dev")
+        ctx.sync()
+        d_all = out.cpu().numpy()
+        order = np.lexsort((np.arange(1, t.n + 1), d_all))[:k]
+        ok &= bool(np.array_equal(ids[i], order + 1) and np.array_equal(dist[i], d_all[order]))
+    log("exhaustive check", ok)
+    if rank != 0:
+        ctx.close()
+        return None
+    cells = edr["work"]
+    line = base_line(args, world, "top-k queries/s (batched, 1M-trajectory set)", "queries/s",
+                     nq * world * args.steps / (tot / 1e3), tot,
+                     {"workload": f"C4 top-k: {nq} query walks log-U[16,4096], k=64, eps 5e-4, against {t.n} walks "
+                                  "U[50,350]; FV 256x256 virtual cells (cell 0.0025, shift 2)",
+                      "l2": "flushed between steps (256 MiB write); set 3.2 GB", "parallelism": f"replicas x{world}"},
+                     dtype="int32")
+    line.update({
+        "gpu_launches": int(launches),
+        "pairs_evaluated_per_query": round(float(stats[0]) / nq, 1),
+        "pruned_fraction": round(1.0 - float(stats[0]) / (nq * t.n), 6),
+        "gcups_evaluated": round(cells / (edr["ms"] / 1e3) / 1e9, 2) if edr["ms"] else None,
+        "kernels": {"edr": edr, "bounds": bnd},
+        "roofline": edr_roofline(edr, clk),
+        "exhaustive_check": {"queries": int(len(chk)), "identical": ok},
+        "clocks": clk,
+    })
+    ctx.close()
+    return line
+
+
 # ---------------------------------------------------------------- workload: config 5
 C5 = dict(requests=4000, range_frac=0.7, loads=(0.25, 0.5, 0.8), lanes=4, budget=40 << 30, eps=5e-4)
 
@@ -953,7 +1054,7 @@ def run_c5(args, world, rank, local, td):
     return line
 
 
-WORKLOADS = {"c1": run_c1, "c2": None, "c3": run_c3, "c4": run_c4, "c5": run_c5}
+WORKLOADS = {"c1": run_c1, "c2": None, "c3": run_c3, "c4": run_c4, "c4k": run_c4k, "c5": run_c5}
 REFERENCE = {"c1": run_reference_c1, "c2": None, "c4": run_reference_c4}
 
 
@@ -963,7 +1064,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c4k", "c5"])
     ap.add_argument("--cpu-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=0, help="C2: use only the first N of the 256 queries")
@@ -972,6 +1073,8 @@ def main():
     ap.add_argument("--c3-n", type=int, default=C3["n"])
     ap.add_argument("--c3-plain-sample", type=int, default=2000)
     ap.add_argument("--c5-requests", type=int, default=C5["requests"])
+    ap.add_argument("--c4k-queries", type=int, default=C4K["nq"])
+    ap.add_argument("--c4k-check", type=int, default=C4K["check"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_env()
@@ -980,6 +1083,10 @@ def main():
         if args.workload == "c3":
             line = {"impl": "reference", "unavailable": "the reference's Grid build is O(trajectories x cells) in memset "
                     "(Grid.cpp:268-269); at 1M trajectories and 1M cells it does not finish in minutes"}
+        elif args.workload == "c4k":
+            line = {"impl": "reference", "unavailable": "the reference's Grid build over the 1M-trajectory set does not "
+                    "finish in minutes (Grid.cpp:268-269), and its GPU EDR kernel stops at 1024 points per side "
+                    "(kernel.cu:249-501) while these queries reach 4096"}
         elif args.workload == "c5":
             line = {"impl": "reference", "unavailable": "the reference has no serving loop, and its Grid build over the "
                     "1M-trajectory set does not finish in minutes (Grid.cpp:268-269)"}

@@ -172,6 +172,12 @@ void timed_add_work(gat_ctx* ctx, int cls, double work);
 
 /* GAT_ERR_STATE for a host-only context (device -1) */
 int require_device(gat_ctx* ctx, const char* what);
+/* Opts a kernel into `bytes` of dynamic shared memory when that (plus the kernel's few KB of
+ * static shared memory) could exceed the 48 KB default. */
+template <class K>
+inline void allow_smem(K kernel, size_t bytes) {
+    if (bytes > 40 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 /* true when `user` may run queries on objects created through `owner` (the same context, or
  * worker contexts of one parent) */
 bool same_owner(const gat_ctx* owner, const gat_ctx* user);

@@ -478,8 +478,7 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
     bool bm_in_smem = smem_bm <= 200 * 1024;
     int blocks_per_sm = 0;
     if (mode == GAT_RESULT_IDS) {
-        if (bm_in_smem && smem_bm > 48 * 1024)
-            cudaFuncSetAttribute(k_range_ids, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bm);
+        if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_range_ids, kThreads, bm_in_smem ? smem_bm : 0);
     } else {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_range_points, kThreads, 0);

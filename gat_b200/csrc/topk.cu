@@ -712,7 +712,7 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     int32_t* qfv_cnt = (int32_t*)(qfv + fvb);
     int32_t* qfv_n = (int32_t*)(qfv + 2 * fvb);
     size_t smem_fv = (size_t)pow2 * 12;
-    if (smem_fv > 48 * 1024) cudaFuncSetAttribute(k_query_fv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fv);
+    allow_smem(k_query_fv, smem_fv);
     k_query_fv<<<std::min(nq, ctx->sm_count * 4), 512, smem_fv, s>>>(g->grid, nq, d_q_len, d_q_off, d_q_xy, stride, pow2,
                                                                       qfv_cell, qfv_cnt, qfv_n);
     count_launch(ctx);
@@ -726,7 +726,7 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     k_near_bitmap<<<nq, kT, 0, s>>>(nq, vbits, qfv_cell, qfv_n, stride, nwords, near);
     count_launch(ctx);
     size_t smem_lb = (size_t)stride * 8;
-    if (smem_lb > 48 * 1024) cudaFuncSetAttribute(k_lower_bounds, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_lb);
+    allow_smem(k_lower_bounds, smem_lb);
     dim3 lgrid((n + kT - 1) / kT, nq);
     timed_begin(ctx, GAT_KERNEL_BOUNDS);
     k_lower_bounds<<<lgrid, kT, smem_lb, s>>>(n, nq, g->d_fv_off, g->d_fv_cell, g->d_fv_cnt, qfv_cell, qfv_cnt, qfv_n, stride,
@@ -751,12 +751,12 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     int32_t* sdist = slb + (size_t)nq * n;
     int* wprefix = (int*)(ws + (size_t)nq * WS_WORDS);
     size_t smem_h = (size_t)bins_lb * 4;
-    if (smem_h > 48 * 1024) cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_h);
+    allow_smem(k_sort_hist, smem_h);
     k_sort_hist<<<dim3(ntile, nq), kT, smem_h, s>>>(n, lb, bins_lb, ntile, H);
     count_launch(ctx);
     if ((st = scan_i64(ctx, H, H, (int64_t)nq * bins_lb * ntile)) != GAT_OK) return st;
     size_t smem_run = (size_t)bins_lb * 8;
-    if (smem_run > 48 * 1024) cudaFuncSetAttribute(k_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_run);
+    allow_smem(k_sort_scatter, smem_run);
     k_sort_scatter<<<dim3(ntile, nq), 32, smem_run, s>>>(n, lb, bins_lb, ntile, H, cand, slb);
     count_launch(ctx);
     /* the walk: a finished query costs nothing in later rounds, `rounds` covers the whole
@@ -777,7 +777,7 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     count_launch(ctx);
     int bins_d = max_q_len + db->maxlen + 2;
     size_t smem_d = (size_t)bins_d * 4;
-    if (smem_d > 48 * 1024) cudaFuncSetAttribute(k_walk_kth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_d);
+    allow_smem(k_walk_kth, smem_d);
     int rows_hint = std::min(max_q_len, db->maxlen);
     int max_cols = std::max(max_q_len, db->maxlen);
     WalkPairs src{n, nq, wprefix, ws, cand, d_q_len, d_q_off, d_q_xy, db->d_len, db->d_off, db->d_xy, sdist};
@@ -803,8 +803,8 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
         gbm = (uint32_t*)scratch(ctx, S_TOPK_DIST, (size_t)nq * words * 4, &st);
         if (!gbm) return st;
         smem_final = 0;
-    } else if (smem_final > 32 * 1024) {
-        cudaFuncSetAttribute(k_final, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_final);
+    } else {
+        allow_smem(k_final, smem_final);
     }
     k_final<<<nq, kT, smem_final, s>>>(n, k, words, gbm, cand, sdist, ws, d_ids, d_dist, ctx->d_flag);
     count_launch(ctx);

@@ -65,3 +65,20 @@ def test_k_larger_than_set(gpu_ctx):
     wi, wd, _ = o.topk(*t.points(3), 25, 5e-4, pruned=False)
     assert np.array_equal(ids[0], wi) and np.array_equal(dist[0], wd)
     assert np.all(ids[0, 20:] == -1)
+
+
+def test_long_queries_against_short_set(gpu_ctx):
+    """Query walks up to 4096 points (the pair lengths of the batched-EDR configuration) against
+    a set of shorter walks (U[50, 350], the batched-range configuration's set): the walk's
+    bound order and stop rule with k = 64, batched and plain, against the oracle."""
+    t = D.walks(D.lengths(20000, 0, 0, 0, 50, 350, 44), 44)
+    db = G.TrajectorySet(gpu_ctx, t)
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.0025, 2, 512)
+    o = po.OracleGrid(t, D.BOX, 0.0025, 2, 512)
+    ql = np.concatenate([[4096, 16], D.lengths(4, 2, 0, 0, 16, 4096, 45)]).astype(np.int32)
+    qs = D.walks(ql, 46)
+    for execution in ("batched", "plain"):
+        ids, dist, _ = g.topk(qs, 64, 5e-4, execution=execution)
+        for j in range(qs.n):
+            wi, wd, _ = o.topk(*qs.points(j + 1), 64, 5e-4)
+            assert np.array_equal(ids[j], wi) and np.array_equal(dist[j], wd), (execution, j, int(ql[j]))
