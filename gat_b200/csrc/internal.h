@@ -89,8 +89,8 @@ struct gat_ctx {
     int64_t t_launches[GAT_KERNEL_CLASSES] = {0, 0, 0};
     double t_work[GAT_KERNEL_CLASSES] = {0, 0, 0};
     int64_t* h_pinned = nullptr; /* pinned host words for small D2H reads */
-    /* EDR rows per lane: 0 = autotune per shape class (edr_tune), else fixed */
     gat_ctx* root = nullptr; /* worker contexts: the context whose indexes they may use */
+    /* EDR rows per lane: 0 = autotune per shape class (edr_tune), else fixed */
     int edr_rows = 0;
     std::map<uint64_t, int> edr_tune;
     uint64_t edr_epoch = 0; /* launches of the tiled EDR kernel; tags its carry words */
@@ -200,6 +200,7 @@ enum Slot {
     S_RANGE_OUT_T,
     S_RANGE_OUT_P,
     S_RANGE_CURSOR,
+    S_RANGE_OVF,
     S_RANGE_CSR,
     S_EDR_PAIRS,
     S_EDR_CARRY,

@@ -15,6 +15,7 @@
  * Plain execution runs the same pipeline once per query.
  */
 #include <algorithm>
+#include <climits>
 
 #include "internal.h"
 
@@ -147,10 +148,19 @@ __global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, 
     Box q = load_box(queries, qi);
     int64_t cnt = 0;
     int64_t w = ioff ? ioff[qi] : 0;
+    int last_e = -1;
+    /* ranges that continue the previous one (neighbouring leaves / cells are contiguous in the
+     * index's point order) extend it, so the scan sees fewer, longer ranges */
     auto emit = [&](int b, int e) {
         if (b >= e) return;
+        if (b == last_e && cnt > 0) {
+            if (ioff) items[w + cnt - 1].y = e;
+            last_e = e;
+            return;
+        }
         if (ioff) items[w + cnt] = make_int2(b, e);
         cnt++;
+        last_e = e;
     };
     bool ok = true;
     if (KIND == GAT_INDEX_GRID) ok = grid_walk(g, q, emit);
@@ -218,21 +228,25 @@ __device__ __forceinline__ void scan_range(const float* __restrict__ X, const fl
         if (in_box(q, __ldg(X + i), __ldg(Y + i))) hit(i);
 }
 
-/* ---------------------------------------------------------------- id sets */
-/* One CTA per query (grid-stride over queries): a bitmap of n+1 trajectory bits in shared
- * memory (or in a per-CTA global slice when it does not fit), set by every candidate hit,
- * then emitted in ascending id order into the arena. */
+/* ---------------------------------------------------------------- id sets, bitmap form */
+/* One CTA per query (grid-stride over the queries, or over qlist): a bitmap of n+1 trajectory
+ * bits in shared memory (or in a per-CTA global slice when it does not fit), set by every
+ * candidate hit, then emitted in ascending id order into the arena. Exact for any result
+ * size; its fixed cost is proportional to n, so it serves the queries the hash form below
+ * cannot hold. */
 __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, int nq, const int64_t* ioff,
                                                         const int2* items, const float* X, const float* Y,
                                                         const int32_t* tid, int words, uint32_t* gbitmap,
                                                         uint32_t* arena, int64_t cap, unsigned long long* cursor,
-                                                        int64_t* segbase, int64_t* segcnt, unsigned long long* work) {
+                                                        int64_t* segbase, int64_t* segcnt, unsigned long long* work,
+                                                        const int* qlist) {
     extern __shared__ uint32_t smem_bm[];
     __shared__ int sh[kThreads / 32 + 1];
     __shared__ unsigned long long base_sh;
     uint32_t* bm = gbitmap ? gbitmap + (size_t)blockIdx.x * words : smem_bm;
     int per = (words + kThreads - 1) / kThreads;
-    for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+    for (int j = blockIdx.x; j < nq; j += gridDim.x) {
+        const int qi = qlist ? qlist[j] : j;
         for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
         __syncthreads();
         Box q = load_box(queries, qi);
@@ -275,6 +289,184 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
                 }
             }
         }
+        __syncthreads();
+    }
+}
+
+/* ---------------------------------------------------------------- id sets, hash form */
+/* Queries are taken from a counter by persistent CTAs. Each warp scans one candidate point
+ * range at a time (128 points per step as float4 x / y / tid), tests MBB::pInBox, and inserts
+ * the trajectory id of every hit that starts a run (the previous point is not a hit of the
+ * same trajectory: a trajectory's points in one cell are contiguous in every index order)
+ * into an open-addressing set in shared memory. The set is then compacted (which also clears
+ * it), sorted (bitonic) and written to the arena. A query whose distinct ids exceed kHashMax
+ * goes on the overflow list for the bitmap kernel; the result is the same set either way. */
+constexpr int kHashBits = 13;
+constexpr int kHashSize = 1 << kHashBits; /* 32 KB of ids */
+constexpr int kHashMax = 4096;            /* distinct ids per query (load factor <= 1/2) */
+
+__device__ __forceinline__ void hs_insert(int* tab, int t, int* count, int* ovf) {
+    unsigned h = ((unsigned)t * 2654435761u) >> (32 - kHashBits);
+    for (int p = 0; p < 64; p++) {
+        int v = tab[h];
+        if (v == t) return;
+        if (v == -1) {
+            v = atomicCAS(&tab[h], -1, t);
+            if (v == -1) {
+                if (atomicAdd(count, 1) >= kHashMax) *ovf = 1;
+                return;
+            }
+            if (v == t) return;
+        }
+        h = (h + 1) & (kHashSize - 1);
+    }
+    *ovf = 1;
+}
+
+__global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queries, int nq, const int64_t* ioff,
+                                                         const int2* items, const float* __restrict__ X,
+                                                         const float* __restrict__ Y, const int32_t* __restrict__ tid,
+                                                         uint32_t* arena, int64_t cap, unsigned long long* ctr,
+                                                         int64_t* segbase, int64_t* segcnt, int* ovf_list,
+                                                         unsigned long long* work) {
+    extern __shared__ int hs_smem[];
+    int* tab = hs_smem;              /* kHashSize */
+    int* buf = hs_smem + kHashSize;  /* kHashMax sorted ids */
+    __shared__ int sh[kThreads / 32 + 1];
+    __shared__ int cnt_sh, ovf_sh, q_sh;
+    __shared__ unsigned long long base_sh;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
+    for (int i = threadIdx.x; i < kHashSize; i += blockDim.x) tab[i] = -1;
+    /* ctr: [0] arena cursor, [1] work bytes, [2] query counter, [3] overflow count */
+    for (;;) {
+        if (threadIdx.x == 0) {
+            q_sh = (int)atomicAdd(&ctr[2], 1ull);
+            cnt_sh = 0;
+            ovf_sh = 0;
+        }
+        __syncthreads();
+        const int qi = q_sh;
+        if (qi >= nq) break;
+        const Box q = load_box(queries, qi);
+        const int64_t i0 = ioff[qi], i1 = ioff[qi + 1];
+        unsigned long long cand = 0, hits = 0;
+        for (int64_t it = i0 + warp; it < i1; it += kThreads / 32) {
+            /* stop early once the set has overflowed (warp-uniform read) */
+            if (__shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
+            const int2 r = items[it];
+            if (lane == 0) cand += (unsigned long long)(r.y - r.x);
+            const int head_end = min(r.y, (r.x + 3) & ~3);
+            const int vb = head_end, ve = head_end + ((r.y - head_end) & ~3);
+            /* unaligned head and tail points: plain inserts */
+            for (int i = r.x + lane; i < head_end; i += 32)
+                if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
+                    hs_insert(tab, __ldg(tid + i), &cnt_sh, &ovf_sh);
+                    hits++;
+                }
+            for (int i = ve + lane; i < r.y; i += 32)
+                if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
+                    hs_insert(tab, __ldg(tid + i), &cnt_sh, &ovf_sh);
+                    hits++;
+                }
+            const float4* X4 = reinterpret_cast<const float4*>(X + vb);
+            const float4* Y4 = reinterpret_cast<const float4*>(Y + vb);
+            const int4* T4 = reinterpret_cast<const int4*>(tid + vb);
+            const int nv = (ve - vb) >> 2;
+            int carry = -1; /* tid of the last point of the previous step if it was a hit */
+            /* the next step's x / y are loaded before the current step is tested */
+            float4 nx = make_float4(0.f, 0.f, 0.f, 0.f), ny = nx;
+            if (lane < nv) {
+                nx = __ldg(X4 + lane);
+                ny = __ldg(Y4 + lane);
+            }
+            for (int k0 = 0; k0 < nv; k0 += 32) {
+                const int k = k0 + lane;
+                const float4 x = nx, y = ny;
+                if (k + 32 < nv) {
+                    nx = __ldg(X4 + k + 32);
+                    ny = __ldg(Y4 + k + 32);
+                }
+                int t0 = -1, t1 = -1, t2 = -1, t3 = -1;
+                if (k < nv) {
+                    const bool h0 = in_box(q, x.x, y.x), h1 = in_box(q, x.y, y.y);
+                    const bool h2 = in_box(q, x.z, y.z), h3 = in_box(q, x.w, y.w);
+                    if (h0 | h1 | h2 | h3) {
+                        const int4 tt = __ldg(T4 + k);
+                        t0 = h0 ? tt.x : -1;
+                        t1 = h1 ? tt.y : -1;
+                        t2 = h2 ? tt.z : -1;
+                        t3 = h3 ? tt.w : -1;
+                        hits += (unsigned long long)(h0 + h1 + h2 + h3);
+                    }
+                }
+                int prev = __shfl_up_sync(FULL, t3, 1);
+                if (lane == 0) prev = carry;
+                carry = __shfl_sync(FULL, t3, 31);
+                if (t0 >= 0 && t0 != prev) hs_insert(tab, t0, &cnt_sh, &ovf_sh);
+                if (t1 >= 0 && t1 != t0) hs_insert(tab, t1, &cnt_sh, &ovf_sh);
+                if (t2 >= 0 && t2 != t1) hs_insert(tab, t2, &cnt_sh, &ovf_sh);
+                if (t3 >= 0 && t3 != t2) hs_insert(tab, t3, &cnt_sh, &ovf_sh);
+            }
+        }
+        if (work) {
+            if (cand) atomicAdd(work, 8ull * cand);
+            if (hits) atomicAdd(work, 4ull * hits);
+        }
+        __syncthreads();
+        const bool overflow = ovf_sh != 0;
+        /* compact the set into buf (clearing it on the way) */
+        constexpr int per = kHashSize / kThreads;
+        int c = 0;
+        for (int w = 0; w < per; w++) c += tab[threadIdx.x * per + w] >= 0;
+        int m;
+        int pre = block_scan_excl(c, &m, sh);
+        for (int w = 0; w < per; w++) {
+            const int v = tab[threadIdx.x * per + w];
+            if (v >= 0) {
+                if (!overflow && pre < kHashMax) buf[pre] = v;
+                pre++;
+                tab[threadIdx.x * per + w] = -1;
+            }
+        }
+        if (overflow) {
+            if (threadIdx.x == 0) {
+                const int o = (int)atomicAdd(&ctr[3], 1ull);
+                ovf_list[o] = qi;
+                segcnt[qi] = 0;
+                segbase[qi] = 0;
+            }
+            __syncthreads();
+            continue;
+        }
+        /* bitonic sort of the m ids (padded to a power of two) */
+        int P = 1;
+        while (P < m) P <<= 1;
+        for (int i = m + threadIdx.x; i < P; i += blockDim.x) buf[i] = INT_MAX;
+        __syncthreads();
+        for (int kk = 2; kk <= P; kk <<= 1)
+            for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+                for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                    const int ixj = i ^ jj;
+                    if (ixj > i) {
+                        const int a = buf[i], b = buf[ixj];
+                        if ((a > b) == ((i & kk) == 0)) {
+                            buf[i] = b;
+                            buf[ixj] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        if (threadIdx.x == 0) {
+            base_sh = atomicAdd(&ctr[0], (unsigned long long)m);
+            segcnt[qi] = m;
+            segbase[qi] = (int64_t)base_sh;
+        }
+        __syncthreads();
+        const int64_t base = (int64_t)base_sh;
+        if (base + m <= cap)
+            for (int i = threadIdx.x; i < m; i += blockDim.x) arena[base + i] = (uint32_t)buf[i];
         __syncthreads();
     }
 }
@@ -473,50 +665,70 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
     int64_t* segcnt = (int64_t*)scratch(ctx, S_RANGE_SEGCNT, (nq + 1) * sizeof(int64_t), &st);
     unsigned long long* cursor = (unsigned long long*)scratch(ctx, S_RANGE_CURSOR, 64, &st);
     if (!segbase || !segcnt || !cursor) return st;
-    int words = (ix->db->n + 1 + 31) / 32;
-    size_t smem_bm = (size_t)words * 4;
-    bool bm_in_smem = smem_bm <= 200 * 1024;
-    int blocks_per_sm = 0;
+    int* ovf_list = (int*)scratch(ctx, S_RANGE_OVF, (size_t)(nq + 1) * sizeof(int), &st);
+    if (!ovf_list) return st;
+    const int words = (ix->db->n + 1 + 31) / 32;
+    const size_t smem_bm = (size_t)words * 4;
+    const bool bm_in_smem = smem_bm <= 200 * 1024;
+    const size_t smem_hs = (size_t)(kHashSize + kHashMax) * sizeof(int);
+    int grid_pts = 0, grid_hs = 0;
     if (mode == GAT_RESULT_IDS) {
-        if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_range_ids, kThreads, bm_in_smem ? smem_bm : 0);
+        allow_smem(k_range_hash, smem_hs);
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_hash, kThreads, smem_hs);
+        grid_hs = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
     } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_range_points, kThreads, 0);
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_points, kThreads, 0);
+        grid_pts = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
     }
-    int grid = std::max(1, std::min(nq, std::max(1, blocks_per_sm) * ctx->sm_count));
-    uint32_t* gbm = nullptr;
-    if (mode == GAT_RESULT_IDS && !bm_in_smem) {
-        gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, (size_t)grid * words * 4, &st);
-        if (!gbm) return st;
-    }
-    int key_bits = key_bits_of(ix);
+    const int key_bits = key_bits_of(ix);
     /* result arena: start from a size guess and grow once if the cursor overshoots */
     int64_t cap = std::max<int64_t>(1 << 20, (int64_t)nq * 256);
     for (int attempt = 0; attempt < 2; attempt++) {
         uint32_t* arena = (uint32_t*)scratch(ctx, S_RANGE_ARENA, (size_t)cap * 4, &st);
         if (!arena) return st;
         cap = (int64_t)(ctx->slot_bytes[S_RANGE_ARENA] / 4);
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 2 * sizeof(unsigned long long), s), "range");
+        /* cursor: [0] arena entries, [1] work bytes, [2] query counter, [3] overflowed queries */
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 4 * sizeof(unsigned long long), s), "range");
+        unsigned long long* work = ctx->timing ? cursor + 1 : nullptr;
         timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
         if (mode == GAT_RESULT_IDS)
-            k_range_ids<<<grid, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid,
-                                                                       words, gbm, arena, cap, cursor, segbase, segcnt,
-                                                                       ctx->timing ? cursor + 1 : nullptr);
+            k_range_hash<<<grid_hs, kThreads, smem_hs, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap,
+                                                           cursor, segbase, segcnt, ovf_list, work);
         else
-            k_range_points<<<grid, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits, arena,
-                                                     cap, cursor, segbase, segcnt);
+            k_range_points<<<grid_pts, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits,
+                                                         arena, cap, cursor, segbase, segcnt);
         timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
         count_launch(ctx);
         GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
         GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
-        int64_t used = ctx->h_pinned[0];
-        if (used <= cap) {
-            if (ctx->timing) {
-                GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 3, cursor + 1, 8, cudaMemcpyDeviceToHost, s), "range");
-                GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
-                timed_add_work(ctx, GAT_KERNEL_RANGE_SCAN, (double)ctx->h_pinned[3]);
+        const int64_t n_ovf = mode == GAT_RESULT_IDS ? ctx->h_pinned[3] : 0;
+        if (n_ovf > 0) {
+            /* queries with more distinct ids than the shared-memory set holds: bitmap form */
+            int per_sm = 0;
+            if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_ids, kThreads, bm_in_smem ? smem_bm : 0);
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_ovf, (int64_t)std::max(1, per_sm) * ctx->sm_count));
+            uint32_t* gbm = nullptr;
+            if (!bm_in_smem) {
+                gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, (size_t)grid * words * 4, &st);
+                if (!gbm) return st;
             }
+            timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
+            k_range_ids<<<grid, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, (int)n_ovf, ioff, items, ix->d_x, ix->d_y,
+                                                                        ix->d_tid, words, gbm, arena, cap, cursor, segbase,
+                                                                        segcnt, work, ovf_list);
+            timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
+            count_launch(ctx);
+            GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+            GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
+        }
+        const int64_t used = ctx->h_pinned[0];
+        if (used <= cap) {
+            if (ctx->timing) timed_add_work(ctx, GAT_KERNEL_RANGE_SCAN, (double)ctx->h_pinned[1]);
             break;
         }
         if (attempt == 1) return fail(ctx, GAT_ERR_OOM, "range: result arena overflow");

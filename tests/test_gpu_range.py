@@ -102,3 +102,21 @@ def test_tiny_leaf_cap_and_single_leaf(gpu_ctx):
         r = g.range_query(q)
         off, ids = o.range(q, 0)
         assert csr_equal(r.offsets, r.tids, off, ids)
+
+
+@pytest.mark.parametrize("kind", ["grid", "stig", "fsg"])
+def test_id_sets_beyond_shared_memory_set(gpu_ctx, c1, kind):
+    """Queries whose result holds more distinct trajectories than the kernel's shared-memory
+    set (4096) go to the bitmap form; mixed with small queries in one batch, every result must
+    still equal the oracle's, in any mix and order."""
+    t, q, db = c1
+    ix = {"grid": lambda: G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512), "stig": lambda: G.STIG(gpu_ctx, db, 512),
+          "fsg": lambda: G.FSG(gpu_ctx, db, D.BOX, 0.01)}[kind]()
+    o = {"grid": lambda: po.OracleGrid(t, D.BOX, 0.01, 2, 512), "stig": lambda: po.OracleSTIG(t, 512),
+         "fsg": lambda: po.OracleFSG(t, D.BOX, 0.01)}[kind]()
+    big = np.array([[121.0, 30.7, 122.0, 31.7], [121.0, 30.7, 121.7, 31.5], [121.2, 30.9, 122.0, 31.7]], np.float32)
+    qq = np.concatenate([q[:40], big[:1], q[40:80], big[1:], q[80:100]])
+    r = ix.range_query(qq)
+    off, ids = o.range(qq, 0)
+    assert np.array_equal(r.offsets, off) and np.array_equal(r.tids, ids)
+    assert off[41] - off[40] > 4096  # the whole-box query really overflows the set
