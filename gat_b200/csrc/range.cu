@@ -24,6 +24,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kStack = 96;
+constexpr int kChunk = 1024; /* candidate points per scan item */
 
 struct Box {
     float xmin, ymin, xmax, ymax;
@@ -148,24 +149,35 @@ __global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, 
     Box q = load_box(queries, qi);
     int64_t cnt = 0;
     int64_t w = ioff ? ioff[qi] : 0;
-    int last_e = -1;
-    /* ranges that continue the previous one (neighbouring leaves / cells are contiguous in the
-     * index's point order) extend it, so the scan sees fewer, longer ranges */
+    /* Ranges that continue the previous one (neighbouring leaves / cells are contiguous in the
+     * index's point order) are joined, and everything is cut into chunks of at most kChunk
+     * points ending on multiples of 4, so the warps of the scan get balanced, 16-byte-aligned
+     * pieces. Chunking only regroups the same points. */
+    int cur_b = -1, cur_e = -1;
+    auto flush = [&]() {
+        while (cur_b < cur_e) {
+            int e = cur_e;
+            if (e - cur_b > kChunk) e = (cur_b + kChunk) & ~3;
+            if (ioff) items[w + cnt] = make_int2(cur_b, e);
+            cnt++;
+            cur_b = e;
+        }
+    };
     auto emit = [&](int b, int e) {
         if (b >= e) return;
-        if (b == last_e && cnt > 0) {
-            if (ioff) items[w + cnt - 1].y = e;
-            last_e = e;
+        if (b == cur_e) {
+            cur_e = e;
             return;
         }
-        if (ioff) items[w + cnt] = make_int2(b, e);
-        cnt++;
-        last_e = e;
+        flush();
+        cur_b = b;
+        cur_e = e;
     };
     bool ok = true;
     if (KIND == GAT_INDEX_GRID) ok = grid_walk(g, q, emit);
     if (KIND == GAT_INDEX_STIG) ok = stig_walk(s, q, emit);
     if (KIND == GAT_INDEX_FSG) fsg_walk(f, q, emit);
+    flush();
     if (!ok) set_flag(flag, GAT_ERR_ARG);
     if (!ioff) icnt[qi] = cnt;
 }
@@ -245,6 +257,7 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
     __shared__ unsigned long long base_sh;
     uint32_t* bm = gbitmap ? gbitmap + (size_t)blockIdx.x * words : smem_bm;
     int per = (words + kThreads - 1) / kThreads;
+    unsigned long long my_work = 0; /* added once at exit */
     for (int j = blockIdx.x; j < nq; j += gridDim.x) {
         const int qi = qlist ? qlist[j] : j;
         for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
@@ -261,10 +274,7 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
             });
         }
         /* algorithmic bytes: x and y of every candidate point, the id of every hit */
-        if (work) {
-            if (threadIdx.x == 0) atomicAdd(work, 8ull * cand);
-            if (hits) atomicAdd(work, 4ull * hits);
-        }
+        my_work += (threadIdx.x == 0 ? 8ull * cand : 0ull) + 4ull * hits;
         __syncthreads();
         int w0 = threadIdx.x * per, w1 = min(words, w0 + per);
         int c = 0;
@@ -290,6 +300,10 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
             }
         }
         __syncthreads();
+    }
+    if (work) {
+        for (int o = 16; o > 0; o >>= 1) my_work += __shfl_down_sync(0xffffffffu, my_work, o);
+        if ((threadIdx.x & 31) == 0 && my_work) atomicAdd(work, my_work);
     }
 }
 
@@ -338,6 +352,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     for (int i = threadIdx.x; i < kHashSize; i += blockDim.x) tab[i] = -1;
+    unsigned long long my_work = 0; /* algorithmic bytes of this thread, added once at exit */
     /* ctr: [0] arena cursor, [1] work bytes, [2] query counter, [3] overflow count */
     for (;;) {
         if (threadIdx.x == 0) {
@@ -409,24 +424,22 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
                 if (t3 >= 0 && t3 != t2) hs_insert(tab, t3, &cnt_sh, &ovf_sh);
             }
         }
-        if (work) {
-            if (cand) atomicAdd(work, 8ull * cand);
-            if (hits) atomicAdd(work, 4ull * hits);
-        }
+        my_work += 8ull * cand + 4ull * hits;
         __syncthreads();
         const bool overflow = ovf_sh != 0;
         /* compact the set into buf (clearing it on the way) */
+        /* slots threadIdx.x + kThreads * w (consecutive threads, consecutive banks) */
         constexpr int per = kHashSize / kThreads;
         int c = 0;
-        for (int w = 0; w < per; w++) c += tab[threadIdx.x * per + w] >= 0;
+        for (int w = 0; w < per; w++) c += tab[threadIdx.x + kThreads * w] >= 0;
         int m;
         int pre = block_scan_excl(c, &m, sh);
         for (int w = 0; w < per; w++) {
-            const int v = tab[threadIdx.x * per + w];
+            const int v = tab[threadIdx.x + kThreads * w];
             if (v >= 0) {
                 if (!overflow && pre < kHashMax) buf[pre] = v;
                 pre++;
-                tab[threadIdx.x * per + w] = -1;
+                tab[threadIdx.x + kThreads * w] = -1;
             }
         }
         if (overflow) {
@@ -468,6 +481,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
         if (base + m <= cap)
             for (int i = threadIdx.x; i < m; i += blockDim.x) arena[base + i] = (uint32_t)buf[i];
         __syncthreads();
+    }
+    if (work) {
+        for (int o = 16; o > 0; o >>= 1) my_work += __shfl_down_sync(FULL, my_work, o);
+        if (lane == 0 && my_work) atomicAdd(work, my_work);
     }
 }
 
