@@ -18,9 +18,23 @@ int cuda_fail(gat_ctx* ctx, cudaError_t e, const char* what) {
     return fail(ctx, e == cudaErrorMemoryAllocation ? GAT_ERR_OOM : GAT_ERR_CUDA, m);
 }
 
+void release_owned(gat_ctx* ctx) {
+    for (auto& o : ctx->owned) o.second(o.first);
+    ctx->owned.clear();
+}
+
 void* scratch(gat_ctx* ctx, int slot, size_t bytes, int* status) {
     if (bytes == 0) bytes = 256;
     if (ctx->slot_bytes[slot] >= bytes) return ctx->slot_ptr[slot];
+    if (ctx->device >= 0) {
+        /* a slot cannot move while a CUDA graph is being captured from this context */
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(ctx->stream, &cs);
+        if (cs != cudaStreamCaptureStatusNone) {
+            *status = fail(ctx, GAT_ERR_STATE, "scratch growth during graph capture");
+            return nullptr;
+        }
+    }
     if (ctx->slot_ptr[slot]) {
         cudaStreamSynchronize(ctx->stream);
         cudaFree(ctx->slot_ptr[slot]);
@@ -199,6 +213,7 @@ int gat_ctx_trim(gat_ctx* ctx) {
     if (ctx->device < 0) return GAT_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    release_owned(ctx);
     for (size_t i = 0; i < ctx->slot_ptr.size(); i++) {
         if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
         ctx->slot_ptr[i] = nullptr;
@@ -215,6 +230,7 @@ void gat_ctx_destroy(gat_ctx* ctx) {
     }
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    release_owned(ctx);
     drain_events(ctx);
     for (cudaEvent_t e : ctx->ev_free) cudaEventDestroy(e);
     for (void* p : ctx->slot_ptr)

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_edr(Src src, float u, int* __re
  * accepts a word whose tag is the one it expects, so the hand-over needs neither a progress
  * flag nor a memory fence: a 64-bit store is seen whole or not at all. Values are the
  * column-shifted distances E = D - c, which lie in [-16384, 16384] and fit 16 bits; epochs
- * only grow (2^40 launches before a repeat), and carry buffers are zeroed when allocated, so a
+ * come from a per-context device counter and only grow (2^40 launches before a repeat), and carry buffers are zeroed when allocated, so a
  * stale word never carries the expected tag. A tile rewrites the buffer its predecessor read
  * (double buffering per pair) only for columns that predecessor has already consumed.
  *
@@ -218,8 +218,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_edr(Src src, float u, int* __re
 constexpr int kSpinLimit = 1 << 22;
 constexpr int kClasses = 48;
 /* counter block: [0] item counter, [1] cooperative slots taken, [2] total items,
- * [4, 4 + kClasses) items per class, [4 + kClasses, 4 + 2 kClasses) class cursors */
-constexpr int kCtrWords = 4 + 2 * kClasses;
+ * [4, 4 + kClasses) items per class, [4 + kClasses, 4 + 2 kClasses) class cursors, then the
+ * launch's epoch (64-bit, 8-byte aligned) */
+constexpr int kCtrEpoch = 4 + 2 * kClasses;
+constexpr int kCtrWords = kCtrEpoch + 2;
 typedef unsigned long long carry_t;
 
 struct TileCtl {
@@ -228,7 +230,7 @@ struct TileCtl {
     carry_t* pair_carry; /* cooperative slot s: rows pair_carry + s * 2 * stride */
     carry_t* warp_carry; /* per-warp double carry rows for single-warp pairs */
     int stride;
-    unsigned long long epoch;
+    const unsigned long long* epoch; /* written by the schedule's write pass */
     int32_t* flag;
 };
 
@@ -285,7 +287,7 @@ __global__ void k_sched_count(Src src, int cap, int coop_cap, int* __restrict__ 
 
 template <class Src>
 __global__ void k_sched_write(Src src, int cap, int* __restrict__ ctr, const int2* __restrict__ meta,
-                              int4* __restrict__ items) {
+                              int4* __restrict__ items, unsigned long long* __restrict__ epochs) {
     __shared__ int off[kClasses];
     __shared__ int lcnt[kClasses];
     __shared__ int lbase[kClasses];
@@ -295,7 +297,12 @@ __global__ void k_sched_write(Src src, int cap, int* __restrict__ ctr, const int
             off[c] = acc;
             acc += ctr[4 + c];
         }
-        if (blockIdx.x == 0) ctr[2] = acc;
+        if (blockIdx.x == 0) {
+            ctr[2] = acc;
+            /* a fresh epoch per launch from the context's device counter, so launches replayed
+             * from a CUDA graph never reuse a tag */
+            *reinterpret_cast<unsigned long long*>(ctr + kCtrEpoch) = atomicAdd(epochs, 1ull) + 1ull;
+        }
     }
     const int n = min(src.count(), cap);
     /* block-sized chunks (uniform trip count over the block) so the local counters reset */
@@ -495,7 +502,7 @@ __global__ void __launch_bounds__(kWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(Src s
     const int gw = blockIdx.x * kWarps + wib;
     carry_t* wc0 = ctl.warp_carry + (size_t)gw * 2 * ctl.stride;
     carry_t* wc1 = wc0 + ctl.stride;
-    const carry_t ep = ctl.epoch << 8;
+    const carry_t ep = *ctl.epoch << 8;
     const unsigned total = (unsigned)*ctl.total;
     for (;;) {
         unsigned idx = 0;
@@ -590,10 +597,10 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->sm_count * 8));
     k_sched_count<R, Src><<<pgrid, 256, 0, s>>>(src, (int)cap, (int)coop, ctr, meta);
     count_launch(ctx);
-    k_sched_write<Src><<<pgrid, 256, 0, s>>>(src, (int)cap, ctr, meta, items);
+    k_sched_write<Src><<<pgrid, 256, 0, s>>>(src, (int)cap, ctr, meta, items, edr_epochs(ctx));
     count_launch(ctx);
-    ctx->edr_epoch++;
-    TileCtl ctl{items, ctr + 2, pcarry, wcarry, stride, (unsigned long long)ctx->edr_epoch, ctx->d_flag};
+    TileCtl ctl{items, ctr + 2, pcarry, wcarry, stride, reinterpret_cast<const unsigned long long*>(ctr + kCtrEpoch),
+                ctx->d_flag};
     timed_begin(ctx, GAT_KERNEL_EDR);
     if (ev0) cudaEventRecord(ev0, s);
     k_edr_tiles<R, Src><<<grid, kWarps * 32, 0, s>>>(src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);

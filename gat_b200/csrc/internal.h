@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <string>
@@ -80,7 +81,8 @@ struct gat_ctx {
     std::vector<void*> slot_ptr;
     std::vector<size_t> slot_bytes;
     std::vector<char> slot_fresh; /* allocated since the last scratch_zeroed clear */
-    int32_t* d_flag = nullptr; /* [0] device status written by kernels (0 = ok), [1] sink word */
+    int32_t* d_flag = nullptr; /* [0] device status written by kernels (0 = ok), [1] sink word,
+                                  [4..5] EDR launch epochs (64-bit counter) */
     /* optional per-kernel-class event timing (gat_ctx_set_timing) */
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[GAT_KERNEL_CLASSES];
@@ -93,7 +95,9 @@ struct gat_ctx {
     /* EDR rows per lane: 0 = autotune per shape class (edr_tune), else fixed */
     int edr_rows = 0;
     std::map<uint64_t, int> edr_tune;
-    uint64_t edr_epoch = 0; /* launches of the tiled EDR kernel; tags its carry words */
+    /* objects that hold device memory of this context's scratch or workers (cached CUDA graphs);
+     * released first by gat_ctx_destroy and gat_ctx_trim */
+    std::vector<std::pair<void*, void (*)(void*)>> owned;
 };
 
 struct gat_db {
@@ -144,6 +148,8 @@ int fail(gat_ctx* ctx, int code, const std::string& msg);
 int cuda_fail(gat_ctx* ctx, cudaError_t e, const char* what);
 /* device scratch slot of at least `bytes` bytes; contents undefined */
 void* scratch(gat_ctx* ctx, int slot, size_t bytes, int* status);
+/* releases the context's owned objects (cached graphs and their workers) */
+void release_owned(gat_ctx* ctx);
 /* same, but a slot that was (re)allocated is cleared to zero (on the context stream) first */
 void* scratch_zeroed(gat_ctx* ctx, int slot, size_t bytes, int* status);
 /* cudaMalloc tracked by an index (freed by gat_index_destroy) */
@@ -182,6 +188,8 @@ inline void allow_smem(K kernel, size_t bytes) {
  * worker contexts of one parent) */
 bool same_owner(const gat_ctx* owner, const gat_ctx* user);
 
+/* the context's device counter of tiled-EDR launches (tags carry words) */
+inline unsigned long long* edr_epochs(gat_ctx* ctx) { return reinterpret_cast<unsigned long long*>(ctx->d_flag + 4); }
 /* smallest float >= eps (the reference compares |float diff| < (double)EPSILON) */
 float match_threshold(double eps);
 
@@ -209,6 +217,7 @@ enum Slot {
     S_EDR_ITEMS,
     S_EDR_PCARRY,
     S_EDR_META,
+    S_TOPK_GSTAGE,
     S_TOPK_QFV,
     S_TOPK_LB,
     S_TOPK_PAIRS,

@@ -588,7 +588,8 @@ __global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* sl
 /* k smallest (distance, id) over the evaluated prefix: the pairs below W sorted, then the
  * smallest ids at W (a bitmap over ids in shared memory or a per-CTA global slice). */
 __global__ void k_final(int n, int k, int words, uint32_t* gbitmap, const int32_t* cand, const int32_t* sdist,
-                        const int32_t* ws, int32_t* out_ids, int32_t* out_dist, int32_t* flag) {
+                        const int32_t* ws, int32_t* out_ids, int32_t* out_dist, int32_t* flag,
+                        unsigned long long* pairs) {
     extern __shared__ uint32_t bm_s[];
     __shared__ unsigned long long lt_keys[1024];
     __shared__ int lt_n;
@@ -598,6 +599,7 @@ __global__ void k_final(int n, int k, int words, uint32_t* gbitmap, const int32_
     const int32_t* s = ws + (size_t)qi * WS_WORDS;
     if (threadIdx.x == 0 && !s[WS_DONE]) atomicCAS(flag, 0, GAT_ERR_STATE);
     const int W = s[WS_W], end = s[WS_END];
+    if (threadIdx.x == 0) atomicAdd(pairs, (unsigned long long)end); /* pairs evaluated */
     const int32_t* dist = sdist + (size_t)qi * n;
     const int32_t* ids = cand + (size_t)qi * n;
     for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0;
@@ -681,26 +683,41 @@ __global__ void k_final(int n, int k, int words, uint32_t* gbitmap, const int32_
     }
 }
 
-int read_word(gat_ctx* ctx, const void* d, int64_t* v) {
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, d, 8, cudaMemcpyDeviceToHost, ctx->stream), "top-k");
-    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "top-k");
-    *v = ctx->h_pinned[0];
-    return GAT_OK;
-}
-
 /* device bytes topk_batch needs per query (sorted candidates, bounds, distances, histograms) */
 size_t topk_bytes_per_query(int n, int bins) {
     int ntile = (n + kSortTile - 1) / kSortTile;
     return (size_t)(n + 1) * 4 + (size_t)n * 12 + (size_t)bins * ntile * 8 + 64;
 }
 
-/* the whole pipeline for queries [0, nq) of the given device arrays */
-int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, const int64_t* d_q_off,
-               const float2* d_q_xy, int max_q_len, int k, float u, int32_t* d_ids, int32_t* d_dist, int64_t* stats) {
+/* State of one batch between its phases (pointers into the context's scratch). */
+struct TopkRun {
+    const gat_index* g = nullptr;
+    int nq = 0, n = 0, k = 0, max_q_len = 0;
+    float u = 0.f;
+    int32_t* lb = nullptr;
+    int32_t *cand = nullptr, *slb = nullptr, *sdist = nullptr, *ws = nullptr;
+    int* wprefix = nullptr;
+    bool lone = false;
+    int chunk0 = 0, growth = 0, rounds = 0;
+    int bins_d = 0;
+    size_t smem_d = 0;
+    int rows_hint = 0, max_cols = 0;
+    WalkPairs src{};
+};
+
+/* Phase 1: query frequency vectors, lower bounds, candidate order, walk state. */
+int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, const int64_t* d_q_off,
+             const float2* d_q_xy, int max_q_len, int k, float u, int64_t* stats, TopkRun& R) {
     cudaStream_t s = ctx->stream;
     const gat_db* db = g->db;
     int n = db->n;
     int st = GAT_OK;
+    R.g = g;
+    R.nq = nq;
+    R.n = n;
+    R.k = k;
+    R.u = u;
+    R.max_q_len = max_q_len;
     int stride = std::max(1, max_q_len);
     int pow2 = 1;
     while (pow2 < max_q_len) pow2 <<= 1;
@@ -719,6 +736,7 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     /* lower bounds */
     int32_t* lb = (int32_t*)scratch(ctx, S_TOPK_LB, (size_t)nq * (n + 1) * 4, &st);
     if (!lb) return st;
+    R.lb = lb;
     int vbits = (int)std::log2((double)(g->grid.cellnum >> 2));
     int nwords = ((1 << vbits) + 31) / 32;
     uint32_t* near = (uint32_t*)scratch(ctx, S_TOPK_NEAR, (size_t)nq * nwords * 4 + 64, &st);
@@ -735,21 +753,19 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
      * per query */
     timed_end(ctx, GAT_KERNEL_BOUNDS, (double)nq * ((double)g->fv_entries * 8.0 + (double)n * 12.0));
     count_launch(ctx);
-    if (stats && stats[3] == -1) { /* bounds only */
-        return check_device_flag(ctx, "frequency-vector bounds");
-    }
+    if (stats && stats[3] == -1) return GAT_OK; /* bounds only */
     /* candidate order */
     int bins_lb = std::max(max_q_len, db->maxlen) + 2;
     int ntile = (n + kSortTile - 1) / kSortTile;
     int64_t* H = (int64_t*)scratch(ctx, S_TOPK_SEG, (size_t)nq * bins_lb * ntile * 8 + 64, &st);
     char* sorted = (char*)scratch(ctx, S_TOPK_PAIRS, (size_t)nq * n * 12 + 1024, &st);
     int32_t* ws = (int32_t*)scratch(ctx, S_TOPK_QSTATE, (size_t)nq * WS_WORDS * 4 + (size_t)(nq + 1) * 4 + 256, &st);
-    unsigned long long* cells = (unsigned long long*)scratch(ctx, S_TOPK_IO, 256, &st);
-    if (!H || !sorted || !ws || !cells) return st;
-    int32_t* cand = (int32_t*)sorted;
-    int32_t* slb = cand + (size_t)nq * n;
-    int32_t* sdist = slb + (size_t)nq * n;
-    int* wprefix = (int*)(ws + (size_t)nq * WS_WORDS);
+    if (!H || !sorted || !ws) return st;
+    R.cand = (int32_t*)sorted;
+    R.slb = R.cand + (size_t)nq * n;
+    R.sdist = R.slb + (size_t)nq * n;
+    R.ws = ws;
+    R.wprefix = (int*)(ws + (size_t)nq * WS_WORDS);
     size_t smem_h = (size_t)bins_lb * 4;
     allow_smem(k_sort_hist, smem_h);
     k_sort_hist<<<dim3(ntile, nq), kT, smem_h, s>>>(n, lb, bins_lb, ntile, H);
@@ -757,71 +773,422 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
     if ((st = scan_i64(ctx, H, H, (int64_t)nq * bins_lb * ntile)) != GAT_OK) return st;
     size_t smem_run = (size_t)bins_lb * 8;
     allow_smem(k_sort_scatter, smem_run);
-    k_sort_scatter<<<dim3(ntile, nq), 32, smem_run, s>>>(n, lb, bins_lb, ntile, H, cand, slb);
+    k_sort_scatter<<<dim3(ntile, nq), 32, smem_run, s>>>(n, lb, bins_lb, ntile, H, R.cand, R.slb);
     count_launch(ctx);
-    /* the walk: a finished query costs nothing in later rounds, `rounds` covers the whole
-     * order with growing chunks, and the loop ends early once no query extends */
-    /* a lone query leaves most of the GPU idle in a small round, so it starts with a larger
-     * chunk and grows faster; a batch keeps rounds tight to limit surplus evaluations */
-    const bool lone = nq <= 4;
-    int chunk0 = lone ? std::max(8 * k, 1024) : std::max(4 * k, 128);
-    int growth = lone ? 4 : 2;
-    int rounds = 1;
-    for (int64_t cover = chunk0, c = chunk0; cover < n; rounds++) {
-        c *= growth;
+    /* the walk: a finished query costs nothing in later rounds and `rounds` covers the whole
+     * order with growing chunks. A lone query leaves most of the GPU idle in a small round, so
+     * it starts with a larger chunk and grows faster; a batch keeps rounds tight to limit
+     * surplus evaluations. */
+    R.lone = nq <= 4;
+    R.chunk0 = R.lone ? std::max(8 * k, 1024) : std::max(4 * k, 128);
+    R.growth = R.lone ? 4 : 2;
+    R.rounds = 1;
+    for (int64_t cover = R.chunk0, c = R.chunk0; cover < n; R.rounds++) {
+        c *= R.growth;
         cover += c;
     }
-    rounds += 1;
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(cells, 0, 8, s), "top-k");
-    k_walk_init<<<(nq + 127) / 128, 128, 0, s>>>(nq, chunk0, ws);
+    R.rounds += 1;
+    k_walk_init<<<(nq + 127) / 128, 128, 0, s>>>(nq, R.chunk0, ws);
     count_launch(ctx);
-    int bins_d = max_q_len + db->maxlen + 2;
-    size_t smem_d = (size_t)bins_d * 4;
-    allow_smem(k_walk_kth, smem_d);
-    int rows_hint = std::min(max_q_len, db->maxlen);
-    int max_cols = std::max(max_q_len, db->maxlen);
-    WalkPairs src{n, nq, wprefix, ws, cand, d_q_len, d_q_off, d_q_xy, db->d_len, db->d_off, db->d_xy, sdist};
-    for (int r = 0; r < rounds; r++) {
-        k_walk_plan<<<1, 1024, 0, s>>>(n, nq, slb, ws, wprefix);
-        count_launch(ctx);
-        /* the round's pair count sizes the EDR launch exactly; it is zero once no query can
-         * extend (every query at the end of its order or with its next bound above W) */
-        int32_t* cnt = reinterpret_cast<int32_t*>(ctx->h_pinned + 4);
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, wprefix + nq, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "top-k");
-        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "top-k");
-        const int64_t npairs = *cnt;
-        if (npairs == 0) break;
-        if ((st = edr::edr_launch(ctx, src, npairs, rows_hint, max_cols, u, cells)) != GAT_OK) return st;
-        k_walk_kth<<<nq, kT, smem_d, s>>>(n, k, bins_d, growth, slb, cand, sdist, ws);
-        count_launch(ctx);
-    }
-    /* selection */
-    int words = (n + 1 + 31) / 32;
+    R.bins_d = max_q_len + db->maxlen + 2;
+    R.smem_d = (size_t)R.bins_d * 4;
+    allow_smem(k_walk_kth, R.smem_d);
+    R.rows_hint = std::min(max_q_len, db->maxlen);
+    R.max_cols = std::max(max_q_len, db->maxlen);
+    R.src = WalkPairs{n, nq, R.wprefix, ws, R.cand, d_q_len, d_q_off, d_q_xy, db->d_len, db->d_off, db->d_xy, R.sdist};
+    return GAT_OK;
+}
+
+/* Phase 2a: each unfinished query extends its evaluated prefix (pair numbering in wprefix). */
+void topk_plan(gat_ctx* ctx, const TopkRun& R) {
+    k_walk_plan<<<1, 1024, 0, ctx->stream>>>(R.n, R.nq, R.slb, R.ws, R.wprefix);
+    count_launch(ctx);
+}
+
+/* Phase 2b: EDR of the planned pairs (at most npairs), then the k-th distance and stop rule. */
+int topk_round(gat_ctx* ctx, const TopkRun& R, int64_t npairs, unsigned long long* cells) {
+    int st = edr::edr_launch(ctx, R.src, npairs, R.rows_hint, R.max_cols, R.u, cells);
+    if (st != GAT_OK) return st;
+    k_walk_kth<<<R.nq, kT, R.smem_d, ctx->stream>>>(R.n, R.k, R.bins_d, R.growth, R.slb, R.cand, R.sdist, R.ws);
+    count_launch(ctx);
+    return GAT_OK;
+}
+
+/* Phase 3: the k smallest (distance, id) pairs per query. */
+int topk_post(gat_ctx* ctx, const TopkRun& R, int32_t* d_ids, int32_t* d_dist, unsigned long long* pairs) {
+    int st = GAT_OK;
+    int words = (R.n + 1 + 31) / 32;
     uint32_t* gbm = nullptr;
     size_t smem_final = (size_t)words * 4;
     if (smem_final > 160 * 1024) {
-        gbm = (uint32_t*)scratch(ctx, S_TOPK_DIST, (size_t)nq * words * 4, &st);
+        gbm = (uint32_t*)scratch(ctx, S_TOPK_DIST, (size_t)R.nq * words * 4, &st);
         if (!gbm) return st;
         smem_final = 0;
     } else {
         allow_smem(k_final, smem_final);
     }
-    k_final<<<nq, kT, smem_final, s>>>(n, k, words, gbm, cand, sdist, ws, d_ids, d_dist, ctx->d_flag);
+    k_final<<<R.nq, kT, smem_final, ctx->stream>>>(R.n, R.k, words, gbm, R.cand, R.sdist, R.ws, d_ids, d_dist, ctx->d_flag,
+                                                   pairs);
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "top-k launch");
-    if (stats || ctx->timing) {
-        /* pairs evaluated = sum of the evaluated prefixes */
-        std::vector<int32_t> h((size_t)nq * WS_WORDS);
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), ws, h.size() * 4, cudaMemcpyDeviceToHost, s), "top-k");
-        int64_t c = 0;
-        if ((st = read_word(ctx, cells, &c)) != GAT_OK) return st;
-        timed_add_work(ctx, GAT_KERNEL_EDR, (double)c);
-        if (stats) {
-            for (int q = 0; q < nq; q++) stats[0] += h[(size_t)q * WS_WORDS + WS_END];
-            stats[1] += c;
+    return GAT_OK;
+}
+
+/* The whole pipeline for queries [0, nq) of the given device arrays. acc: device counters
+ * [0] DP cells, [1] pairs evaluated, accumulated over calls; status and counters are read by
+ * the caller once per API call. */
+int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, const int64_t* d_q_off,
+               const float2* d_q_xy, int max_q_len, int k, float u, int32_t* d_ids, int32_t* d_dist, int64_t* stats,
+               unsigned long long* acc) {
+    TopkRun R;
+    int st = topk_pre(ctx, g, nq, d_q_len, d_q_off, d_q_xy, max_q_len, k, u, stats, R);
+    if (st != GAT_OK) return st;
+    if (stats && stats[3] == -1) return check_device_flag(ctx, "frequency-vector bounds");
+    /* A lone query's first rounds are launched without a host round trip, sized by their upper
+     * bound (each query extends by at most its chunk; a finished query adds no pairs and the
+     * kernels of an empty round exit at once). Later rounds, and every round of a batch, read
+     * the exact pair count first; it is zero once no query can extend (every query at the end
+     * of its order or with its next bound above W). */
+    const int blind_rounds = R.lone ? 2 : 0;
+    int64_t chunk_r = R.chunk0;
+    for (int r = 0; r < R.rounds; r++) {
+        topk_plan(ctx, R);
+        int64_t npairs = std::min<int64_t>((int64_t)nq * chunk_r, (int64_t)nq * R.n);
+        if (r >= blind_rounds) {
+            int32_t* cnt = reinterpret_cast<int32_t*>(ctx->h_pinned + 4);
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, R.wprefix + nq, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream),
+                         "top-k");
+            GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "top-k");
+            npairs = *cnt;
+            if (npairs == 0) break;
         }
+        if ((st = topk_round(ctx, R, npairs, acc)) != GAT_OK) return st;
+        chunk_r = std::min<int64_t>(chunk_r * R.growth, (int64_t)1 << 30);
     }
-    return check_device_flag(ctx, "top-k");
+    return topk_post(ctx, R, d_ids, d_dist, acc + 1);
+}
+
+/* ---------------------------------------------------------------- lone queries as a CUDA graph */
+/* One query of the plain form is a chain of ~20 small launches with data-dependent rounds.
+ * Launched one by one from the host, the chain waits on launch latency and on a host read of
+ * each round's size. Instead the whole chain of one query is a CUDA graph: a stage kernel takes
+ * the next query index from a device counter and copies that query into fixed buffers; the
+ * bound / order kernels follow; the walk rounds sit in a conditional while node whose
+ * condition the last kernel of each round sets from the query's done flag; the selection and
+ * an unstage kernel write the k results to the caller's arrays. The host launches the graph
+ * once per query with no synchronisation in between. Every buffer the graph touches belongs
+ * to a worker context used by nothing else, sized by a first, uncaptured run of the same
+ * kernels, so no pointer in the graph moves. EDR rounds are sized for the whole set (empty
+ * slots cost nothing) and use a fixed tile height (no host-side tuning inside a graph). */
+struct StageDesc {
+    const int32_t* q_len;
+    const int64_t* q_off;
+    const float2* q_xy;
+    int32_t* ids;
+    int32_t* dist;
+    int nq;
+    int max_len;
+};
+
+__global__ void k_stage(const StageDesc* d, int* next, int* cur, int32_t* len1, int64_t* off1, float2* xy1,
+                        int32_t* flag) {
+    __shared__ int qi_s, len_s;
+    __shared__ long long off_s;
+    if (threadIdx.x == 0) {
+        const int qi = atomicAdd(next, 1);
+        int L = 1;
+        long long o = 0;
+        if (qi < d->nq) {
+            L = d->q_len[qi];
+            o = d->q_off[qi];
+            if (L < 1 || L > d->max_len) {
+                atomicCAS(flag, 0, GAT_ERR_ARG); /* the longest query was understated */
+                L = min(max(L, 1), d->max_len);
+            }
+        }
+        *cur = qi;
+        qi_s = qi;
+        len_s = L;
+        off_s = o;
+        len1[0] = L;
+        off1[0] = 0;
+        off1[1] = L;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < len_s; i += blockDim.x)
+        xy1[i] = qi_s < d->nq ? d->q_xy[off_s + i] : make_float2(0.f, 0.f);
+}
+
+__global__ void k_unstage(const StageDesc* d, const int* cur, const int32_t* ids1, const int32_t* dist1, int k) {
+    const int qi = *cur;
+    if (qi >= d->nq) return;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        d->ids[(size_t)qi * k + i] = ids1[i];
+        d->dist[(size_t)qi * k + i] = dist1[i];
+    }
+}
+
+/* ends the round loop once the query is done; a bound on the rounds guards the loop */
+__global__ void k_loop_cond(const int32_t* ws, int* iter, int maxit, int32_t* flag, unsigned long long* rounds,
+                            cudaGraphConditionalHandle h) {
+    const int it = ++(*iter);
+    atomicAdd(rounds, 1ull);
+    bool more = ws[WS_DONE] == 0;
+    if (more && it >= maxit) {
+        atomicCAS(flag, 0, GAT_ERR_STATE);
+        more = false;
+    }
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+struct LoneGraph {
+    const gat_index* g = nullptr;
+    int max_q_len = 0, k = 0;
+    float u = 0.f;
+    gat_ctx* w = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev = nullptr;
+    int64_t launches_fixed = 0, launches_round = 0; /* per replay: outside / inside the loop */
+    StageDesc* d_desc = nullptr;
+    int *d_next = nullptr, *d_cur = nullptr, *d_iter = nullptr;
+    int32_t* len1 = nullptr;
+    int64_t* off1 = nullptr;
+    float2* xy1 = nullptr;
+    int32_t *ids1 = nullptr, *dist1 = nullptr;
+    unsigned long long* acc = nullptr; /* [0] cells, [1] pairs, [2] rounds */
+};
+
+void lone_graph_free(void* p) {
+    auto* L = static_cast<LoneGraph*>(p);
+    if (L->exec) cudaGraphExecDestroy(L->exec);
+    if (L->graph) cudaGraphDestroy(L->graph);
+    if (L->ev) cudaEventDestroy(L->ev);
+    if (L->w) gat_ctx_destroy(L->w);
+    delete L;
+}
+
+constexpr int kLoneGraphCache = 2;
+constexpr int kLoneRows = 4; /* tile height 128: the best of 2/4/8 on one query's pairs (a few hundred rows) */
+
+int lone_graph_get(gat_ctx* ctx, const gat_index* g, int max_q_len, int k, float u, LoneGraph** out) {
+    for (auto& o : ctx->owned)
+        if (o.second == lone_graph_free) {
+            auto* L = static_cast<LoneGraph*>(o.first);
+            if (L->g == g && L->max_q_len == max_q_len && L->k == k && L->u == u) {
+                *out = L;
+                return GAT_OK;
+            }
+        }
+    int n_graphs = 0;
+    for (auto& o : ctx->owned) n_graphs += o.second == lone_graph_free;
+    if (n_graphs >= kLoneGraphCache) {
+        for (auto it = ctx->owned.begin(); it != ctx->owned.end(); ++it)
+            if (it->second == lone_graph_free) {
+                lone_graph_free(it->first);
+                ctx->owned.erase(it);
+                break;
+            }
+    }
+    auto* L = new LoneGraph();
+    L->g = g;
+    L->max_q_len = max_q_len;
+    L->k = k;
+    L->u = u;
+    int st = gat_ctx_create_worker(ctx, &L->w);
+    if (st != GAT_OK) {
+        delete L;
+        return fail(ctx, st, "top-k: worker context for the query graph");
+    }
+    L->w->edr_rows = ctx->edr_rows ? ctx->edr_rows : kLoneRows;
+    if (cudaEventCreateWithFlags(&L->ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        lone_graph_free(L);
+        return fail(ctx, GAT_ERR_CUDA, "top-k: event");
+    }
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t b_desc = up(sizeof(StageDesc)), b_ctr = 256, b_len = 256, b_off = 256;
+    const size_t b_xy = up((size_t)max_q_len * sizeof(float2)), b_out = up((size_t)k * 4);
+    char* p = (char*)scratch(L->w, S_TOPK_GSTAGE, b_desc + b_ctr + b_len + b_off + b_xy + 2 * b_out, &st);
+    L->acc = (unsigned long long*)scratch(L->w, S_TOPK_IO, 256, &st);
+    if (!p || !L->acc) {
+        lone_graph_free(L);
+        return fail(ctx, GAT_ERR_OOM, "top-k: query graph buffers");
+    }
+    L->d_desc = (StageDesc*)p;
+    p += b_desc;
+    L->d_next = (int*)p;
+    L->d_cur = L->d_next + 1;
+    L->d_iter = L->d_next + 2;
+    p += b_ctr;
+    L->len1 = (int32_t*)p;
+    p += b_len;
+    L->off1 = (int64_t*)p;
+    p += b_off;
+    L->xy1 = (float2*)p;
+    p += b_xy;
+    L->ids1 = (int32_t*)p;
+    L->dist1 = (int32_t*)(p + b_out);
+    ctx->owned.emplace_back(L, lone_graph_free);
+    *out = L;
+    return GAT_OK;
+}
+
+/* the kernels of one query before / inside / after the round loop, on the worker's stream */
+int lone_pre(LoneGraph* L, TopkRun& R) {
+    gat_ctx* w = L->w;
+    k_stage<<<1, 256, 0, w->stream>>>(L->d_desc, L->d_next, L->d_cur, L->len1, L->off1, L->xy1, w->d_flag);
+    count_launch(w);
+    GAT_CUDA_TRY(w, cudaMemsetAsync(L->d_iter, 0, sizeof(int), w->stream), "top-k");
+    return topk_pre(w, L->g, 1, L->len1, L->off1, L->xy1, L->max_q_len, L->k, L->u, nullptr, R);
+}
+
+int lone_round(LoneGraph* L, const TopkRun& R, const cudaGraphConditionalHandle* h) {
+    gat_ctx* w = L->w;
+    topk_plan(w, R);
+    int st = topk_round(w, R, R.n, L->acc);
+    if (st != GAT_OK) return st;
+    if (h) {
+        k_loop_cond<<<1, 1, 0, w->stream>>>(R.ws, L->d_iter, R.rounds + 1, w->d_flag, L->acc + 2, *h);
+        count_launch(w);
+    }
+    return GAT_OK;
+}
+
+int lone_post(LoneGraph* L, const TopkRun& R) {
+    gat_ctx* w = L->w;
+    int st = topk_post(w, R, L->ids1, L->dist1, L->acc + 1);
+    if (st != GAT_OK) return st;
+    k_unstage<<<1, 256, 0, w->stream>>>(L->d_desc, L->d_cur, L->ids1, L->dist1, L->k);
+    count_launch(w);
+    return GAT_OK;
+}
+
+/* The first query of a new graph runs uncaptured (this sizes every scratch slot), then the
+ * graph is captured: pre and post as child graphs, the rounds as the body of a while node. */
+int lone_build(LoneGraph* L) {
+    gat_ctx* w = L->w;
+    cudaStream_t s = w->stream;
+    TopkRun R;
+    int st = lone_pre(L, R);
+    if (st != GAT_OK) return st;
+    for (int r = 0; r < R.rounds; r++) {
+        if ((st = lone_round(L, R, nullptr)) != GAT_OK) return st;
+        int32_t* done = reinterpret_cast<int32_t*>(w->h_pinned + 4);
+        GAT_CUDA_TRY(w, cudaMemcpyAsync(done, R.ws + WS_DONE, 4, cudaMemcpyDeviceToHost, s), "top-k");
+        GAT_CUDA_TRY(w, cudaStreamSynchronize(s), "top-k");
+        if (*done) break;
+    }
+    if ((st = lone_post(L, R)) != GAT_OK) return st;
+    GAT_CUDA_TRY(w, cudaStreamSynchronize(s), "top-k");
+    GAT_CUDA_TRY(w, cudaGetLastError(), "top-k");
+
+    cudaGraph_t gpre = nullptr, gpost = nullptr, G = nullptr;
+    auto cleanup = [&]() {
+        if (gpre) cudaGraphDestroy(gpre);
+        if (gpost) cudaGraphDestroy(gpost);
+        if (G) cudaGraphDestroy(G);
+        cudaGetLastError();
+    };
+    auto capture = [&](cudaGraph_t* out, auto&& fn) -> int {
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_fail(w, cudaGetLastError(), "capture");
+        int rc = fn();
+        cudaGraph_t gr = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s, &gr);
+        if (rc != GAT_OK) {
+            if (gr) cudaGraphDestroy(gr);
+            return rc;
+        }
+        if (e != cudaSuccess) return cuda_fail(w, e, "capture");
+        *out = gr;
+        return GAT_OK;
+    };
+    int64_t l0 = w->launches;
+    TopkRun RC;
+    if ((st = capture(&gpre, [&] { return lone_pre(L, RC); })) != GAT_OK) return cleanup(), st;
+    const int64_t l1 = w->launches;
+    if ((st = capture(&gpost, [&] { return lone_post(L, RC); })) != GAT_OK) return cleanup(), st;
+    const int64_t l2 = w->launches;
+    if (cudaGraphCreate(&G, 0) != cudaSuccess) return cleanup(), cuda_fail(w, cudaGetLastError(), "graph");
+    cudaGraphNode_t npre = nullptr, nloop = nullptr, npost = nullptr;
+    cudaGraphConditionalHandle h;
+    if (cudaGraphAddChildGraphNode(&npre, G, nullptr, 0, gpre) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&h, G, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+        return cleanup(), cuda_fail(w, cudaGetLastError(), "graph");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (cudaGraphAddNode(&nloop, G, &npre, 1, &cp) != cudaSuccess) return cleanup(), cuda_fail(w, cudaGetLastError(), "graph");
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return cleanup(), cuda_fail(w, cudaGetLastError(), "graph");
+    const int64_t l3 = w->launches;
+    st = lone_round(L, RC, &h);
+    const int64_t l4 = w->launches;
+    cudaGraph_t body_out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &body_out);
+    if (st != GAT_OK) return cleanup(), st;
+    if (e != cudaSuccess) return cleanup(), cuda_fail(w, e, "graph");
+    if (cudaGraphAddChildGraphNode(&npost, G, &nloop, 1, gpost) != cudaSuccess ||
+        cudaGraphInstantiate(&L->exec, G, 0) != cudaSuccess)
+        return cleanup(), cuda_fail(w, cudaGetLastError(), "graph instantiate");
+    cudaGraphDestroy(gpre);
+    cudaGraphDestroy(gpost);
+    gpre = gpost = nullptr;
+    L->graph = G;
+    L->launches_fixed = (l1 - l0) + (l2 - l1);
+    L->launches_round = l4 - l3;
+    w->launches = l0; /* captured launches run at replay time; counted there */
+    return GAT_OK;
+}
+
+/* Plain form through the query graph: queries [0, nq), one graph launch each. */
+int topk_plain_graph(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, const int64_t* d_q_off,
+                     const float2* d_q_xy, int max_q_len, int k, float u, int32_t* d_ids, int32_t* d_dist, int64_t* stats) {
+    LoneGraph* L = nullptr;
+    int st = lone_graph_get(ctx, g, max_q_len, k, u, &L);
+    if (st != GAT_OK) return st;
+    gat_ctx* w = L->w;
+    cudaStream_t s = w->stream;
+    /* the worker's stream starts after the caller's work on the context stream */
+    GAT_CUDA_TRY(ctx, cudaEventRecord(L->ev, ctx->stream), "top-k");
+    GAT_CUDA_TRY(ctx, cudaStreamWaitEvent(s, L->ev, 0), "top-k");
+    StageDesc* hd = reinterpret_cast<StageDesc*>(w->h_pinned);
+    *hd = StageDesc{d_q_len, d_q_off, d_q_xy, d_ids, d_dist, nq, max_q_len};
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(L->d_desc, hd, sizeof(StageDesc), cudaMemcpyHostToDevice, s), "top-k");
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(L->d_next, 0, sizeof(int), s), "top-k");
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(L->acc, 0, 3 * sizeof(unsigned long long), s), "top-k");
+    const int64_t lw0 = w->launches;
+    int first = 0;
+    if (!L->exec) {
+        if ((st = lone_build(L)) != GAT_OK) {
+            /* leave no half-built graph behind; the error names the failing step */
+            std::string msg = w->err;
+            for (auto it = ctx->owned.begin(); it != ctx->owned.end(); ++it)
+                if (it->first == L) {
+                    ctx->owned.erase(it);
+                    break;
+                }
+            lone_graph_free(L);
+            return fail(ctx, st, "top-k graph: " + msg);
+        }
+        first = 1;
+    }
+    for (int q = first; q < nq; q++) GAT_CUDA_TRY(ctx, cudaGraphLaunch(L->exec, s), "top-k graph launch");
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(w->h_pinned + 8, L->acc, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+                 "top-k");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "top-k");
+    if ((st = check_device_flag(w, "top-k")) != GAT_OK) return fail(ctx, st, w->err);
+    const int64_t rounds = w->h_pinned[10];
+    ctx->launches += (w->launches - lw0) + (int64_t)(nq - first) * L->launches_fixed + rounds * L->launches_round;
+    if (stats) {
+        stats[0] = w->h_pinned[9];
+        stats[1] = w->h_pinned[8];
+        stats[2] = 0;
+    }
+    return GAT_OK;
 }
 
 int topk_dev(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, const int64_t* d_q_off,
@@ -831,6 +1198,9 @@ int topk_dev(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
     int64_t l0 = ctx->launches;
     int64_t local[4] = {0, 0, 0, 0};
     int st = GAT_OK;
+    unsigned long long* acc = (unsigned long long*)scratch(ctx, S_TOPK_IO, 256, &st);
+    if (!acc) return st;
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(acc, 0, 2 * sizeof(unsigned long long), ctx->stream), "top-k");
     if (exec == GAT_EXEC_BATCHED) {
         /* query batches sized so the per-batch candidate arrays stay below ~8 GiB */
         int bins = std::max(max_q_len, g->db->maxlen) + 2;
@@ -838,18 +1208,28 @@ int topk_dev(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
         for (int q0 = 0; q0 < nq && st == GAT_OK; q0 += (int)per) {
             int c = (int)std::min<int64_t>(per, nq - q0);
             st = topk_batch(ctx, g, c, d_q_len + q0, d_q_off + q0, d_q_xy, max_q_len, k, u, d_ids + (size_t)q0 * k,
-                            d_dist + (size_t)q0 * k, local);
+                            d_dist + (size_t)q0 * k, local, acc);
         }
+    } else if (!ctx->timing) {
+        /* plain form: one query per launch of the query graph */
+        st = topk_plain_graph(ctx, g, nq, d_q_len, d_q_off, d_q_xy, max_q_len, k, u, d_ids, d_dist, stats);
+        if (st == GAT_OK && stats) stats[2] = ctx->launches - l0;
+        return st;
     } else {
+        /* plain form with per-kernel timing: the same kernels launched one by one */
         for (int qi = 0; qi < nq && st == GAT_OK; qi++)
             st = topk_batch(ctx, g, 1, d_q_len + qi, d_q_off + qi, d_q_xy, max_q_len, k, u, d_ids + (size_t)qi * k,
-                            d_dist + (size_t)qi * k, local);
+                            d_dist + (size_t)qi * k, local, acc);
     }
     if (st != GAT_OK) return st;
-    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "top-k");
+    /* one read for the whole call: counters, then the device status word */
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 6, acc, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                      ctx->stream), "top-k");
+    if ((st = check_device_flag(ctx, "top-k")) != GAT_OK) return st;
+    timed_add_work(ctx, GAT_KERNEL_EDR, (double)ctx->h_pinned[6]);
     if (stats) {
-        stats[0] = local[0];
-        stats[1] = local[1];
+        stats[0] = ctx->h_pinned[7];
+        stats[1] = ctx->h_pinned[6];
         stats[2] = ctx->launches - l0;
     }
     return GAT_OK;
@@ -976,7 +1356,7 @@ int gat_fv_lower_bounds(gat_ctx* ctx, const gat_index* grid, int nq, const int32
     float2* dxy;
     if ((st = upload_queries(ctx, nq, q_len, q_lon, q_lat, h, &dl, &doff, &dxy)) != GAT_OK) return st;
     int64_t stats[4] = {0, 0, 0, -1}; /* bounds only */
-    st = topk_batch(ctx, grid, nq, dl, doff, dxy, h.maxlen, 1, match_threshold(1e-9), nullptr, nullptr, stats);
+    st = topk_batch(ctx, grid, nq, dl, doff, dxy, h.maxlen, 1, match_threshold(1e-9), nullptr, nullptr, stats, nullptr);
     if (st != GAT_OK) return st;
     int n = grid->db->n;
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(out, ctx->slot_ptr[S_TOPK_LB], (size_t)nq * (n + 1) * 4, cudaMemcpyDeviceToHost, ctx->stream), "bounds D2H");

@@ -82,3 +82,27 @@ def test_long_queries_against_short_set(gpu_ctx):
         for j in range(qs.n):
             wi, wd, _ = o.topk(*qs.points(j + 1), 64, 5e-4)
             assert np.array_equal(ids[j], wi) and np.array_equal(dist[j], wd), (execution, j, int(ql[j]))
+
+
+def test_plain_graph_matches_stream_path(gpu_ctx, small):
+    """The plain form runs each query as one launch of a CUDA graph (rounds in a device-side
+    loop); with per-kernel timing on, the same kernels are launched one by one. Both, over
+    repeated calls (graph reuse), several k (several cached graphs, one evicted) and a single
+    query (the uncaptured sizing run only), equal the batched form."""
+    t, g, o, qids = small
+    q = t.subset(qids)
+    for k in (4, 16, 8, 16):
+        b_ids, b_d, _ = g.topk(q, k, 5e-4, execution="batched")
+        p_ids, p_d, st = g.topk(q, k, 5e-4, execution="plain")
+        assert np.array_equal(p_ids, b_ids) and np.array_equal(p_d, b_d), k
+        assert st["launches"] > 0 and st["pairs"] > 0
+    gpu_ctx.set_timing(True)
+    try:
+        s_ids, s_d, _ = g.topk(q, 16, 5e-4, execution="plain")
+    finally:
+        gpu_ctx.set_timing(False)
+    b_ids, b_d, _ = g.topk(q, 16, 5e-4, execution="batched")
+    assert np.array_equal(s_ids, b_ids) and np.array_equal(s_d, b_d)
+    one = t.subset(qids[:1])
+    i1, d1, _ = g.topk(one, 5, 5e-4, execution="plain")
+    assert np.array_equal(i1[0], b_ids[0, :5]) and np.array_equal(d1[0], b_d[0, :5])
