@@ -81,6 +81,9 @@ class Context:
         """Rows per lane of the EDR wavefront: 0 = autotune (default), 2, 4 or 8."""
         self.check(lib.gat_ctx_set_tuning(self.h, L.GAT_TUNE_EDR_ROWS, int(rows)), "gat_ctx_set_tuning")
 
+    def set_tuning(self, knob: int, value: int) -> None:
+        self.check(lib.gat_ctx_set_tuning(self.h, knob, int(value)), "gat_ctx_set_tuning")
+
     def tuning(self, knob: int) -> int:
         v = C.c_int32(0)
         self.check(lib.gat_ctx_get_tuning(self.h, knob, C.byref(v)), "gat_ctx_get_tuning")

@@ -283,6 +283,16 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int cls, double* ms, int64_t* launches, d
 int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
     if (!ctx) return GAT_ERR_ARG;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    if (knob == GAT_TUNE_TOPK_CHUNK) {
+        if (value < 0 || value > (1 << 24)) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: chunk outside 0..2^24");
+        ctx->topk_chunk = value;
+        return GAT_OK;
+    }
+    if (knob == GAT_TUNE_TOPK_GROWTH) {
+        if (value < 0 || value == 1 || value > 64) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: growth must be 0 or 2..64");
+        ctx->topk_growth = value;
+        return GAT_OK;
+    }
     if (knob != GAT_TUNE_EDR_ROWS) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: unknown knob");
     if (value != 0 && value != 2 && value != 4 && value != 8)
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR rows per lane must be 0 (autotune), 2, 4 or 8");
@@ -298,6 +308,10 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
         *value = ctx->edr_rows;
     else if (knob == GAT_TUNE_EDR_TUNED)
         *value = (int)ctx->edr_tune.size();
+    else if (knob == GAT_TUNE_TOPK_CHUNK)
+        *value = ctx->topk_chunk;
+    else if (knob == GAT_TUNE_TOPK_GROWTH)
+        *value = ctx->topk_growth;
     else
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_get_tuning: unknown knob");
     return GAT_OK;

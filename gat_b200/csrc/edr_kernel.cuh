@@ -28,7 +28,8 @@
 namespace gat {
 namespace edr {
 
-constexpr int kWarps = 8;
+constexpr int kWarps = 8; /* k_edr (one warp per pair) */
+constexpr int kTileWarps = 8; /* k_edr_tiles (2-warp CTAs measured no better on small launches) */
 constexpr int kBig = 1 << 29; /* above any distance; up + 1 never overflows against it */
 
 /* Pair source over (a_off, a_len, b_off, b_len) arrays; results to out[p]. A pair with a side
@@ -493,13 +494,13 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
 }
 
 template <int R, class Src>
-__global__ void __launch_bounds__(kWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(Src src, float u, TileCtl ctl, unsigned* __restrict__ work,
+__global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(Src src, float u, TileCtl ctl, unsigned* __restrict__ work,
                                                            unsigned long long* __restrict__ cells) {
-    __shared__ float2 bring[kWarps][64];
-    __shared__ int cring[kWarps][32];
+    __shared__ float2 bring[kTileWarps][64];
+    __shared__ int cring[kTileWarps][32];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int gw = blockIdx.x * kWarps + wib;
+    const int gw = blockIdx.x * kTileWarps + wib;
     carry_t* wc0 = ctl.warp_carry + (size_t)gw * 2 * ctl.stride;
     carry_t* wc1 = wc0 + ctl.stride;
     const carry_t ep = *ctl.epoch << 8;
@@ -576,7 +577,7 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     int st = GAT_OK;
     cudaStream_t s = ctx->stream;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr_tiles<R, Src>, kWarps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr_tiles<R, Src>, kTileWarps * 32, 0);
     const int grid = ctx->sm_count * (per_sm > 0 ? per_sm : 1);
     const int stride = max_cols + 2;
     const int maxT = max_rows <= 0 ? 1 : (max_rows + 32 * R - 1) / (32 * R);
@@ -591,7 +592,7 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     int4* items = (int4*)scratch(ctx, S_EDR_ITEMS, (size_t)item_cap * sizeof(int4), &st);
     carry_t* pcarry =
         coop > 0 ? (carry_t*)scratch_zeroed(ctx, S_EDR_PCARRY, (size_t)coop * 2 * stride * sizeof(carry_t), &st) : nullptr;
-    carry_t* wcarry = (carry_t*)scratch_zeroed(ctx, S_EDR_CARRY, (size_t)grid * kWarps * 2 * stride * sizeof(carry_t), &st);
+    carry_t* wcarry = (carry_t*)scratch_zeroed(ctx, S_EDR_CARRY, (size_t)grid * kTileWarps * 2 * stride * sizeof(carry_t), &st);
     if (!ctr || !meta || !items || !wcarry || (coop > 0 && !pcarry)) return st;
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(ctr, 0, kCtrWords * sizeof(int), s), "edr");
     const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->sm_count * 8));
@@ -603,7 +604,7 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
                 ctx->d_flag};
     timed_begin(ctx, GAT_KERNEL_EDR);
     if (ev0) cudaEventRecord(ev0, s);
-    k_edr_tiles<R, Src><<<grid, kWarps * 32, 0, s>>>(src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
+    k_edr_tiles<R, Src><<<grid, kTileWarps * 32, 0, s>>>(src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
     if (ev1) cudaEventRecord(ev1, s);
     timed_end(ctx, GAT_KERNEL_EDR, 0.0);
     count_launch(ctx);

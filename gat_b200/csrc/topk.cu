@@ -780,8 +780,9 @@ int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
      * it starts with a larger chunk and grows faster; a batch keeps rounds tight to limit
      * surplus evaluations. */
     R.lone = nq <= 4;
-    R.chunk0 = R.lone ? std::max(8 * k, 1024) : std::max(4 * k, 128);
-    R.growth = R.lone ? 4 : 2;
+    R.chunk0 = ctx->topk_chunk ? ctx->topk_chunk : (R.lone ? 1024 : 128);
+    R.chunk0 = std::max(R.chunk0, R.lone ? 8 * k : 4 * k);
+    R.growth = ctx->topk_growth ? ctx->topk_growth : (R.lone ? 4 : 2);
     R.rounds = 1;
     for (int64_t cover = R.chunk0, c = R.chunk0; cover < n; R.rounds++) {
         c *= R.growth;
@@ -945,6 +946,7 @@ struct LoneGraph {
     const gat_index* g = nullptr;
     int max_q_len = 0, k = 0;
     float u = 0.f;
+    int chunk = 0, growth = 0, rows = 0; /* the context's knobs when the graph was built */
     gat_ctx* w = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -975,7 +977,8 @@ int lone_graph_get(gat_ctx* ctx, const gat_index* g, int max_q_len, int k, float
     for (auto& o : ctx->owned)
         if (o.second == lone_graph_free) {
             auto* L = static_cast<LoneGraph*>(o.first);
-            if (L->g == g && L->max_q_len == max_q_len && L->k == k && L->u == u) {
+            if (L->g == g && L->max_q_len == max_q_len && L->k == k && L->u == u && L->chunk == ctx->topk_chunk &&
+                L->growth == ctx->topk_growth && L->rows == ctx->edr_rows) {
                 *out = L;
                 return GAT_OK;
             }
@@ -1000,7 +1003,12 @@ int lone_graph_get(gat_ctx* ctx, const gat_index* g, int max_q_len, int k, float
         delete L;
         return fail(ctx, st, "top-k: worker context for the query graph");
     }
+    L->chunk = ctx->topk_chunk;
+    L->growth = ctx->topk_growth;
+    L->rows = ctx->edr_rows;
     L->w->edr_rows = ctx->edr_rows ? ctx->edr_rows : kLoneRows;
+    L->w->topk_chunk = ctx->topk_chunk;
+    L->w->topk_growth = ctx->topk_growth;
     if (cudaEventCreateWithFlags(&L->ev, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         lone_graph_free(L);

@@ -121,3 +121,16 @@ def test_tuning_knob(host_ctx):
         assert e.value.status == L.GAT_ERR_ARG
     with pytest.raises(G.GatError):
         host_ctx.tuning(99)
+
+
+def test_topk_walk_knobs(host_ctx):
+    """GAT_TUNE_TOPK_CHUNK (0..2^24) and GAT_TUNE_TOPK_GROWTH (0 or 2..64) round-trip; other
+    values are refused."""
+    for knob, good, bad in ((L.GAT_TUNE_TOPK_CHUNK, (512, 0), (-1, 1 << 25)),
+                            (L.GAT_TUNE_TOPK_GROWTH, (2, 8, 0), (1, 65, -2))):
+        for v in good:
+            host_ctx.set_tuning(knob, v)
+            assert host_ctx.tuning(knob) == v
+        for v in bad:
+            with pytest.raises(G.GatError):
+                host_ctx.set_tuning(knob, v)
