@@ -283,6 +283,12 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int cls, double* ms, int64_t* launches, d
 int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
     if (!ctx) return GAT_ERR_ARG;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    if (knob == GAT_TUNE_EDR_FORM) {
+        if (value < 0 || value > 2) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR form must be 0, 1 or 2");
+        ctx->edr_form = value;
+        ctx->edr_tune.clear();
+        return GAT_OK;
+    }
     if (knob == GAT_TUNE_TOPK_CHUNK) {
         if (value < 0 || value > (1 << 24)) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: chunk outside 0..2^24");
         ctx->topk_chunk = value;
@@ -310,6 +316,8 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
         *value = (int)ctx->edr_tune.size();
     else if (knob == GAT_TUNE_TOPK_CHUNK)
         *value = ctx->topk_chunk;
+    else if (knob == GAT_TUNE_EDR_FORM)
+        *value = ctx->edr_form;
     else if (knob == GAT_TUNE_TOPK_GROWTH)
         *value = ctx->topk_growth;
     else

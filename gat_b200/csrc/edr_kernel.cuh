@@ -255,7 +255,7 @@ __device__ __forceinline__ int duration_class(long long d) {
     return min(2 * e + half, kClasses - 1);
 }
 
-template <int R, class Src>
+template <int R, bool COL, class Src>
 __global__ void k_sched_count(Src src, int cap, int coop_cap, int* __restrict__ ctr, int2* __restrict__ meta) {
     __shared__ int hist[kClasses];
     for (int i = threadIdx.x; i < kClasses; i += blockDim.x) hist[i] = 0;
@@ -267,7 +267,8 @@ __global__ void k_sched_count(Src src, int cap, int coop_cap, int* __restrict__ 
         int32_t* o;
         src.get(p, a, la, b, lb, o);
         const int len1 = min(la, lb), len2 = max(la, lb);
-        const int T = len1 <= 0 ? 1 : (len1 + 32 * R - 1) / (32 * R);
+        const int nlane = COL ? len2 : len1, nstep = COL ? len1 : len2;
+        const int T = nlane <= 0 ? 1 : (nlane + 32 * R - 1) / (32 * R);
         int slot = -1, items = 1;
         if (T >= 2) {
             const int sl = atomicAdd(&ctr[1], 1);
@@ -276,7 +277,7 @@ __global__ void k_sched_count(Src src, int cap, int coop_cap, int* __restrict__ 
                 items = T;
             }
         }
-        const long long dur = slot >= 0 ? (long long)len2 + 32LL * (T - 1) : (long long)T * (len2 + 31);
+        const long long dur = slot >= 0 ? (long long)nstep + 32LL * (T - 1) : (long long)T * (nstep + 31);
         const int c = duration_class(dur);
         atomicAdd(&hist[c], items);
         meta[p] = make_int2(slot, (c << 16) | items);
@@ -373,6 +374,33 @@ __device__ __forceinline__ int wf_step(const float (&ax)[R], const float (&ay)[R
     return up;
 }
 
+/* Column-tile form of the same recurrence: a lane owns R consecutive DP columns and a step
+ * advances one DP row r. Values are held shifted by their row: F[r][c] = D[r][c] - r, so in
+ * row r's shift u = F[r-1][c] needs no add, m = F[r-1][c-1] + (match ? -1 : 0) and
+ * l = F[r][c-1] + 1, whose chain runs along the lane's columns: with mm1 = m - 1 and
+ * prev = F[r][c-1], m == l exactly when mm1 == prev, min(m, l) = min(mm1, prev) + 1, and the
+ * cell is u when they are equal, else min(u, min(m, l)). State per column j: F[j] =
+ * F[r-1][c_j] on entry, F[r][c_j] on exit; diag0 = F[r-1][c_0 - 1]; left = F[r][c_0 - 1] (the
+ * value to the left of the lane's first column). Same interface as wf_step. */
+template <int R>
+__device__ __forceinline__ int cf_step(const float (&bx)[R], const float (&by)[R], int (&F)[R], int& diag0, float2 a,
+                                       int left, float u) {
+    int prev = left;
+    int diag = diag0;
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const int up = F[j];
+        const int mm1 = diag + match_mask(bx[j], by[j], a, u) - 1;
+        const int mn = min(mm1, prev);
+        const int d = (mm1 == prev) ? up : __viaddmin_s32(mn, 1, up);
+        diag = up;
+        F[j] = d;
+        prev = d;
+    }
+    diag0 = left;
+    return prev;
+}
+
 /* One row tile of one pair (rows r0 = t * 32R ...). cin: the carry words of tile t-1's bottom
  * row (nullptr for t == 0), accepted with tag tag_in; cout: this tile's bottom row for tile t+1
  * (nullptr for the last tile), written with tag tag_out. Returns false when a wait gave up.
@@ -383,7 +411,10 @@ __device__ __forceinline__ int wf_step(const float (&ax)[R], const float (&ay)[R
  * column s0 + k - L of step k at window index 32 + k - L (a per-lane base plus a constant).
  * The next chunk's points and carry words are loaded one chunk early. Chunks where every
  * lane's column is inside the pair skip the bounds test. */
-template <int R>
+/* COL: the column-tile form (cf_step); rows / cols / len1 / len2 then name the lane side
+ * (columns) and the step side (rows), the carry runs along the tile's last column, and the
+ * result is F + len2 (the step side's length), exactly as the row form's E + len2. */
+template <int R, bool COL = false>
 __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const float2* __restrict__ cols, int len1,
                                          int len2, int t, const carry_t* cin, carry_t* cout, carry_t tag_in,
                                          carry_t tag_out, float u, float2* sb, int* sc, int& result) {
@@ -467,7 +498,7 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
             for (int k = 0; k < 32; k++) {
                 const int from_above = __shfl_up_sync(FULL, bottom, 1);
                 const int up0 = lane0 ? sc[k] : from_above;
-                bottom = wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u);
+                bottom = COL ? cf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u) : wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u);
                 if (writer) st_carry(cout + (s0 + k - 30), tag_hi | (carry_t)(unsigned short)bottom);
             }
         } else {
@@ -477,7 +508,8 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
                 const int j = s0 + k - lane;
                 if (j >= 0 && j < len2) {
                     const int up0 = lane0 ? sc[k] : from_above;
-                    bottom = wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u);
+                    bottom = COL ? cf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u)
+                                 : wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u);
                     if (writer) st_carry(cout + (j + 1), tag_hi | (carry_t)(unsigned short)bottom);
                 }
             }
@@ -493,7 +525,7 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
     return true;
 }
 
-template <int R, class Src>
+template <int R, bool COL, class Src>
 __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(Src src, float u, TileCtl ctl, unsigned* __restrict__ work,
                                                            unsigned long long* __restrict__ cells) {
     __shared__ float2 bring[kTileWarps][64];
@@ -533,21 +565,25 @@ __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(S
             if (lane == 0) *outp = len1 + len2;
             continue;
         }
+        /* lane side and step side: rows / columns for row tiles, columns / rows for column tiles */
+        const float2* lpts = COL ? cols : rows;
+        const float2* spts = COL ? rows : cols;
+        const int nlane = COL ? len2 : len1, nstep = COL ? len1 : len2;
         constexpr int kTile = 32 * R;
-        const int T = (len1 + kTile - 1) / kTile;
+        const int T = (nlane + kTile - 1) / kTile;
         int result = 0;
         bool ok = true, finished = false;
         if (t < 0) {
             for (int tt = 0; tt < T && ok; tt++)
-                ok = edr_tile<R>(rows, cols, len1, len2, tt, tt > 0 ? ((tt - 1) & 1 ? wc1 : wc0) : nullptr,
-                                 tt + 1 < T ? ((tt & 1) ? wc1 : wc0) : nullptr, ep | ((tt - 1) & 0xff),
-                                 ep | (tt & 0xff), u, bring[wib], cring[wib], result);
+                ok = edr_tile<R, COL>(lpts, spts, nlane, nstep, tt, tt > 0 ? ((tt - 1) & 1 ? wc1 : wc0) : nullptr,
+                                      tt + 1 < T ? ((tt & 1) ? wc1 : wc0) : nullptr, ep | ((tt - 1) & 0xff),
+                                      ep | (tt & 0xff), u, bring[wib], cring[wib], result);
             finished = true;
         } else {
             carry_t* pc = ctl.pair_carry + (size_t)it.z * 2 * ctl.stride;
-            ok = edr_tile<R>(rows, cols, len1, len2, t, t > 0 ? pc + ((t - 1) & 1) * ctl.stride : nullptr,
-                             t + 1 < T ? pc + (t & 1) * ctl.stride : nullptr, ep | ((t - 1) & 0xff), ep | (t & 0xff),
-                             u, bring[wib], cring[wib], result);
+            ok = edr_tile<R, COL>(lpts, spts, nlane, nstep, t, t > 0 ? pc + ((t - 1) & 1) * ctl.stride : nullptr,
+                                  t + 1 < T ? pc + (t & 1) * ctl.stride : nullptr, ep | ((t - 1) & 0xff),
+                                  ep | (t & 0xff), u, bring[wib], cring[wib], result);
             finished = t == T - 1;
         }
         if (!ok) {
@@ -558,7 +594,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(S
             continue;
         }
         if (finished) {
-            const int owner = ((len1 - 1) % kTile) / R;
+            const int owner = ((nlane - 1) % kTile) / R;
             result = __shfl_sync(FULL, result, owner);
             if (lane == 0) {
                 *outp = result;
@@ -571,16 +607,18 @@ __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(S
 /* Host side: schedule (count, write) -> tiled kernel. cap is the number of pairs (exact for
  * host-known lists, an upper bound for device-counted ones); max_rows / max_cols bound the
  * shorter / longer side of every pair. ev0/ev1, when given, bracket the tile kernel. */
-template <int R, class Src>
+template <int R, bool COL, class Src>
 int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
                  unsigned long long* cells, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
     int st = GAT_OK;
     cudaStream_t s = ctx->stream;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr_tiles<R, Src>, kTileWarps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr_tiles<R, COL, Src>, kTileWarps * 32, 0);
     const int grid = ctx->sm_count * (per_sm > 0 ? per_sm : 1);
-    const int stride = max_cols + 2;
-    const int maxT = max_rows <= 0 ? 1 : (max_rows + 32 * R - 1) / (32 * R);
+    /* carry rows run along the step side; tiles are cut along the lane side */
+    const int max_lane = COL ? max_cols : max_rows, max_step = COL ? max_rows : max_cols;
+    const int stride = max_step + 2;
+    const int maxT = max_lane <= 0 ? 1 : (max_lane + 32 * R - 1) / (32 * R);
     const size_t budget = (size_t)512 << 20; /* cooperative carry rows */
     int64_t coop = (int64_t)(budget / ((size_t)2 * stride * sizeof(carry_t)));
     if (coop > cap) coop = cap;
@@ -596,7 +634,7 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     if (!ctr || !meta || !items || !wcarry || (coop > 0 && !pcarry)) return st;
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(ctr, 0, kCtrWords * sizeof(int), s), "edr");
     const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->sm_count * 8));
-    k_sched_count<R, Src><<<pgrid, 256, 0, s>>>(src, (int)cap, (int)coop, ctr, meta);
+    k_sched_count<R, COL, Src><<<pgrid, 256, 0, s>>>(src, (int)cap, (int)coop, ctr, meta);
     count_launch(ctx);
     k_sched_write<Src><<<pgrid, 256, 0, s>>>(src, (int)cap, ctr, meta, items, edr_epochs(ctx));
     count_launch(ctx);
@@ -604,7 +642,7 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
                 ctx->d_flag};
     timed_begin(ctx, GAT_KERNEL_EDR);
     if (ev0) cudaEventRecord(ev0, s);
-    k_edr_tiles<R, Src><<<grid, kTileWarps * 32, 0, s>>>(src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
+    k_edr_tiles<R, COL, Src><<<grid, kTileWarps * 32, 0, s>>>(src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
     if (ev1) cudaEventRecord(ev1, s);
     timed_end(ctx, GAT_KERNEL_EDR, 0.0);
     count_launch(ctx);
@@ -612,13 +650,19 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     return GAT_OK;
 }
 
+/* Tile shapes: rows (or columns) per lane 2, 4, 8, in row or column form. shape = R | COL << 4 */
+constexpr int kShapeCol = 16;
+
 template <class Src>
-int launch_rows(gat_ctx* ctx, int R, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
-                unsigned long long* cells, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
-    switch (R) {
-        case 2: return launch_tiles<2, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
-        case 4: return launch_tiles<4, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
-        default: return launch_tiles<8, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+int launch_shape(gat_ctx* ctx, int shape, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
+                 unsigned long long* cells, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
+    switch (shape) {
+        case 2: return launch_tiles<2, false, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 4: return launch_tiles<4, false, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 8: return launch_tiles<8, false, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 2 | kShapeCol: return launch_tiles<2, true, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 8 | kShapeCol: return launch_tiles<8, true, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        default: return launch_tiles<4, true, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
     }
 }
 
@@ -628,30 +672,38 @@ inline uint64_t ceil_log2(int64_t v) {
     return e;
 }
 
-/* EDR over a pair source with the context's rows-per-lane choice. Autotune (edr_rows == 0):
- * the first launch of a shape class times 8, 4 and 2 rows per lane on this launch's own
- * pairs (every candidate writes the same results; the cell counter is fed once) and records
- * the fastest; later launches of the class use it. */
+/* EDR over a pair source with the context's tile shape. Rows per lane (GAT_TUNE_EDR_ROWS) and
+ * form (GAT_TUNE_EDR_FORM) are fixed by the knobs or autotuned: the first launch of a shape
+ * class times the open candidates on this launch's own pairs (every candidate writes the same
+ * results; the cell counter is fed once) and records the fastest; later launches of the class
+ * use it. */
 template <class Src>
 int edr_launch(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
                unsigned long long* cells) {
     if (cap <= 0) return GAT_OK;
-    if (ctx->edr_rows != 0) return launch_rows(ctx, ctx->edr_rows, src, cap, max_rows, max_cols, u, cells);
+    int cand[6], nc = 0;
+    for (int form = 0; form < 2; form++) {
+        if (ctx->edr_form && ctx->edr_form != form + 1) continue;
+        for (int r : {4, 8, 2}) {
+            if (ctx->edr_rows && ctx->edr_rows != r) continue;
+            cand[nc++] = r | (form ? kShapeCol : 0);
+        }
+    }
+    if (nc == 1) return launch_shape(ctx, cand[0], src, cap, max_rows, max_cols, u, cells);
     const uint64_t key = ((uint64_t)Src::kKind << 60) | (ceil_log2(cap) << 40) | (ceil_log2(max_rows) << 20) |
                          ceil_log2(max_cols);
     auto hit = ctx->edr_tune.find(key);
-    if (hit != ctx->edr_tune.end()) return launch_rows(ctx, hit->second, src, cap, max_rows, max_cols, u, cells);
+    if (hit != ctx->edr_tune.end()) return launch_shape(ctx, hit->second, src, cap, max_rows, max_cols, u, cells);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         if (e0) cudaEventDestroy(e0);
         cudaGetLastError();
-        return launch_rows(ctx, 8, src, cap, max_rows, max_cols, u, cells);
+        return launch_shape(ctx, cand[0], src, cap, max_rows, max_cols, u, cells);
     }
-    int best = 8, st = GAT_OK;
+    int best = cand[0], st = GAT_OK;
     float best_ms = 0.f;
-    const int cand[3] = {8, 4, 2};
-    for (int i = 0; i < 3 && st == GAT_OK; i++) {
-        st = launch_rows(ctx, cand[i], src, cap, max_rows, max_cols, u, i == 0 ? cells : nullptr, e0, e1);
+    for (int i = 0; i < nc && st == GAT_OK; i++) {
+        st = launch_shape(ctx, cand[i], src, cap, max_rows, max_cols, u, i == 0 ? cells : nullptr, e0, e1);
         if (st != GAT_OK) break;
         float ms = 0.f;
         if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {

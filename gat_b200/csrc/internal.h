@@ -94,6 +94,7 @@ struct gat_ctx {
     gat_ctx* root = nullptr; /* worker contexts: the context whose indexes they may use */
     /* EDR rows per lane: 0 = autotune per shape class (edr_tune), else fixed */
     int edr_rows = 0;
+    int edr_form = 0; /* 0 = autotune, 1 = row tiles, 2 = column tiles */
     int topk_chunk = 0, topk_growth = 0; /* 0 = defaults */
     std::map<uint64_t, int> edr_tune;
     /* objects that hold device memory of this context's scratch or workers (cached CUDA graphs);

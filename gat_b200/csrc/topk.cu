@@ -946,7 +946,7 @@ struct LoneGraph {
     const gat_index* g = nullptr;
     int max_q_len = 0, k = 0;
     float u = 0.f;
-    int chunk = 0, growth = 0, rows = 0; /* the context's knobs when the graph was built */
+    int chunk = 0, growth = 0, rows = 0, form = 0; /* the context's knobs when the graph was built */
     gat_ctx* w = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -971,14 +971,15 @@ void lone_graph_free(void* p) {
 }
 
 constexpr int kLoneGraphCache = 2;
-constexpr int kLoneRows = 4; /* tile height 128: the best of 2/4/8 on one query's pairs (a few hundred rows) */
+constexpr int kLoneRows = 4; /* 128-point tiles: the best of 2/4/8 on one query's pairs (a few hundred points) */
+constexpr int kLoneForm = 1; /* row tiles: column tiles measured slower on one query's pairs (many short tiles) */
 
 int lone_graph_get(gat_ctx* ctx, const gat_index* g, int max_q_len, int k, float u, LoneGraph** out) {
     for (auto& o : ctx->owned)
         if (o.second == lone_graph_free) {
             auto* L = static_cast<LoneGraph*>(o.first);
             if (L->g == g && L->max_q_len == max_q_len && L->k == k && L->u == u && L->chunk == ctx->topk_chunk &&
-                L->growth == ctx->topk_growth && L->rows == ctx->edr_rows) {
+                L->growth == ctx->topk_growth && L->rows == ctx->edr_rows && L->form == ctx->edr_form) {
                 *out = L;
                 return GAT_OK;
             }
@@ -1006,7 +1007,9 @@ int lone_graph_get(gat_ctx* ctx, const gat_index* g, int max_q_len, int k, float
     L->chunk = ctx->topk_chunk;
     L->growth = ctx->topk_growth;
     L->rows = ctx->edr_rows;
+    L->form = ctx->edr_form;
     L->w->edr_rows = ctx->edr_rows ? ctx->edr_rows : kLoneRows;
+    L->w->edr_form = ctx->edr_form ? ctx->edr_form : kLoneForm;
     L->w->topk_chunk = ctx->topk_chunk;
     L->w->topk_growth = ctx->topk_growth;
     if (cudaEventCreateWithFlags(&L->ev, cudaEventDisableTiming) != cudaSuccess) {

@@ -96,11 +96,15 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  *   same for every choice. 2, 4 or 8 fixes the value. Setting the knob clears the tuned table.
  * gat_ctx_get_tuning(GAT_TUNE_EDR_ROWS) returns the knob; GAT_TUNE_EDR_TUNED returns the
  * number of tuned shape classes.
+ * GAT_TUNE_EDR_FORM: 0 (default) = autotune, 1 = row tiles (lanes own rows of the shorter
+ *   side, steps walk the longer side), 2 = column tiles (lanes own columns, steps walk the
+ *   shorter side: a shorter critical path for pairs of uneven length). Same results.
  * GAT_TUNE_TOPK_CHUNK / GAT_TUNE_TOPK_GROWTH: candidates a query evaluates in the first round
  *   of the top-k walk, and the factor each later round grows by (0 = defaults: 1024 and 4 for up
  *   to 4 queries per batch, 128 and 2 for larger batches; the first round is never below 8k
  *   or 4k). Results never depend on them; they trade rounds against surplus evaluations. */
-enum { GAT_TUNE_EDR_ROWS = 1, GAT_TUNE_EDR_TUNED = 2, GAT_TUNE_TOPK_CHUNK = 3, GAT_TUNE_TOPK_GROWTH = 4 };
+enum { GAT_TUNE_EDR_ROWS = 1, GAT_TUNE_EDR_TUNED = 2, GAT_TUNE_TOPK_CHUNK = 3, GAT_TUNE_TOPK_GROWTH = 4,
+       GAT_TUNE_EDR_FORM = 5 };
 int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value);
 int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value);
 

@@ -77,18 +77,26 @@ def _mixed_pairs():
     return la, a, lb, b
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("rows", [2, 4, 8])
-def test_rows_per_lane_variants(gpu_ctx, rows):
-    """Every tile height (64, 128, 256 rows) gives the oracle's distances, across single-tile
-    pairs, pipelined multi-tile pairs and the tile boundaries."""
+def test_tile_shapes(gpu_ctx, rows, form):
+    """Every tile shape (64, 128 or 256 points per tile; row tiles or column tiles) gives the
+    oracle's distances, across single-tile pairs, pipelined multi-tile pairs and the tile
+    boundaries."""
+    from gat_b200 import _lib as L
+
     la, a, lb, b = _mixed_pairs()
     want = po.edr_batch(la, a, lb, b, 5e-4)
     gpu_ctx.set_edr_rows(rows)
+    gpu_ctx.set_tuning(L.GAT_TUNE_EDR_FORM, form)
     try:
         got = G.edr_pairs(gpu_ctx, la, a, lb, b, 5e-4)
+        got2 = G.edr_pairs(gpu_ctx, la, a, lb, b, 5e-3)
     finally:
         gpu_ctx.set_edr_rows(0)
+        gpu_ctx.set_tuning(L.GAT_TUNE_EDR_FORM, 0)
     assert np.array_equal(got, want)
+    assert np.array_equal(got2, po.edr_batch(la, a, lb, b, 5e-3))
 
 
 def test_autotune_classes(gpu_ctx):
@@ -123,18 +131,21 @@ def test_device_api_beyond_cooperative_pool(gpu_ctx):
     dev = torch.device("cuda", 0)
     T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
     d = [T(la.astype(np.int32)), T(oa), T(a), T(lb.astype(np.int32)), T(ob), T(b)]
-    out = torch.full((len(la),), -7, dtype=torch.int32, device=dev)
     want = po.edr_batch(la, a, lb, b, 5e-4)
-    gpu_ctx.set_edr_rows(2)
-    try:
-        torch.cuda.synchronize()
-        gpu_ctx.check(L.lib.gat_edr_pairs_dev(gpu_ctx.h, len(la), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
-                                              d[3].data_ptr(), d[4].data_ptr(), d[5].data_ptr(), 5e-4, out.data_ptr()),
-                      "gat_edr_pairs_dev")
-        gpu_ctx.check(L.lib.gat_ctx_sync(gpu_ctx.h), "gat_ctx_sync")
-    finally:
-        gpu_ctx.set_edr_rows(0)
-    assert np.array_equal(out.cpu().numpy(), want)
+    for form in (1, 2):
+        out = torch.full((len(la),), -7, dtype=torch.int32, device=dev)
+        gpu_ctx.set_edr_rows(2)
+        gpu_ctx.set_tuning(L.GAT_TUNE_EDR_FORM, form)
+        try:
+            torch.cuda.synchronize()
+            gpu_ctx.check(L.lib.gat_edr_pairs_dev(gpu_ctx.h, len(la), d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                                  d[3].data_ptr(), d[4].data_ptr(), d[5].data_ptr(), 5e-4, out.data_ptr()),
+                          "gat_edr_pairs_dev")
+            gpu_ctx.check(L.lib.gat_ctx_sync(gpu_ctx.h), "gat_ctx_sync")
+        finally:
+            gpu_ctx.set_edr_rows(0)
+            gpu_ctx.set_tuning(L.GAT_TUNE_EDR_FORM, 0)
+        assert np.array_equal(out.cpu().numpy(), want), form
 
 
 def test_device_api_rejects_bad_lengths(gpu_ctx):
