@@ -286,6 +286,7 @@ int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
     if (knob == GAT_TUNE_EDR_FORM) {
         if (value < 0 || value > 2) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR form must be 0, 1 or 2");
         ctx->edr_form = value;
+        std::lock_guard<std::mutex> tk(ctx->tune_mu);
         ctx->edr_tune.clear();
         return GAT_OK;
     }
@@ -303,6 +304,7 @@ int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
     if (value != 0 && value != 2 && value != 4 && value != 8)
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR rows per lane must be 0 (autotune), 2, 4 or 8");
     ctx->edr_rows = value;
+    std::lock_guard<std::mutex> tk(ctx->tune_mu);
     ctx->edr_tune.clear();
     return GAT_OK;
 }
@@ -312,8 +314,10 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     if (knob == GAT_TUNE_EDR_ROWS)
         *value = ctx->edr_rows;
-    else if (knob == GAT_TUNE_EDR_TUNED)
+    else if (knob == GAT_TUNE_EDR_TUNED) {
+        std::lock_guard<std::mutex> tk(ctx->tune_mu);
         *value = (int)ctx->edr_tune.size();
+    }
     else if (knob == GAT_TUNE_TOPK_CHUNK)
         *value = ctx->topk_chunk;
     else if (knob == GAT_TUNE_EDR_FORM)

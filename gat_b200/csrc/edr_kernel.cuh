@@ -690,10 +690,18 @@ int edr_launch(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_
         }
     }
     if (nc == 1) return launch_shape(ctx, cand[0], src, cap, max_rows, max_cols, u, cells);
-    const uint64_t key = ((uint64_t)Src::kKind << 60) | (ceil_log2(cap) << 40) | (ceil_log2(max_rows) << 20) |
-                         ceil_log2(max_cols);
-    auto hit = ctx->edr_tune.find(key);
-    if (hit != ctx->edr_tune.end()) return launch_shape(ctx, hit->second, src, cap, max_rows, max_cols, u, cells);
+    const uint64_t key = ((uint64_t)Src::kKind << 60) | ((uint64_t)(ctx->edr_rows | ctx->edr_form << 4) << 52) |
+                         (ceil_log2(cap) << 40) | (ceil_log2(max_rows) << 20) | ceil_log2(max_cols);
+    /* worker contexts share their parent's table (one tuning per shape class per device) */
+    gat_ctx* tab = ctx->root ? ctx->root : ctx;
+    {
+        std::lock_guard<std::mutex> lk(tab->tune_mu);
+        auto hit = tab->edr_tune.find(key);
+        if (hit != tab->edr_tune.end()) {
+            const int shape = hit->second;
+            return launch_shape(ctx, shape, src, cap, max_rows, max_cols, u, cells);
+        }
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         if (e0) cudaEventDestroy(e0);
@@ -717,7 +725,10 @@ int edr_launch(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (st == GAT_OK) ctx->edr_tune[key] = best;
+    if (st == GAT_OK) {
+        std::lock_guard<std::mutex> lk(tab->tune_mu);
+        tab->edr_tune[key] = best;
+    }
     return st;
 }
 

@@ -96,7 +96,8 @@ struct gat_ctx {
     int edr_rows = 0;
     int edr_form = 0; /* 0 = autotune, 1 = row tiles, 2 = column tiles */
     int topk_chunk = 0, topk_growth = 0; /* 0 = defaults */
-    std::map<uint64_t, int> edr_tune;
+    std::map<uint64_t, int> edr_tune; /* worker contexts use their root's table */
+    std::mutex tune_mu;
     /* objects that hold device memory of this context's scratch or workers (cached CUDA graphs);
      * released first by gat_ctx_destroy and gat_ctx_trim */
     std::vector<std::pair<void*, void (*)(void*)>> owned;

@@ -1,16 +1,21 @@
 /* Range queries over the Grid (GT-quadtree), STIG and FSG indexes.
  *
  * Pipeline for a batch of queries (all launches on the context stream):
- *   1. candidates  one thread per query walks the index (Grid: quadtree with BoxIntersect,
- *                  Grid.cpp:428-446; STIG: median slabs + leaf MBBs, STIG.cpp:179-252; FSG:
- *                  the rows of the candidate cell rectangle, FSG.cpp:183-262) and emits point
- *                  ranges; a count pass and a scan give each query its item slice.
- *   2. scan        one CTA per query tests every candidate point with the inclusive
- *                  MBB::pInBox (MBB.cpp:21-26) on SoA float32 x/y read with 128-bit loads,
- *                  and either sets trajectory bits in a shared-memory bitmap (id sets: the
- *                  reference's per-query vector<bool>, Grid.cpp:384-387) or compacts hit keys
- *                  with warp ballots and prefix sums (point lists), which it then sorts with a
- *                  stable in-CTA radix sort and de-duplicates.
+ *   1. candidates  64 threads per query walk the index, each its own subtree (Grid: quadtree
+ *                  with BoxIntersect, Grid.cpp:428-446; STIG: median slabs + leaf MBBs,
+ *                  STIG.cpp:179-252; FSG: the rows of the candidate cell rectangle,
+ *                  FSG.cpp:183-262) and emit point ranges, contiguous ranges joined and cut into
+ *                  chunks of at most 1024 points; a count pass and a scan give each thread its
+ *                  item slice.
+ *   2. scan        id sets: persistent CTAs take queries from a counter; each warp scans one
+ *                  chunk at a time with 128-bit loads of x / y / tid and the inclusive
+ *                  MBB::pInBox (MBB.cpp:21-26), inserting the trajectory id of each run of hits
+ *                  into a shared-memory hash set, which is then sorted and written (the
+ *                  reference's per-query vector<bool>, Grid.cpp:384-387, as a sorted id list);
+ *                  queries with more distinct ids than the set holds use a bitmap over all
+ *                  trajectory ids instead. Point lists: one CTA per query compacts hit keys with
+ *                  warp ballots and prefix sums, sorts them with a stable in-CTA radix sort and
+ *                  de-duplicates.
  *   3. offsets     scan of per-query result counts; one CTA per query copies its segment.
  * Plain execution runs the same pipeline once per query.
  */
@@ -70,10 +75,10 @@ __device__ __forceinline__ void set_flag(int32_t* flag, int code) { atomicCAS(fl
 /* ---------------------------------------------------------------- candidates */
 /* emit(pbeg, pend) for each candidate leaf; returns false on stack overflow */
 template <class Emit>
-__device__ bool grid_walk(const GridDev& g, const Box& q, Emit emit) {
+__device__ bool grid_walk(const GridDev& g, const Box& q, Emit emit, int start = 0) {
     int stack[kStack];
     int sp = 0;
-    stack[sp++] = 0;
+    stack[sp++] = start;
     while (sp > 0) {
         int nd = stack[--sp];
         int ch = g.node_child[nd];
@@ -95,10 +100,10 @@ __device__ bool grid_walk(const GridDev& g, const Box& q, Emit emit) {
 }
 
 template <class Emit>
-__device__ bool stig_walk(const StigDev& s, const Box& q, Emit emit) {
+__device__ bool stig_walk(const StigDev& s, const Box& q, Emit emit, int start = 0) {
     int stack[kStack];
     int sp = 0;
-    stack[sp++] = 0;
+    stack[sp++] = start;
     while (sp > 0) {
         int nd = stack[--sp];
         if (s.kind[nd]) {
@@ -121,7 +126,7 @@ __device__ bool stig_walk(const StigDev& s, const Box& q, Emit emit) {
 }
 
 template <class Emit>
-__device__ void fsg_walk(const FsgDev& f, const Box& q, Emit emit) {
+__device__ void fsg_walk(const FsgDev& f, const Box& q, Emit emit, int first = 0, int step = 1) {
     /* FSG::rangeQueryBatchGPU (FSG.cpp:183-262): the border ring plus the interior cover the
      * cells (row, col) for rows g3..g4 and cols g1..g2, addressed row * nx + col without
      * clamping. Row r is one contiguous run of cell ids; ids outside the grid are skipped (the
@@ -130,7 +135,7 @@ __device__ void fsg_walk(const FsgDev& f, const Box& q, Emit emit) {
     int g2 = (int)__fdiv_rn(__fsub_rn(q.xmax, f.rxmin), f.cell);
     int g3 = (int)__fdiv_rn(__fsub_rn(f.rymax, q.ymax), f.cell);
     int g4 = (int)__fdiv_rn(__fsub_rn(f.rymax, q.ymin), f.cell);
-    for (int r = g3; r <= g4; r++) {
+    for (long long r = (long long)g3 + first; r <= g4; r += step) {
         long long lo = (long long)g1 + (long long)r * f.nx;
         long long hi = (long long)g2 + (long long)r * f.nx;
         if (lo < 0) lo = 0;
@@ -141,14 +146,22 @@ __device__ void fsg_walk(const FsgDev& f, const Box& q, Emit emit) {
     }
 }
 
+/* kSub threads per query: thread `sub` takes the path given by its digits (base 4 over
+ * kGridDepth quadtree levels, base 2 over kStigDepth STIG levels), with the traversal's own
+ * intersection tests, and walks the subtree it reaches; a leaf met on the way belongs to the
+ * thread whose remaining digits are all zero. FSG rows are dealt round robin. Concatenated in
+ * thread order the items are the sequential traversal's, cut at subtree boundaries. */
+constexpr int kGridDepth = 3, kStigDepth = 6, kSub = 64;
+
 template <int KIND>
 __global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, int nq, const int64_t* ioff,
                         int64_t* icnt, int2* items, int32_t* flag) {
-    int qi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (qi >= nq) return;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (int64_t)nq * kSub) return;
+    const int qi = (int)(tid / kSub), sub = (int)(tid % kSub);
     Box q = load_box(queries, qi);
     int64_t cnt = 0;
-    int64_t w = ioff ? ioff[qi] : 0;
+    int64_t w = ioff ? ioff[tid] : 0;
     /* Ranges that continue the previous one (neighbouring leaves / cells are contiguous in the
      * index's point order) are joined, and everything is cut into chunks of at most kChunk
      * points ending on multiples of 4, so the warps of the scan get balanced, 16-byte-aligned
@@ -174,12 +187,49 @@ __global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, 
         cur_e = e;
     };
     bool ok = true;
-    if (KIND == GAT_INDEX_GRID) ok = grid_walk(g, q, emit);
-    if (KIND == GAT_INDEX_STIG) ok = stig_walk(s, q, emit);
-    if (KIND == GAT_INDEX_FSG) fsg_walk(f, q, emit);
+    if (KIND == GAT_INDEX_GRID) {
+        int nd = 0; /* the root is taken without a test (Grid.cpp:428-446) */
+        bool walk = true;
+        for (int lev = 0; lev < kGridDepth && walk; lev++) {
+            const int ch = g.node_child[nd];
+            if (ch < 0) {
+                if ((sub & ((1 << (2 * (kGridDepth - lev))) - 1)) == 0) emit(g.node_pbeg[nd], g.node_pend[nd]);
+                walk = false;
+                break;
+            }
+            const int c = ch + ((sub >> (2 * (kGridDepth - 1 - lev))) & 3);
+            const float4 m = g.node_mbb[c];
+            if (!box_intersect(q, Box{m.x, m.y, m.z, m.w})) walk = false;
+            nd = c;
+        }
+        if (walk) ok = grid_walk(g, q, emit, nd);
+    }
+    if (KIND == GAT_INDEX_STIG) {
+        int nd = 0;
+        bool walk = true;
+        for (int lev = 0; lev < kStigDepth && walk; lev++) {
+            if (s.kind[nd]) {
+                if ((sub & ((1 << (kStigDepth - lev)) - 1)) == 0) {
+                    const float4 m = s.mbb[nd];
+                    if (box_intersect(Box{m.x, m.y, m.z, m.w}, q)) emit(s.lo[nd], s.hi[nd] + 1);
+                }
+                walk = false;
+                break;
+            }
+            const float lo = s.dim[nd] == 0 ? q.xmin : q.ymin;
+            const float hi = s.dim[nd] == 0 ? q.xmax : q.ymax;
+            const float med = s.median[nd];
+            const bool right = (sub >> (kStigDepth - 1 - lev)) & 1;
+            const bool go = right ? (!(hi < med) && !(lo > 180.0f)) : (!(hi < 0.0f) && !(lo > med));
+            if (!go) walk = false;
+            nd = right ? s.right[nd] : s.left[nd];
+        }
+        if (walk) ok = stig_walk(s, q, emit, nd);
+    }
+    if (KIND == GAT_INDEX_FSG) fsg_walk(f, q, emit, sub, kSub);
     flush();
     if (!ok) set_flag(flag, GAT_ERR_ARG);
-    if (!ioff) icnt[qi] = cnt;
+    if (!ioff) icnt[tid] = cnt;
 }
 
 /* ---------------------------------------------------------------- block helpers */
@@ -264,7 +314,7 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
         __syncthreads();
         Box q = load_box(queries, qi);
         unsigned long long cand = 0, hits = 0;
-        for (int64_t it = ioff[qi]; it < ioff[qi + 1]; it++) {
+        for (int64_t it = ioff[(int64_t)qi * kSub]; it < ioff[(int64_t)(qi + 1) * kSub]; it++) {
             int2 r = items[it];
             cand += (unsigned long long)(r.y - r.x);
             scan_range(X, Y, r.x, r.y, q, [&](int i) {
@@ -364,7 +414,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
         const int qi = q_sh;
         if (qi >= nq) break;
         const Box q = load_box(queries, qi);
-        const int64_t i0 = ioff[qi], i1 = ioff[qi + 1];
+        const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
         unsigned long long cand = 0, hits = 0;
         for (int64_t it = i0 + warp; it < i1; it += kThreads / 32) {
             /* stop early once the set has overflowed (warp-uniform read) */
@@ -508,7 +558,7 @@ __global__ void __launch_bounds__(kThreads) k_range_points(const gat_mbb* querie
         Box q = load_box(queries, qi);
         /* pass 1: count */
         int c = 0;
-        for (int64_t it = ioff[qi]; it < ioff[qi + 1]; it++) {
+        for (int64_t it = ioff[(int64_t)qi * kSub]; it < ioff[(int64_t)(qi + 1) * kSub]; it++) {
             int2 r = items[it];
             scan_range(X, Y, r.x, r.y, q, [&](int) { c++; });
         }
@@ -529,7 +579,7 @@ __global__ void __launch_bounds__(kThreads) k_range_points(const gat_mbb* querie
         uint32_t* B = A + total;
         /* pass 2: compact keys in item order, tile by tile (kThreads points per tile) */
         int written = 0;
-        for (int64_t it = ioff[qi]; it < ioff[qi + 1]; it++) {
+        for (int64_t it = ioff[(int64_t)qi * kSub]; it < ioff[(int64_t)(qi + 1) * kSub]; it++) {
             int2 r = items[it];
             for (int t0 = r.x; t0 < r.y; t0 += kThreads) {
                 int i = t0 + threadIdx.x;
@@ -650,9 +700,11 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
               int64_t* total) {
     cudaStream_t s = ctx->stream;
     int st = GAT_OK;
-    int64_t* icnt = (int64_t*)scratch(ctx, S_RANGE_ICNT, (nq + 1) * sizeof(int64_t), &st);
+    /* one count per (query, subtree thread); the item offsets of query q start at q * kSub */
+    const int64_t nsub = (int64_t)nq * kSub;
+    int64_t* icnt = (int64_t*)scratch(ctx, S_RANGE_ICNT, (nsub + 1) * sizeof(int64_t), &st);
     if (!icnt) return st;
-    int tb = 128, gb = (nq + tb - 1) / tb;
+    int tb = 128, gb = (int)((nsub + tb - 1) / tb);
     auto launch_items = [&](const int64_t* ioff, int64_t* cnt, int2* items) {
         switch (ix->kind) {
             case GAT_INDEX_GRID:
@@ -667,10 +719,10 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         count_launch(ctx);
     };
     launch_items(nullptr, icnt, nullptr);
-    int64_t* ioff = (int64_t*)scratch(ctx, S_RANGE_IOFF, (nq + 1) * sizeof(int64_t), &st);
+    int64_t* ioff = (int64_t*)scratch(ctx, S_RANGE_IOFF, (nsub + 1) * sizeof(int64_t), &st);
     if (!ioff) return st;
-    if ((st = scan_i64(ctx, icnt, ioff, nq)) != GAT_OK) return st;
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, ioff + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+    if ((st = scan_i64(ctx, icnt, ioff, nsub)) != GAT_OK) return st;
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, ioff + nsub, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
     GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
     int64_t nitems = ctx->h_pinned[0];
     int2* items = (int2*)scratch(ctx, S_RANGE_ITEMS, (nitems + 1) * sizeof(int2), &st);
