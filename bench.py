@@ -332,12 +332,12 @@ def cpu_baseline_c2(t, qids, sample=32, reps=1):
     queries, compiled from its sources (oracle/_ref/gatref); the oracle port otherwise."""
     from oracle import pyoracle as po
 
-    qs = np.asarray(qids[:sample], np.int32)
+    qs = np.asarray(qids[::max(1, len(qids) // sample)][:sample], np.int32)
     if po.ref_available():
         r = po.RefRunner().topk(t, qs, (121.0, 30.7, 122.0, 31.7), C2["cell"], C2["k"], C2["eps"], reps=reps)
         sec = float(np.sum(r["t_reps"]))
         return {"value": round(len(qs) * reps / sec, 3), "unit": "queries/s", "cores": min(os.cpu_count() or 1, len(qs)),
-                "kind": "reference", "sample": f"{len(qs)} of the 256 queries x {reps}, Grid::SimilarityQueryBatchCPUParallel "
+                "kind": "reference", "sample": f"{len(qs)} of the 256 queries (evenly spaced) x {reps}, Grid::SimilarityQueryBatchCPUParallel "
                                                 f"(one thread per query for the bounds, 20 for EDR)"}
     o = po.OracleGrid(t, (121.0, 30.7, 122.0, 31.7), C2["cell"], C2["vparam"], C2["leaf_cap"])
     t0 = time.time()
@@ -355,13 +355,15 @@ def run_reference_c2(args, world, rank):
 
     t, qids = c2_workload(seed=0)
     sample = args.cpu_sample
-    qs = np.asarray(qids[:sample], np.int32)
+    # evenly spaced over the query sample, so light and heavy queries are both represented
+    qs = np.asarray(qids[::max(1, len(qids) // sample)][:sample], np.int32)
     if po.ref_available():
         r = po.RefRunner().topk(t, qs, (121.0, 30.7, 122.0, 31.7), C2["cell"], C2["k"], C2["eps"], reps=args.warmup + args.steps)
         times = list(r["t_reps"])[args.warmup:]
         kind = "reference"
         cores = min(os.cpu_count() or 1, len(qs))
-        desc = f"{len(qs)} of the 256 queries per step, Grid::SimilarityQueryBatchCPUParallel compiled from the reference"
+        desc = (f"{len(qs)} of the 256 queries (every {max(1, len(qids) // sample)}th) per step, "
+                "Grid::SimilarityQueryBatchCPUParallel compiled from the reference")
     else:
         o = __import__("oracle.pyoracle", fromlist=["OracleGrid"]).OracleGrid(t, (121.0, 30.7, 122.0, 31.7), C2["cell"], 2, 512)
         times = []

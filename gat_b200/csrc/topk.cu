@@ -850,7 +850,8 @@ int topk_batch(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len,
      * kernels of an empty round exit at once). Later rounds, and every round of a batch, read
      * the exact pair count first; it is zero once no query can extend (every query at the end
      * of its order or with its next bound above W). */
-    const int blind_rounds = R.lone ? 2 : 0;
+    /* with per-kernel timing on, rounds follow the exact sizes, as the query graph's loop does */
+    const int blind_rounds = (R.lone && !ctx->timing) ? 2 : 0;
     int64_t chunk_r = R.chunk0;
     for (int r = 0; r < R.rounds; r++) {
         topk_plan(ctx, R);
