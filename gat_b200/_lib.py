@@ -87,6 +87,9 @@ SIGNATURES = [
     ("gat_server_request_times", c_int, [c_p, c_i64, P_i64]),
     ("gat_server_release", c_int, [c_p, c_i64]),
     ("gat_server_stats", c_int, [c_p, P_i64]),
+    ("gat_traj_file_info", c_int, [C.c_char_p, P_i32, P_i64, P_f32]),
+    ("gat_traj_file_read", c_int, [C.c_char_p, c_int, c_i64, P_i32, P_f32, P_f32, P_i32]),
+    ("gat_traj_file_write", c_int, [C.c_char_p, c_int, P_i32, P_f32, P_f32, P_i32, P_f32]),
     ("gat_gen_lengths", c_int, [c_int, c_int, c_d, c_d, c_int, c_int, c_u64, P_i32]),
     ("gat_gen_walks", c_int, [c_int, P_i32, P_f32, c_d, c_u64, P_f32, P_f32]),
     ("gat_gen_boxes", c_int, [c_int, c_int, c_d, c_d, P_f32, c_u64, P_f32]),

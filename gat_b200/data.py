@@ -6,6 +6,7 @@ with the shapes and distributions of the five workloads (random walks in the
 """
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
@@ -125,3 +126,28 @@ def config4_pairs(seed: int = 0, npairs: int = 4096, lo: int = 16, hi: int = 409
     lb = lengths(npairs, L.GAT_LEN_LOGUNIFORM, 0, 0, lo, hi, seed + 1)
     a, b = pairs(la, lb, seed)
     return la, a, lb, b
+
+
+# ---------------------------------------------------------------- trajectory files
+def read_trajectory_file(path: str):
+    """(Trajectories, box, times) from the reference's formatted trajectory file
+    (PreProcess::readTraFromFormatedFile)."""
+    n, npts = C.c_int32(0), C.c_int64(0)
+    box = np.zeros(4, np.float32)
+    _check(L.lib.gat_traj_file_info(path.encode(), C.byref(n), C.byref(npts), _p(box, L.P_f32)), "gat_traj_file_info")
+    lens = np.zeros(n.value, np.int32)
+    lon, lat = np.zeros(npts.value, np.float32), np.zeros(npts.value, np.float32)
+    times = np.zeros(npts.value, np.int32)
+    _check(L.lib.gat_traj_file_read(path.encode(), n.value, npts.value, _p(lens, L.P_i32), _p(lon, L.P_f32),
+                                    _p(lat, L.P_f32), _p(times, L.P_i32)), "gat_traj_file_read")
+    return Trajectories(lens, lon, lat), tuple(float(v) for v in box), times
+
+
+def write_trajectory_file(path: str, t: Trajectories, box=BOX, times=None) -> None:
+    """The reference's formatted trajectory file (PreProcess::writeTraDataToFile)."""
+    lens = np.ascontiguousarray(t.lengths, np.int32)
+    lon, lat = np.ascontiguousarray(t.lon, np.float32), np.ascontiguousarray(t.lat, np.float32)
+    b = np.asarray(box, np.float32)
+    tm = None if times is None else np.ascontiguousarray(times, np.int32)
+    _check(L.lib.gat_traj_file_write(path.encode(), t.n, _p(lens, L.P_i32), _p(lon, L.P_f32), _p(lat, L.P_f32),
+                                     None if tm is None else _p(tm, L.P_i32), _p(b, L.P_f32)), "gat_traj_file_write")

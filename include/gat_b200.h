@@ -239,6 +239,20 @@ int gat_server_release(gat_server* server, int64_t id);
  * [5] peak admitted bytes, [6] largest batch, [7] failed requests */
 int gat_server_stats(gat_server* server, int64_t stats[8]);
 
+/* ---------------------------------------------------------------- trajectory files */
+/* The reference's formatted trajectory file (PreProcess.cpp:203-315): the count, the box
+ * (xmin,ymin,xmax,ymax), a line of lengths, then per trajectory one "lat,lon,tid,time;" record
+ * per point. No context needed. gat_traj_file_info reads the three header lines: n, the total
+ * number of points and the box (box may be NULL). gat_traj_file_read fills caller arrays sized
+ * by those counts (GAT_ERR_TRUNCATED when n or points do not match the file; times may be NULL).
+ * gat_traj_file_write writes the reference writer's bytes (times NULL writes 0; a point's tid
+ * field is its trajectory's number). Malformed files and unopenable paths give GAT_ERR_ARG. */
+int gat_traj_file_info(const char* path, int* n, int64_t* points, float box[4]);
+int gat_traj_file_read(const char* path, int n, int64_t points, int32_t* lengths, float* lon, float* lat,
+                       int32_t* times);
+int gat_traj_file_write(const char* path, int n, const int32_t* lengths, const float* lon, const float* lat,
+                        const int32_t* times, const float box[4]);
+
 /* ---------------------------------------------------------------- synthetic inputs */
 enum { GAT_LEN_UNIFORM = 0, GAT_LEN_LOGNORMAL = 1, GAT_LEN_LOGUNIFORM = 2 };
 enum { GAT_SIDE_FIXED = 0, GAT_SIDE_LOGUNIFORM = 1 };

@@ -176,6 +176,44 @@ public:
     float cell_size;
 };
 
+/* PreProcess::readTraFromFormatedFile (PreProcess.cpp:224-315): the formatted trajectory file
+ * into tradb[1..n] (tradb[0] empty, as the reference's global table) and the file's box. */
+inline int readTrajectoryFile(const char* path, std::vector<Trajectory>& tradb, MBB* range = nullptr) {
+    int n = 0;
+    int64_t points = 0;
+    float box[4] = {0, 0, 0, 0};
+    int rc = gat_traj_file_info(path, &n, &points, box);
+    if (rc != GAT_OK) return rc;
+    std::vector<int32_t> len((size_t)n), times((size_t)points);
+    std::vector<float> lon((size_t)points), lat((size_t)points);
+    rc = gat_traj_file_read(path, n, points, len.data(), lon.data(), lat.data(), times.data());
+    if (rc != GAT_OK) return rc;
+    tradb.assign((size_t)n + 1, Trajectory());
+    size_t o = 0;
+    for (int t = 1; t <= n; t++) {
+        tradb[(size_t)t].tid = t;
+        for (int i = 0; i < len[(size_t)t - 1]; i++, o++) tradb[(size_t)t].addSamplePoints(lon[o], lat[o], times[o]);
+    }
+    if (range) *range = MBB(box[0], box[1], box[2], box[3]);
+    return GAT_OK;
+}
+
+/* PreProcess::writeTraDataToFile (PreProcess.cpp:203-222) of tradb[1..n]. */
+inline int writeTrajectoryFile(const char* path, const Trajectory* tradb, int n, const MBB& range) {
+    std::vector<int32_t> len((size_t)n), times;
+    std::vector<float> lon, lat;
+    for (int t = 1; t <= n; t++) {
+        len[(size_t)t - 1] = (int32_t)tradb[t].points.size();
+        for (const SamplePoint& p : tradb[t].points) {
+            lon.push_back(p.lon);
+            lat.push_back(p.lat);
+            times.push_back(p.time);
+        }
+    }
+    const float box[4] = {range.xmin, range.ymin, range.xmax, range.ymax};
+    return gat_traj_file_write(path, n, len.data(), lon.data(), lat.data(), times.data(), box);
+}
+
 /* Per query: offsets[q] .. offsets[q+1] into tids (and pidx for point results). */
 struct RangeResult {
     std::vector<int64_t> offsets;

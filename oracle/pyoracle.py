@@ -369,6 +369,12 @@ class RefRunner:
         self._run(["gtq", d, q, o, repr(float(cell)), leaf_cap, *[repr(float(v)) for v in box], int(layout), threads])
         return read_out(o)
 
+    def wfile(self, traj, path, box):
+        """PreProcess::writeTraDataToFile of the given trajectories (point times 0) to path."""
+        d = self._path("d.bin")
+        write_data(d, traj)
+        self._run(["wfile", d, path, *[repr(float(v)) for v in box]])
+
     def stig(self, traj, queries, block, layout=False):
         d, q, o = self._path("d.bin"), self._path("q.bin"), self._path("o.bin")
         write_data(d, traj)

@@ -28,6 +28,8 @@
  *    of Grid/STIG/FSG/FVTable but never reached by the CPU calls made here; they are defined
  *    below as stubs that abort, so kernel.cu is not needed.
  */
+#include <map>
+#include "PreProcess.h"
 #include <Grid.h>
 #include <STIG.h>
 #include <FSG.h>
@@ -44,6 +46,11 @@
 #include <vector>
 
 Trajectory* tradb = nullptr;
+/* globals PreProcess.cpp refers to (defined in the reference's main.cpp, not linked here) */
+std::map<std::string, tidLinkTable*> vidTotid;
+std::map<std::string, tidLinkTable*>::iterator iter;
+std::string baseDate;
+int DaysBetween2Date(std::string, std::string) { return 0; }
 void* baseAddrGPU = nullptr;
 double gat_ref_epsilon = 0.005;
 int gat_ref_leaf_cap = 20000;
@@ -699,6 +706,22 @@ int cmd_nbr(int argc, char** argv) {
 
 }  // namespace
 
+/* wfile DATA OUT xmin ymin xmax ymax: PreProcess::writeTraDataToFile (PreProcess.cpp:203-222)
+ * over the trajectories of DATA (point times 0) */
+int cmd_wfile(int argc, char** argv) {
+    if (argc < 8) die("usage: gatref wfile DATA OUT xmin ymin xmax ymax");
+    Data d = read_data(argv[2]);
+    load_tradb(d);
+    PreProcess pp;
+    pp.maxTid = d.n;
+    pp.xmin = (float)atof(argv[4]);
+    pp.ymin = (float)atof(argv[5]);
+    pp.xmax = (float)atof(argv[6]);
+    pp.ymax = (float)atof(argv[7]);
+    pp.writeTraDataToFile(argv[3]);
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 2) die("usage: gatref {gtq|stig|fsg|edr|fvlb|topk} ...");
     std::string c = argv[1];
@@ -709,5 +732,6 @@ int main(int argc, char** argv) {
     if (c == "fvlb") return cmd_fvlb(argc, argv);
     if (c == "topk") return cmd_topk(argc, argv);
     if (c == "nbr") return cmd_nbr(argc, argv);
+    if (c == "wfile") return cmd_wfile(argc, argv);
     die("unknown command");
 }

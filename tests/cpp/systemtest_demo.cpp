@@ -2,7 +2,7 @@
 // a seeded synthetic set, runs the SystemTest entry points and the batch forms, and prints every
 // result as "name count v0 v1 ..." lines for the test that checks them against the oracle.
 //
-//   systemtest_demo <device> <n_trajectories>
+//   systemtest_demo <device> <n_trajectories> [trajectory file to write and read back]
 //
 // device < 0 runs host-only: the indexes are built, the queries return GAT_ERR_STATE.
 #include <cstdio>
@@ -34,6 +34,25 @@ int main(int argc, char** argv) {
     for (int t = 1; t <= n; t++) {
         tradb[t].tid = t;
         for (int i = 0; i < len[t - 1]; i++, o++) tradb[t].addSamplePoints(lon[o], lat[o], i);
+    }
+    if (argc > 3) {
+        /* the reference's file format: write, read back, and read back the rewritten file */
+        const gat::MBB box_mbb(box[0], box[1], box[2], box[3]);
+        std::vector<gat::Trajectory> back, again;
+        gat::MBB r1, r2;
+        const std::string p2 = std::string(argv[3]) + ".2";
+        int rc = gat::writeTrajectoryFile(argv[3], tradb.data(), n, box_mbb);
+        rc = rc ? rc : gat::readTrajectoryFile(argv[3], back, &r1);
+        rc = rc ? rc : gat::writeTrajectoryFile(p2.c_str(), back.data(), n, r1);
+        rc = rc ? rc : gat::readTrajectoryFile(p2.c_str(), again, &r2);
+        bool same = rc == GAT_OK && (int)back.size() == n + 1;
+        for (int t = 1; same && t <= n; t++) {
+            same = back[t].points.size() == tradb[t].points.size() && again[t].points.size() == back[t].points.size();
+            for (size_t i = 0; same && i < back[t].points.size(); i++)
+                same = back[t].points[i].lon == again[t].points[i].lon && back[t].points[i].lat == again[t].points[i].lat &&
+                       back[t].points[i].time == (int)i;
+        }
+        printf("file_roundtrip %d\n", same ? 1 : 0);
     }
     try {
         gat::Context ctx(device);

@@ -23,13 +23,13 @@ def demo(tmp_path_factory):
     return exe
 
 
-def run(exe, device, n=2000):
-    r = subprocess.run([exe, str(device), str(n)], capture_output=True, text=True, timeout=600)
+def run(exe, device, n=2000, path=None):
+    r = subprocess.run([exe, str(device), str(n)] + ([path] if path else []), capture_output=True, text=True, timeout=600)
     out = {}
     for line in r.stdout.splitlines():
         f = line.split()
         if len(f) >= 2 and f[0] in ("build", "rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest",
-                                    "rangeQueryBatch", "similarityQueryTest"):
+                                    "rangeQueryBatch", "similarityQueryTest", "file_roundtrip"):
             out[f[0]] = int(f[1])
         elif len(f) >= 2:
             out[f[0]] = np.array([int(x) for x in f[2:]], np.int64)
@@ -37,12 +37,12 @@ def run(exe, device, n=2000):
     return r.returncode, out, r.stdout + r.stderr
 
 
-def test_host_only(demo):
+def test_host_only(demo, tmp_path):
     """Without a GPU the indexes build through the C++ classes and every query reports
-    GAT_ERR_STATE instead of aborting."""
-    rc, out, log = run(demo, -1)
+    GAT_ERR_STATE instead of aborting; the trajectory file helpers round-trip."""
+    rc, out, log = run(demo, -1, path=str(tmp_path / "tradb.txt"))
     assert rc == 0, log
-    assert out["build"] == 0
+    assert out["build"] == 0 and out["file_roundtrip"] == 1
     for k in ("rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest", "rangeQueryBatch", "similarityQueryTest"):
         assert out[k] == L.GAT_ERR_STATE, (k, log)
 
