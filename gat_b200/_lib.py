@@ -69,6 +69,8 @@ SIGNATURES = [
     ("gat_index_destroy", None, [c_p]),
     ("gat_index_info", c_int, [c_p, P_i64]),
     ("gat_index_points", c_int, [c_p, c_p, c_i64, P_f32, P_f32, P_i32, P_i32]),
+    ("gat_index_save", c_int, [c_p, c_p, C.c_char_p]),
+    ("gat_index_load", c_int, [c_p, c_p, C.c_char_p, C.POINTER(c_p)]),
     ("gat_range_query", c_int, [c_p, c_p, c_p, c_int, c_int, c_int, P_i64, P_i32, P_i32, c_i64, P_i64]),
     ("gat_range_query_dev", c_int, [c_p, c_p, c_p, c_int, c_int, c_int, c_p, c_p, c_p, c_i64, P_i64]),
     ("gat_edr_pairs", c_int, [c_p, c_int, P_i32, P_i64, P_f32, c_i64, P_i32, P_i64, P_f32, c_i64, c_d, P_i32]),

@@ -172,6 +172,23 @@ class Index:
         return dict(kind=int(a[0]), points=int(a[1]), leaves=int(a[2]), nodes=int(a[3]), nx=int(a[4]), ny=int(a[5]),
                     device_bytes=int(a[6]))
 
+    def save(self, path: str) -> None:
+        """Index snapshot (gat_index_save): reload with Index.load instead of rebuilding."""
+        self.ctx.check(lib.gat_index_save(self.ctx.h, self.h, path.encode()), "gat_index_save")
+
+    @staticmethod
+    def load(ctx: "Context", db: "TrajectorySet", path: str) -> "Index":
+        """The index saved at path, over the trajectory set it was built from."""
+        h = C.c_void_p()
+        ctx.check(lib.gat_index_load(ctx.h, db.h, path.encode(), C.byref(h)), "gat_index_load")
+        a = np.zeros(8, np.int64)
+        lib.gat_index_info(h, _p(a, L.P_i64))
+        cls = {L.GAT_INDEX_GRID: Grid, L.GAT_INDEX_STIG: STIG, L.GAT_INDEX_FSG: FSG}[int(a[0])]
+        ix = cls.__new__(cls)
+        Index.__init__(ix, ctx, db)
+        ix.h = h
+        return ix
+
     def points(self):
         n = self.info()["points"]
         x, y = np.zeros(n, np.float32), np.zeros(n, np.float32)

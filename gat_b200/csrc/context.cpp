@@ -80,6 +80,7 @@ void* index_alloc(gat_index* ix, size_t bytes, int* status) {
         return nullptr;
     }
     ix->allocs.push_back(p);
+    ix->alloc_bytes.push_back(bytes ? bytes : 16);
     ix->device_bytes += bytes;
     return p;
 }

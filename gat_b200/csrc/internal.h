@@ -123,7 +123,8 @@ struct gat_index {
     int64_t npoints = 0;
     int pidx_bits = 0;
     size_t device_bytes = 0;
-    std::vector<void*> allocs;
+    std::vector<void*> allocs;        /* device arrays in upload order (index snapshots rely on it) */
+    std::vector<size_t> alloc_bytes;
     /* points in index order */
     float* d_x = nullptr;
     float* d_y = nullptr;

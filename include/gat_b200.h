@@ -135,6 +135,14 @@ int gat_index_info(const gat_index* index, int64_t info[8]);
 int gat_index_points(gat_ctx* ctx, const gat_index* index, int64_t n, float* x, float* y,
                      int32_t* tid, int32_t* pidx);
 
+/* Index snapshots (no counterpart in the reference): gat_index_save writes a built index (any
+ * kind) to a file; gat_index_load rebuilds it on a context from that file and the trajectory set
+ * it was built over, without sorting the set again. The file records a hash of the set's
+ * lengths and coordinates; a different set, a truncated or corrupted file, or a file of another
+ * build gives GAT_ERR_ARG. Saving needs a device context. */
+int gat_index_save(gat_ctx* ctx, const gat_index* index, const char* path);
+int gat_index_load(gat_ctx* ctx, const gat_db* db, const char* path, gat_index** out);
+
 /* ---------------------------------------------------------------- range query */
 /* Per query, the result set in the reference's inclusive MBB::pInBox semantics (MBB.cpp:21)
  * over the index's candidate leaves / blocks / cells. offsets has nq + 1 entries (CSR);

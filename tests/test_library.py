@@ -134,3 +134,20 @@ def test_topk_walk_knobs(host_ctx):
         for v in bad:
             with pytest.raises(G.GatError):
                 host_ctx.set_tuning(knob, v)
+
+
+def test_snapshot_errors(host_ctx, tmp_path):
+    """Saving needs a device context; loading refuses missing and foreign files."""
+    t = D.walks(D.lengths(50, 0, 0, 0, 1, 20, 25), 25)
+    db = G.TrajectorySet(host_ctx, t)
+    g = G.Grid(host_ctx, db, D.BOX, 0.01)
+    with pytest.raises(G.GatError) as e:
+        g.save(str(tmp_path / "g.idx"))
+    assert e.value.status == L.GAT_ERR_STATE
+    with pytest.raises(G.GatError) as e:
+        G.api.Index.load(host_ctx, db, str(tmp_path / "missing.idx"))
+    assert e.value.status == L.GAT_ERR_ARG
+    (tmp_path / "junk.idx").write_bytes(b"GATIDX01" + bytes(64))
+    with pytest.raises(G.GatError) as e:
+        G.api.Index.load(host_ctx, db, str(tmp_path / "junk.idx"))
+    assert e.value.status == L.GAT_ERR_ARG
