@@ -43,7 +43,8 @@ class ServerConfig(C.Structure):
     _fields_ = [("lanes", c_int), ("budget_bytes", c_i64), ("max_range_batch", c_int), ("max_topk_batch", c_int)]
 
 
-GAT_TUNE_EDR_ROWS, GAT_TUNE_EDR_TUNED, GAT_TUNE_TOPK_CHUNK, GAT_TUNE_TOPK_GROWTH, GAT_TUNE_EDR_FORM = 1, 2, 3, 4, 5
+(GAT_TUNE_EDR_ROWS, GAT_TUNE_EDR_TUNED, GAT_TUNE_TOPK_CHUNK, GAT_TUNE_TOPK_GROWTH, GAT_TUNE_EDR_FORM,
+ GAT_TUNE_INDEX_BUILD) = 1, 2, 3, 4, 5, 6
 
 # (name, restype, argtypes) for every symbol of include/gat_b200.h
 SIGNATURES = [

@@ -301,6 +301,11 @@ int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
         ctx->topk_growth = value;
         return GAT_OK;
     }
+    if (knob == GAT_TUNE_INDEX_BUILD) {
+        if (value < 0 || value > 2) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: index build must be 0, 1 or 2");
+        ctx->index_build = value;
+        return GAT_OK;
+    }
     if (knob != GAT_TUNE_EDR_ROWS) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: unknown knob");
     if (value != 0 && value != 2 && value != 4 && value != 8)
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR rows per lane must be 0 (autotune), 2, 4 or 8");
@@ -325,6 +330,8 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
         *value = ctx->edr_form;
     else if (knob == GAT_TUNE_TOPK_GROWTH)
         *value = ctx->topk_growth;
+    else if (knob == GAT_TUNE_INDEX_BUILD)
+        *value = ctx->index_build;
     else
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_get_tuning: unknown knob");
     return GAT_OK;

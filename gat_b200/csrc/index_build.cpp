@@ -1,11 +1,12 @@
-/* Host builders of the three range indexes, in the reference's exact layouts, uploaded to HBM.
+/* Builders of the three range indexes, in the reference's exact layouts, uploaded to HBM.
  *
  * The builders reproduce the reference's float arithmetic (cell assignment, cell and node MBBs)
  * with the same expressions in the same types and no FP contraction, so every point lands in
  * the same cell and every node gets the same MBB as in the reference. The work is organised
  * differently: runs are produced per trajectory in parallel and placed with a stable counting
  * sort by cell, which yields the reference's order (cells ascending, trajectories ascending
- * within a cell, runs in trajectory order) without its per-cell linked lists.
+ * within a cell, runs in trajectory order) without its per-cell linked lists. On a context with
+ * a device the Grid and FSG placements run there instead (index_gpu.cu), with the same result.
  */
 #include <algorithm>
 #include <atomic>
@@ -211,6 +212,61 @@ int upload_points(gat_index* ix) {
     return GAT_OK;
 }
 
+/* Whether points are placed on the device (GAT_TUNE_INDEX_BUILD); GAT_ERR_STATE when the device
+ * is asked for on a host-only context. */
+int use_device(gat_index* ix, const char* what, bool* dev) {
+    const gat_ctx* ctx = ix->ctx;
+    if (ctx->index_build == 2 && ctx->device < 0)
+        return fail(ix->ctx, GAT_ERR_STATE, std::string(what) + ": device build asked for on a host-only context");
+    *dev = ctx->device >= 0 && ctx->index_build != 1;
+    return GAT_OK;
+}
+
+/* Host placement for the Grid: runs, the stable counting sort by cell and the frequency vectors
+ * over virtual cells cell >> vparam (Grid.cpp:152-166; FVTable.cpp:18-30). cb stays empty when a
+ * point lies outside the grid. */
+template <class CellOf>
+void host_place_grid(gat_index* ix, const CellOf& cell_of, int vparam, std::vector<int64_t>& cb,
+                     std::vector<int64_t>& fv_off, std::vector<int32_t>& fv_cell, std::vector<int32_t>& fv_cnt) {
+    const gat_db* db = ix->db;
+    RunSet rs;
+    if (make_runs(db, cell_of, rs) != GAT_OK) return;
+    place_points(db, rs, ix->grid.cellnum, ix, cb);
+    int n = db->n;
+    fv_off.assign(n + 2, 0);
+    std::vector<std::vector<std::pair<int32_t, int32_t>>> fv_tmp(n + 1);
+    parallel_chunks(n, [&](int64_t s, int64_t e, int) {
+        for (int64_t i = s; i < e; i++) {
+            int t = (int)i + 1;
+            auto& v = fv_tmp[t];
+            for (int64_t r = rs.traj_first[t]; r < rs.traj_first[t + 1]; r++) v.push_back({rs.cell[r] >> vparam, rs.count[r]});
+            std::sort(v.begin(), v.end(), [](auto& a, auto& b) { return a.first < b.first; });
+            size_t w = 0;
+            for (size_t k = 0; k < v.size(); k++) {
+                if (w > 0 && v[w - 1].first == v[k].first)
+                    v[w - 1].second += v[k].second;
+                else
+                    v[w++] = v[k];
+            }
+            v.resize(w);
+        }
+    });
+    int maxnnz = 0;
+    for (int t = 0; t <= n; t++) {
+        fv_off[t + 1] = fv_off[t] + (int64_t)fv_tmp[t].size();
+        maxnnz = std::max(maxnnz, (int)fv_tmp[t].size());
+    }
+    ix->fv_max_nnz = maxnnz;
+    ix->fv_entries = fv_off[n + 1];
+    fv_cell.resize(fv_off[n + 1]);
+    fv_cnt.resize(fv_off[n + 1]);
+    for (int t = 0; t <= n; t++)
+        for (size_t k = 0; k < fv_tmp[t].size(); k++) {
+            fv_cell[fv_off[t] + k] = fv_tmp[t][k].first;
+            fv_cnt[fv_off[t] + k] = fv_tmp[t][k].second;
+        }
+}
+
 }  // namespace
 
 /* ================================================================ Grid (GT-quadtree) */
@@ -239,47 +295,25 @@ static int build_grid(gat_index* ix, gat_mbb range, float cell, int vparam, int 
         if (row < 0 || col < 0 || row >= axis || col >= axis) return -1;
         return morton(col, row);
     };
-    RunSet rs;
-    if (make_runs(db, cell_of, rs) != GAT_OK)
-        return fail(ix->ctx, GAT_ERR_ARG, "gat_grid_build: a point lies outside the grid range");
+    bool dev = false;
+    if (int st = use_device(ix, "gat_grid_build", &dev)) return st;
     std::vector<int64_t> cb;
-    place_points(db, rs, g.cellnum, ix, cb);
-
-    /* FVTable over virtual cells cell >> vparam (Grid.cpp:152-166; FVTable.cpp:18-30) */
-    int n = db->n;
-    std::vector<int64_t> fv_off(n + 2, 0);
-    std::vector<std::vector<std::pair<int32_t, int32_t>>> fv_tmp(n + 1);
-    parallel_chunks(n, [&](int64_t s, int64_t e, int) {
-        for (int64_t i = s; i < e; i++) {
-            int t = (int)i + 1;
-            auto& v = fv_tmp[t];
-            for (int64_t r = rs.traj_first[t]; r < rs.traj_first[t + 1]; r++) v.push_back({rs.cell[r] >> vparam, rs.count[r]});
-            std::sort(v.begin(), v.end(), [](auto& a, auto& b) { return a.first < b.first; });
-            size_t w = 0;
-            for (size_t k = 0; k < v.size(); k++) {
-                if (w > 0 && v[w - 1].first == v[k].first)
-                    v[w - 1].second += v[k].second;
-                else
-                    v[w++] = v[k];
-            }
-            v.resize(w);
-        }
-    });
-    int maxnnz = 0;
-    for (int t = 0; t <= n; t++) {
-        fv_off[t + 1] = fv_off[t] + (int64_t)fv_tmp[t].size();
-        maxnnz = std::max(maxnnz, (int)fv_tmp[t].size());
+    std::vector<int64_t> fv_off;
+    std::vector<int32_t> fv_cell, fv_cnt;
+    if (dev) {
+        /* points, cell boundaries and frequency vectors placed on the device (index_gpu.cu) */
+        DevicePlaceArgs a{"gat_grid_build", true, range.xmin, range.ymax, cell, axis, 0, 0, vparam, g.cellnum};
+        DeviceFv fv;
+        if (int st = device_place(ix, a, cb, &fv)) return st;
+        fv_off.swap(fv.off);
+        fv_cell.swap(fv.cell);
+        fv_cnt.swap(fv.cnt);
+        ix->fv_max_nnz = fv.max_nnz;
+        ix->fv_entries = fv_off[db->n + 1];
+    } else {
+        host_place_grid(ix, cell_of, vparam, cb, fv_off, fv_cell, fv_cnt);
+        if (cb.empty()) return fail(ix->ctx, GAT_ERR_ARG, "gat_grid_build: a point lies outside the grid range");
     }
-    ix->fv_max_nnz = maxnnz;
-    ix->fv_entries = fv_off[n + 1];
-    std::vector<int32_t> fv_cell(fv_off[n + 1]), fv_cnt(fv_off[n + 1]);
-    for (int t = 0; t <= n; t++)
-        for (size_t k = 0; k < fv_tmp[t].size(); k++) {
-            fv_cell[fv_off[t] + k] = fv_tmp[t][k].first;
-            fv_cnt[fv_off[t] + k] = fv_tmp[t][k].second;
-        }
-    fv_tmp.clear();
-
     /* quadtree, breadth first (Grid::buildQuadTree, Grid.cpp:58-94) */
     auto cell_box = [&](int c) {
         int col = (int)compact((uint32_t)c), row = (int)compact((uint32_t)c >> 1);
@@ -318,7 +352,7 @@ static int build_grid(gat_index* ix, gat_mbb range, float cell, int vparam, int 
     ix->nodes = g.nnodes;
     ix->leaves = leaves;
 
-    int st = upload_points(ix);
+    int st = dev ? GAT_OK : upload_points(ix);
     if (st != GAT_OK || ix->ctx->device < 0) return st;
     if (!(g.node_mbb = index_upload(ix, nmbb, &st))) return st;
     if (!(g.node_child = index_upload(ix, nchild, &st))) return st;
@@ -498,18 +532,26 @@ static int build_fsg(gat_index* ix, gat_mbb range, float cell) {
         if (row < 0 || col < 0 || row >= ny || col >= nx) return -1;
         return row * nx + col;
     };
-    RunSet rs;
-    if (make_runs(ix->db, cell_of, rs) != GAT_OK)
-        return fail(ix->ctx, GAT_ERR_ARG, "gat_fsg_build: a point lies outside the grid range");
+    bool dev = false;
+    if (int st = use_device(ix, "gat_fsg_build", &dev)) return st;
     std::vector<int64_t> cb;
-    place_points(ix->db, rs, f.cellnum, ix, cb);
+    if (dev) {
+        /* points and cell boundaries placed on the device (index_gpu.cu) */
+        DevicePlaceArgs a{"gat_fsg_build", false, range.xmin, range.ymax, cell, 0, nx, ny, 0, f.cellnum};
+        if (int st = device_place(ix, a, cb, nullptr)) return st;
+    } else {
+        RunSet rs;
+        if (make_runs(ix->db, cell_of, rs) != GAT_OK)
+            return fail(ix->ctx, GAT_ERR_ARG, "gat_fsg_build: a point lies outside the grid range");
+        place_points(ix->db, rs, f.cellnum, ix, cb);
+    }
     std::vector<int32_t> cbeg(f.cellnum), cend(f.cellnum);
     for (int c = 0; c < f.cellnum; c++) {
         cbeg[c] = (int32_t)cb[c];
         cend[c] = (int32_t)cb[c + 1];
     }
     ix->leaves = f.cellnum;
-    int st = upload_points(ix);
+    int st = dev ? GAT_OK : upload_points(ix);
     if (st != GAT_OK || ix->ctx->device < 0) return st;
     if (!(f.cbeg = index_upload(ix, cbeg, &st))) return st;
     if (!(f.cend = index_upload(ix, cend, &st))) return st;

@@ -96,6 +96,7 @@ struct gat_ctx {
     int edr_rows = 0;
     int edr_form = 0; /* 0 = autotune, 1 = row tiles, 2 = column tiles */
     int topk_chunk = 0, topk_growth = 0; /* 0 = defaults */
+    int index_build = 0;                 /* 0 = device when present, 1 = host, 2 = device */
     std::map<uint64_t, int> edr_tune; /* worker contexts use their root's table */
     std::mutex tune_mu;
     /* objects that hold device memory of this context's scratch or workers (cached CUDA graphs);
@@ -162,12 +163,11 @@ template <class T>
 T* index_upload(gat_index* ix, const std::vector<T>& v, int* status) {
     T* p = (T*)index_alloc(ix, v.size() * sizeof(T) + sizeof(T), status);
     if (!p) return nullptr;
-    if (!v.empty()) {
-        cudaError_t e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            *status = cuda_fail(ix->ctx, e, "upload");
-            return nullptr;
-        }
+    cudaError_t e = v.empty() ? cudaSuccess : cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(p + v.size(), 0, sizeof(T)); /* the padding element */
+    if (e != cudaSuccess) {
+        *status = cuda_fail(ix->ctx, e, "upload");
+        return nullptr;
     }
     return p;
 }
@@ -242,6 +242,23 @@ int scan_i64(gat_ctx* ctx, const int64_t* in, int64_t* out, int64_t n);
 int edr_launch_soa(gat_ctx* ctx, int npairs, const int* d_npairs, const int64_t* a_off, const int32_t* a_len,
                    const int64_t* b_off, const int32_t* b_len, int rows_hint, int max_cols, const float2* A,
                    const float2* B, float u, int32_t* d_out, unsigned long long* d_cells);
+
+/* Device placement of a Grid or FSG index's points (index_gpu.cu): cells, the stable sort by
+ * cell, the index-order arrays (allocated and uploaded as the host builder does) with their host
+ * copies, the cell boundaries cb[0..ncells] and, when fv is given, the frequency vectors. */
+struct DevicePlaceArgs {
+    const char* what; /* the API call, for error messages */
+    bool morton;      /* Grid (Morton ids on axis x axis) or FSG (row-major nx x ny) */
+    float rxmin, rymax, cell;
+    int axis, nx, ny, vparam;
+    int64_t ncells;
+};
+struct DeviceFv {
+    std::vector<int64_t> off; /* [n+2] */
+    std::vector<int32_t> cell, cnt;
+    int max_nnz = 0;
+};
+int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& cb, DeviceFv* fv);
 
 }  // namespace gat
 

@@ -136,6 +136,33 @@ def test_topk_walk_knobs(host_ctx):
                 host_ctx.set_tuning(knob, v)
 
 
+def test_index_build_knob(host_ctx):
+    """GAT_TUNE_INDEX_BUILD takes 0, 1 and 2; a device build on a host-only context is refused
+    and the host build (0 or 1) still works there."""
+    t = D.walks(D.lengths(50, 0, 0, 0, 1, 20, 26), 26)
+    db = G.TrajectorySet(host_ctx, t)
+    try:
+        for v in (1, 2, 0):
+            host_ctx.set_tuning(L.GAT_TUNE_INDEX_BUILD, v)
+            assert host_ctx.tuning(L.GAT_TUNE_INDEX_BUILD) == v
+        for v in (-1, 3):
+            with pytest.raises(G.GatError) as e:
+                host_ctx.set_tuning(L.GAT_TUNE_INDEX_BUILD, v)
+            assert e.value.status == L.GAT_ERR_ARG
+        host_ctx.set_tuning(L.GAT_TUNE_INDEX_BUILD, 2)
+        for build in (lambda: G.Grid(host_ctx, db, D.BOX, 0.01), lambda: G.FSG(host_ctx, db, D.BOX, 0.01)):
+            with pytest.raises(G.GatError) as e:
+                build()
+            assert e.value.status == L.GAT_ERR_STATE
+        host_ctx.set_tuning(L.GAT_TUNE_INDEX_BUILD, 1)
+        a = G.Grid(host_ctx, db, D.BOX, 0.01).points()
+        host_ctx.set_tuning(L.GAT_TUNE_INDEX_BUILD, 0)
+        b = G.Grid(host_ctx, db, D.BOX, 0.01).points()
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    finally:
+        host_ctx.set_tuning(L.GAT_TUNE_INDEX_BUILD, 0)
+
+
 def test_snapshot_errors(host_ctx, tmp_path):
     """Saving needs a device context; loading refuses missing and foreign files."""
     t = D.walks(D.lengths(50, 0, 0, 0, 1, 20, 25), 25)
