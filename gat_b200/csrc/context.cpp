@@ -419,6 +419,7 @@ void gat_index_destroy(gat_index* ix) {
     cudaSetDevice(ix->ctx->device);
     cudaStreamSynchronize(ix->ctx->stream);
     for (void* p : ix->allocs) cudaFree(p);
+    if (ix->d_pidx) cudaFree(ix->d_pidx);
     delete ix;
 }
 
@@ -441,6 +442,11 @@ int gat_index_info(const gat_index* ix, int64_t info[8]) {
 int gat_index_points(gat_ctx* ctx, const gat_index* ix, int64_t n, float* x, float* y, int32_t* tid,
                      int32_t* pidx) {
     if (!ctx || !ix || n != ix->npoints) return fail(ctx, GAT_ERR_ARG, "gat_index_points: size mismatch");
+    {
+        /* a device-placed index whose host copies were never asked for: read the device arrays */
+        std::lock_guard<std::mutex> lk(const_cast<gat_index*>(ix)->host_mu);
+        if (ix->host_pending) return index_points_device(ix, x, y, tid, pidx);
+    }
     size_t b = (size_t)n * 4;
     if (x) memcpy(x, ix->h_x.data(), b);
     if (y) memcpy(y, ix->h_y.data(), b);

@@ -271,7 +271,6 @@ void host_place_grid(gat_index* ix, const CellOf& cell_of, int vparam, std::vect
 
 /* ================================================================ Grid (GT-quadtree) */
 static int build_grid(gat_index* ix, gat_mbb range, float cell, int vparam, int leaf_cap) {
-    const gat_db* db = ix->db;
     GridDev& g = ix->grid;
     g.rxmin = range.xmin;
     g.rymin = range.ymin;
@@ -300,16 +299,11 @@ static int build_grid(gat_index* ix, gat_mbb range, float cell, int vparam, int 
     std::vector<int64_t> cb;
     std::vector<int64_t> fv_off;
     std::vector<int32_t> fv_cell, fv_cnt;
+    DeviceFvHandle fv_runs;
     if (dev) {
-        /* points, cell boundaries and frequency vectors placed on the device (index_gpu.cu) */
+        /* points, cell boundaries and frequency-vector runs placed on the device (index_gpu.cu) */
         DevicePlaceArgs a{"gat_grid_build", true, range.xmin, range.ymax, cell, axis, 0, 0, vparam, g.cellnum};
-        DeviceFv fv;
-        if (int st = device_place(ix, a, cb, &fv)) return st;
-        fv_off.swap(fv.off);
-        fv_cell.swap(fv.cell);
-        fv_cnt.swap(fv.cnt);
-        ix->fv_max_nnz = fv.max_nnz;
-        ix->fv_entries = fv_off[db->n + 1];
+        if (int st = device_place(ix, a, cb, &fv_runs)) return st;
     } else {
         host_place_grid(ix, cell_of, vparam, cb, fv_off, fv_cell, fv_cnt);
         if (cb.empty()) return fail(ix->ctx, GAT_ERR_ARG, "gat_grid_build: a point lies outside the grid range");
@@ -358,6 +352,7 @@ static int build_grid(gat_index* ix, gat_mbb range, float cell, int vparam, int 
     if (!(g.node_child = index_upload(ix, nchild, &st))) return st;
     if (!(g.node_pbeg = index_upload(ix, npbeg, &st))) return st;
     if (!(g.node_pend = index_upload(ix, npend, &st))) return st;
+    if (dev) return device_fv(ix, fv_runs.get());
     if (!(ix->d_fv_off = index_upload(ix, fv_off, &st))) return st;
     if (!(ix->d_fv_cell = index_upload(ix, fv_cell, &st))) return st;
     if (!(ix->d_fv_cnt = index_upload(ix, fv_cnt, &st))) return st;

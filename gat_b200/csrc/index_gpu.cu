@@ -11,7 +11,8 @@
  * each trajectory's (virtual cell, count) list in ascending cell order, which is what merging
  * the runs' (cell >> vparam, count) pairs per trajectory yields (Grid.cpp:152-166).
  *
- * The quadtree stays on the host: it is a walk over the cell boundaries only.
+ * Only the cell boundaries travel to the host, where the quadtree is a walk over them; the host
+ * copies of the points are downloaded when first asked for (gat_index_points, snapshots).
  * The sorts and the run-length encoding are CUB's (the CUDA toolkit's header library); an index
  * build runs once per trajectory set and is not on the query path. */
 #include <cub/device/device_radix_sort.cuh>
@@ -90,10 +91,10 @@ __global__ void k_point_cells(int64_t P, int n, const int64_t* __restrict__ off,
 }
 
 /* index-order arrays from the sorted positions; key = tid << pidx_bits | pidx, or 0 when the
- * pair does not fit 32 bits (pidx_bits < 0) */
+ * pair does not fit 32 bits (pidx_bits < 0; the point index then goes to pidx) */
 __global__ void k_gather_points(int64_t P, const int32_t* __restrict__ order, const float2* __restrict__ xy,
                                 const int32_t* __restrict__ tid_in, const int32_t* __restrict__ pidx_in, float* x,
-                                float* y, int32_t* tid, int32_t* pidx, uint32_t* key, int pidx_bits) {
+                                float* y, int32_t* tid, uint32_t* key, int32_t* pidx, int pidx_bits) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x) {
         const int s = order[i];
         const float2 v = xy[s];
@@ -101,30 +102,41 @@ __global__ void k_gather_points(int64_t P, const int32_t* __restrict__ order, co
         y[i] = v.y;
         const int t = tid_in[s], k = pidx_in[s];
         tid[i] = t;
-        pidx[i] = k;
         key[i] = pidx_bits >= 0 ? ((uint32_t)t << pidx_bits) | (uint32_t)k : 0u;
+        if (pidx) pidx[i] = k;
     }
 }
 
-/* cb[c] = the first sorted position whose cell is >= c, for c = 0..ncells */
-__global__ void k_cell_bounds(int64_t P, int64_t ncells, const uint32_t* __restrict__ cells, int64_t* cb) {
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c <= ncells; c += (int64_t)gridDim.x * blockDim.x) {
+/* bound[j] = the first position p in the sorted keys with keys[p] >= j << shift, j = 0..m */
+template <class K>
+__global__ void k_bounds(int64_t P, int64_t m, const K* __restrict__ keys, int shift, int64_t* bound) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j <= m; j += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long want = (unsigned long long)j << shift;
         int64_t lo = 0, hi = P;
         while (lo < hi) {
             const int64_t mid = (lo + hi) >> 1;
-            if ((int64_t)cells[mid] < c)
+            if ((unsigned long long)keys[mid] < want)
                 lo = mid + 1;
             else
                 hi = mid;
         }
-        cb[c] = lo;
+        bound[j] = lo;
     }
 }
 
-/* temporaries of one build, freed on every exit */
+/* frequency-vector cells: the low half of each (trajectory, virtual cell) run key */
+__global__ void k_fv_cells(int64_t R, const unsigned long long* __restrict__ runs, int32_t* cell) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x)
+        cell[r] = (int32_t)(runs[r] & 0xffffffffull);
+}
+
+/* device allocations of one build, freed with it */
 struct Temps {
     std::vector<void*> ptrs;
     cudaError_t err = cudaSuccess;
+    Temps() = default;
+    Temps(const Temps&) = delete;
+    Temps& operator=(const Temps&) = delete;
     ~Temps() {
         for (void* p : ptrs) cudaFree(p);
     }
@@ -152,7 +164,16 @@ int grid_size(const gat_ctx* ctx, int64_t work) {
 
 }  // namespace
 
-int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& cb, DeviceFv* fv) {
+/* the Grid's sorted, counted (trajectory, virtual cell) runs between device_place and device_fv */
+struct DeviceFvRuns {
+    Temps tmp;
+    unsigned long long* runs = nullptr;
+    int32_t* cnt = nullptr;
+    int32_t* nruns = nullptr;
+};
+void DeviceFvRunsFree::operator()(DeviceFvRuns* r) const { delete r; }
+
+int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& cb, DeviceFvHandle* fv) {
     gat_ctx* ctx = ix->ctx;
     const gat_db* db = ix->db;
     cudaStream_t s = ctx->stream;
@@ -166,7 +187,6 @@ int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& 
     int32_t* order = tmp.get<int32_t>(P);
     int32_t* tid0 = tmp.get<int32_t>(P);
     int32_t* pidx0 = tmp.get<int32_t>(P);
-    int32_t* pidx1 = tmp.get<int32_t>(P);
     int64_t* d_cb = tmp.get<int64_t>((size_t)a.ncells + 1);
     unsigned long long* fvk = fv ? tmp.get<unsigned long long>(P) : nullptr;
     if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
@@ -210,75 +230,123 @@ int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& 
     ix->d_y = dy;
     ix->d_tid = dt;
     ix->d_key = dk;
+    if (pidx_bits < 0) GAT_CUDA_TRY(ctx, cudaMalloc(&ix->d_pidx, std::max<size_t>((size_t)P, 1) * 4), "index build");
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(dx + P, 0, 4, s), "index build");
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(dy + P, 0, 4, s), "index build");
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(dt + P, 0, 4, s), "index build");
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(dk + P, 0, 4, s), "index build");
     if (P > 0) {
-        k_gather_points<<<grid_size(ctx, P), 256, 0, s>>>(P, order, db->d_xy, tid0, pidx0, dx, dy, dt, pidx1, dk, pidx_bits);
+        k_gather_points<<<grid_size(ctx, P), 256, 0, s>>>(P, order, db->d_xy, tid0, pidx0, dx, dy, dt, dk, ix->d_pidx,
+                                                          pidx_bits);
         count_launch(ctx);
     }
-    k_cell_bounds<<<grid_size(ctx, a.ncells + 1), 256, 0, s>>>(P, a.ncells, cells_s, d_cb);
+    k_bounds<uint32_t><<<grid_size(ctx, a.ncells + 1), 256, 0, s>>>(P, a.ncells, cells_s, 0, d_cb);
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (gather)");
-    /* host copies: gat_index_points, snapshots and the quadtree walk read them */
-    ix->h_x.resize(P);
-    ix->h_y.resize(P);
-    ix->h_tid.resize(P);
-    ix->h_pidx.resize(P);
     cb.resize((size_t)a.ncells + 1);
-    if (P > 0) {
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ix->h_x.data(), dx, P * 4, cudaMemcpyDeviceToHost, s), "index build");
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ix->h_y.data(), dy, P * 4, cudaMemcpyDeviceToHost, s), "index build");
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ix->h_tid.data(), dt, P * 4, cudaMemcpyDeviceToHost, s), "index build");
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ix->h_pidx.data(), pidx1, P * 4, cudaMemcpyDeviceToHost, s), "index build");
-    }
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cb.data(), d_cb, cb.size() * 8, cudaMemcpyDeviceToHost, s), "index build");
+    ix->host_pending = true;
     if (fv) {
-        fv->off.assign((size_t)n + 2, 0);
-        fv->cell.clear();
-        fv->cnt.clear();
-        fv->max_nnz = 0;
+        /* (trajectory, virtual cell) keys sorted and run-length counted; kept for device_fv */
+        DeviceFvHandle r(new DeviceFvRuns());
+        unsigned long long* fvk_s = r->tmp.get<unsigned long long>(P);
+        r->runs = r->tmp.get<unsigned long long>(P);
+        r->cnt = r->tmp.get<int32_t>(P + 1);
+        r->nruns = r->tmp.get<int32_t>(1);
+        if (r->tmp.err != cudaSuccess) return cuda_fail(ctx, r->tmp.err, "index build (device temporaries)");
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(r->nruns, 0, 4, s), "index build fv");
         if (P > 0) {
-            unsigned long long* fvk_s = tmp.get<unsigned long long>(P);
-            unsigned long long* uk = tmp.get<unsigned long long>(P);
-            int32_t* cnt = tmp.get<int32_t>(P);
-            int32_t* nruns = tmp.get<int32_t>(1);
-            if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
             /* keys hold the trajectory above bit 32 and the virtual cell below it */
             const int kbits = 32 + bits_to_hold(n);
             size_t b1 = 0, b2 = 0;
             GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortKeys(nullptr, b1, fvk, fvk_s, (int)P, 0, kbits, s), "index build fv");
-            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(nullptr, b2, fvk_s, uk, cnt, nruns, (int)P, s),
+            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(nullptr, b2, fvk_s, r->runs, r->cnt, r->nruns, (int)P, s),
                          "index build fv");
             void* t2 = tmp.get<char>(std::max(b1, b2));
             if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
             GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortKeys(t2, b1, fvk, fvk_s, (int)P, 0, kbits, s), "index build fv");
-            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(t2, b2, fvk_s, uk, cnt, nruns, (int)P, s), "index build fv");
+            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(t2, b2, fvk_s, r->runs, r->cnt, r->nruns, (int)P, s),
+                         "index build fv");
             count_launch(ctx, 2 * ((kbits + 7) / 8) + 3);
-            int32_t R = 0;
-            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R, nruns, 4, cudaMemcpyDeviceToHost, s), "index build");
-            GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build");
-            std::vector<unsigned long long> hk((size_t)R);
-            fv->cnt.resize((size_t)R);
-            if (R > 0) {
-                GAT_CUDA_TRY(ctx, cudaMemcpyAsync(hk.data(), uk, (size_t)R * 8, cudaMemcpyDeviceToHost, s), "index build");
-                GAT_CUDA_TRY(ctx, cudaMemcpyAsync(fv->cnt.data(), cnt, (size_t)R * 4, cudaMemcpyDeviceToHost, s),
-                             "index build");
-            }
-            GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build");
-            fv->cell.resize((size_t)R);
-            for (int32_t r = 0; r < R; r++) {
-                fv->cell[(size_t)r] = (int32_t)(hk[(size_t)r] & 0xffffffffull);
-                fv->off[(size_t)(hk[(size_t)r] >> 32) + 1]++;
-            }
-            for (int t = 0; t <= n; t++) {
-                fv->max_nnz = std::max<int>(fv->max_nnz, (int)fv->off[(size_t)t + 1]);
-                fv->off[(size_t)t + 1] += fv->off[(size_t)t];
-            }
         }
+        *fv = std::move(r);
     }
+    /* the temporaries are freed on return: wait for the work that reads them */
     GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build");
+    return GAT_OK;
+}
+
+int device_fv(gat_index* ix, DeviceFvRuns* fv) {
+    gat_ctx* ctx = ix->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = ix->db->n;
+    int32_t R = 0;
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R, fv->nruns, 4, cudaMemcpyDeviceToHost, s), "index build fv");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
+    /* sizes and order of the host builder's uploads: fv_off [n+2], fv_cell [R], fv_cnt [R], each
+     * with one zeroed element of padding */
+    int st = GAT_OK;
+    int64_t* off = (int64_t*)index_alloc(ix, (size_t)(n + 3) * 8, &st);
+    int32_t* cell = off ? (int32_t*)index_alloc(ix, (size_t)(R + 1) * 4, &st) : nullptr;
+    int32_t* cnt = cell ? (int32_t*)index_alloc(ix, (size_t)(R + 1) * 4, &st) : nullptr;
+    if (!cnt) return st;
+    ix->d_fv_off = off;
+    ix->d_fv_cell = cell;
+    ix->d_fv_cnt = cnt;
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(off + n + 2, 0, 8, s), "index build fv");
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(cell + R, 0, 4, s), "index build fv");
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(cnt + R, 0, 4, s), "index build fv");
+    if (R > 0) {
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, fv->cnt, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "index build fv");
+        k_fv_cells<<<grid_size(ctx, R), 256, 0, s>>>(R, fv->runs, cell);
+        count_launch(ctx);
+    }
+    /* off[t] = entries of trajectories below t: the first run whose key is >= t << 32 */
+    k_bounds<unsigned long long><<<grid_size(ctx, n + 2), 256, 0, s>>>(R, n + 1, fv->runs, 32, off);
+    count_launch(ctx);
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build fv");
+    std::vector<int64_t> h((size_t)n + 2);
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), off, h.size() * 8, cudaMemcpyDeviceToHost, s), "index build fv");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
+    int mx = 0;
+    for (int t = 0; t <= n; t++) mx = std::max<int>(mx, (int)(h[(size_t)t + 1] - h[(size_t)t]));
+    ix->fv_max_nnz = mx;
+    ix->fv_entries = R;
+    return GAT_OK;
+}
+
+int index_points_device(const gat_index* ix, float* x, float* y, int32_t* tid, int32_t* pidx) {
+    gat_ctx* ctx = ix->ctx;
+    const int64_t P = ix->npoints;
+    if (P == 0) return GAT_OK;
+    cudaSetDevice(ctx->device);
+    const size_t b = (size_t)P * 4;
+    if (x) GAT_CUDA_TRY(ctx, cudaMemcpy(x, ix->d_x, b, cudaMemcpyDeviceToHost), "index points");
+    if (y) GAT_CUDA_TRY(ctx, cudaMemcpy(y, ix->d_y, b, cudaMemcpyDeviceToHost), "index points");
+    if (tid) GAT_CUDA_TRY(ctx, cudaMemcpy(tid, ix->d_tid, b, cudaMemcpyDeviceToHost), "index points");
+    if (pidx && ix->pidx_bits >= 0) {
+        /* the point index is the key's low pidx_bits bits */
+        GAT_CUDA_TRY(ctx, cudaMemcpy(pidx, ix->d_key, b, cudaMemcpyDeviceToHost), "index points");
+        const uint32_t mask = (uint32_t)((1ull << ix->pidx_bits) - 1);
+        for (int64_t i = 0; i < P; i++) pidx[i] = (int32_t)((uint32_t)pidx[i] & mask);
+    } else if (pidx) {
+        GAT_CUDA_TRY(ctx, cudaMemcpy(pidx, ix->d_pidx, b, cudaMemcpyDeviceToHost), "index points");
+    }
+    return GAT_OK;
+}
+
+int index_host_copies(gat_index* ix) {
+    std::lock_guard<std::mutex> lk(ix->host_mu);
+    if (!ix->host_pending) return GAT_OK;
+    const size_t P = (size_t)ix->npoints;
+    std::vector<float> x(P), y(P);
+    std::vector<int32_t> tid(P), pidx(P);
+    if (int st = index_points_device(ix, x.data(), y.data(), tid.data(), pidx.data())) return st;
+    ix->h_x.swap(x);
+    ix->h_y.swap(y);
+    ix->h_tid.swap(tid);
+    ix->h_pidx.swap(pidx);
+    ix->host_pending = false;
     return GAT_OK;
 }
 

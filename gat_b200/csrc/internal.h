@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <functional>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -131,9 +132,13 @@ struct gat_index {
     float* d_y = nullptr;
     uint32_t* d_key = nullptr;
     int32_t* d_tid = nullptr;
-    /* host copies kept for gat_index_points and the tree walks of the builders */
+    /* host copies kept for gat_index_points, snapshots and the tree walks of the builders; an
+     * index placed on the device downloads them on first use (host_pending, under host_mu) */
     std::vector<int32_t> h_tid, h_pidx;
     std::vector<float> h_x, h_y;
+    bool host_pending = false;
+    std::mutex host_mu;
+    int32_t* d_pidx = nullptr; /* device-placed index whose point index does not fit the key */
     int64_t leaves = 0, nodes = 0;
     gat::GridDev grid{};
     gat::StigDev stig{};
@@ -244,8 +249,10 @@ int edr_launch_soa(gat_ctx* ctx, int npairs, const int* d_npairs, const int64_t*
                    const float2* B, float u, int32_t* d_out, unsigned long long* d_cells);
 
 /* Device placement of a Grid or FSG index's points (index_gpu.cu): cells, the stable sort by
- * cell, the index-order arrays (allocated and uploaded as the host builder does) with their host
- * copies, the cell boundaries cb[0..ncells] and, when fv is given, the frequency vectors. */
+ * cell, the index-order arrays (allocated in the host builder's order; host copies deferred) and
+ * the cell boundaries cb[0..ncells]. With fv given it also sorts and counts the Grid's
+ * (trajectory, virtual cell) pairs and keeps them for device_fv, which allocates and fills the
+ * frequency-vector CSR after the quadtree's arrays. */
 struct DevicePlaceArgs {
     const char* what; /* the API call, for error messages */
     bool morton;      /* Grid (Morton ids on axis x axis) or FSG (row-major nx x ny) */
@@ -253,12 +260,18 @@ struct DevicePlaceArgs {
     int axis, nx, ny, vparam;
     int64_t ncells;
 };
-struct DeviceFv {
-    std::vector<int64_t> off; /* [n+2] */
-    std::vector<int32_t> cell, cnt;
-    int max_nnz = 0;
+struct DeviceFvRuns;
+struct DeviceFvRunsFree {
+    void operator()(DeviceFvRuns* r) const;
 };
-int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& cb, DeviceFv* fv);
+using DeviceFvHandle = std::unique_ptr<DeviceFvRuns, DeviceFvRunsFree>;
+int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& cb, DeviceFvHandle* fv);
+int device_fv(gat_index* ix, DeviceFvRuns* fv);
+/* downloads the host copies of a device-placed index (no-op otherwise) */
+int index_host_copies(gat_index* ix);
+/* gat_index_points for a device-placed index without host copies: device arrays straight into
+ * the caller's buffers (any may be NULL); the caller holds ix->host_mu */
+int index_points_device(const gat_index* ix, float* x, float* y, int32_t* tid, int32_t* pidx);
 
 }  // namespace gat
 

@@ -122,6 +122,7 @@ int gat_index_save(gat_ctx* ctx, const gat_index* index, const char* path) {
     gat_index* ix = const_cast<gat_index*>(index);
     if (ix->allocs.size() != fields(ix).size())
         return fail(ctx, GAT_ERR_STATE, "gat_index_save: the index's arrays do not match its kind");
+    if (int st = index_host_copies(ix)) return st;
     FILE* f = fopen(path, "wb");
     if (!f) return fail(ctx, GAT_ERR_ARG, std::string("gat_index_save: cannot open ") + path);
     Out o{f};

@@ -140,3 +140,15 @@ def test_out_of_grid_fails_on_both_paths(gpu_ctx, bad):
             with pytest.raises(G.GatError) as e:
                 build(gpu_ctx, db, kind, mode, cell=0.01)
             assert e.value.status == L.GAT_ERR_ARG
+
+
+def test_point_index_beyond_the_key(gpu_ctx, tmp_path):
+    """2^17 trajectories and one of 40000 points: trajectory and point index need 18 + 16 bits,
+    more than the 32-bit key holds, so the device keeps the point index apart; the host copies
+    read back later must still match the host build's."""
+    lens = np.full(1 << 17, 2, np.int32)
+    lens[1000] = 40000
+    t = D.walks(lens, 65)
+    db = G.TrajectorySet(gpu_ctx, t)
+    assert_same_index(gpu_ctx, db, "grid", tmp_path, cell=0.01)
+    assert_same_index(gpu_ctx, db, "fsg", tmp_path, cell=0.02)
