@@ -36,7 +36,7 @@ GAT_LEN_UNIFORM, GAT_LEN_LOGNORMAL, GAT_LEN_LOGUNIFORM = 0, 1, 2
 GAT_SIDE_FIXED, GAT_SIDE_LOGUNIFORM = 0, 1
 GAT_EDR_MAX_LEN = 16384
 GAT_EDR_NOALLOC_MAX_LEN = 4096
-GAT_KERNEL_EDR, GAT_KERNEL_BOUNDS, GAT_KERNEL_RANGE_SCAN = 0, 1, 2
+GAT_KERNEL_EDR, GAT_KERNEL_BOUNDS, GAT_KERNEL_RANGE_SCAN, GAT_KERNEL_INDEX_BUILD = 0, 1, 2, 3
 class ServerConfig(C.Structure):
     """gat_server_config."""
 

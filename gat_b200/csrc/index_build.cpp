@@ -6,7 +6,7 @@
  * differently: runs are produced per trajectory in parallel and placed with a stable counting
  * sort by cell, which yields the reference's order (cells ascending, trajectories ascending
  * within a cell, runs in trajectory order) without its per-cell linked lists. On a context with
- * a device the Grid and FSG placements run there instead (index_gpu.cu), with the same result.
+ * a device the Grid and FSG builds run there instead (index_gpu.cu), with the same result.
  */
 #include <algorithm>
 #include <atomic>
@@ -296,18 +296,16 @@ static int build_grid(gat_index* ix, gat_mbb range, float cell, int vparam, int 
     };
     bool dev = false;
     if (int st = use_device(ix, "gat_grid_build", &dev)) return st;
+    if (dev) {
+        /* points, quadtree and frequency vectors built in HBM (index_gpu.cu) */
+        DevicePlaceArgs a{"gat_grid_build", true, range.xmin, range.ymax, cell, axis, 0, 0, vparam, g.cellnum};
+        return device_build_grid(ix, a, g.total_level, leaf_cap);
+    }
     std::vector<int64_t> cb;
     std::vector<int64_t> fv_off;
     std::vector<int32_t> fv_cell, fv_cnt;
-    DeviceFvHandle fv_runs;
-    if (dev) {
-        /* points, cell boundaries and frequency-vector runs placed on the device (index_gpu.cu) */
-        DevicePlaceArgs a{"gat_grid_build", true, range.xmin, range.ymax, cell, axis, 0, 0, vparam, g.cellnum};
-        if (int st = device_place(ix, a, cb, &fv_runs)) return st;
-    } else {
-        host_place_grid(ix, cell_of, vparam, cb, fv_off, fv_cell, fv_cnt);
-        if (cb.empty()) return fail(ix->ctx, GAT_ERR_ARG, "gat_grid_build: a point lies outside the grid range");
-    }
+    host_place_grid(ix, cell_of, vparam, cb, fv_off, fv_cell, fv_cnt);
+    if (cb.empty()) return fail(ix->ctx, GAT_ERR_ARG, "gat_grid_build: a point lies outside the grid range");
     /* quadtree, breadth first (Grid::buildQuadTree, Grid.cpp:58-94) */
     auto cell_box = [&](int c) {
         int col = (int)compact((uint32_t)c), row = (int)compact((uint32_t)c >> 1);
@@ -346,13 +344,12 @@ static int build_grid(gat_index* ix, gat_mbb range, float cell, int vparam, int 
     ix->nodes = g.nnodes;
     ix->leaves = leaves;
 
-    int st = dev ? GAT_OK : upload_points(ix);
+    int st = upload_points(ix);
     if (st != GAT_OK || ix->ctx->device < 0) return st;
     if (!(g.node_mbb = index_upload(ix, nmbb, &st))) return st;
     if (!(g.node_child = index_upload(ix, nchild, &st))) return st;
     if (!(g.node_pbeg = index_upload(ix, npbeg, &st))) return st;
     if (!(g.node_pend = index_upload(ix, npend, &st))) return st;
-    if (dev) return device_fv(ix, fv_runs.get());
     if (!(ix->d_fv_off = index_upload(ix, fv_off, &st))) return st;
     if (!(ix->d_fv_cell = index_upload(ix, fv_cell, &st))) return st;
     if (!(ix->d_fv_cnt = index_upload(ix, fv_cnt, &st))) return st;
@@ -529,24 +526,23 @@ static int build_fsg(gat_index* ix, gat_mbb range, float cell) {
     };
     bool dev = false;
     if (int st = use_device(ix, "gat_fsg_build", &dev)) return st;
-    std::vector<int64_t> cb;
     if (dev) {
-        /* points and cell boundaries placed on the device (index_gpu.cu) */
+        /* points and cell ranges built in HBM (index_gpu.cu) */
         DevicePlaceArgs a{"gat_fsg_build", false, range.xmin, range.ymax, cell, 0, nx, ny, 0, f.cellnum};
-        if (int st = device_place(ix, a, cb, nullptr)) return st;
-    } else {
-        RunSet rs;
-        if (make_runs(ix->db, cell_of, rs) != GAT_OK)
-            return fail(ix->ctx, GAT_ERR_ARG, "gat_fsg_build: a point lies outside the grid range");
-        place_points(ix->db, rs, f.cellnum, ix, cb);
+        return device_build_fsg(ix, a);
     }
+    std::vector<int64_t> cb;
+    RunSet rs;
+    if (make_runs(ix->db, cell_of, rs) != GAT_OK)
+        return fail(ix->ctx, GAT_ERR_ARG, "gat_fsg_build: a point lies outside the grid range");
+    place_points(ix->db, rs, f.cellnum, ix, cb);
     std::vector<int32_t> cbeg(f.cellnum), cend(f.cellnum);
     for (int c = 0; c < f.cellnum; c++) {
         cbeg[c] = (int32_t)cb[c];
         cend[c] = (int32_t)cb[c + 1];
     }
     ix->leaves = f.cellnum;
-    int st = dev ? GAT_OK : upload_points(ix);
+    int st = upload_points(ix);
     if (st != GAT_OK || ix->ctx->device < 0) return st;
     if (!(f.cbeg = index_upload(ix, cbeg, &st))) return st;
     if (!(f.cend = index_upload(ix, cend, &st))) return st;

@@ -1,27 +1,39 @@
-/* Device placement of index points for the Grid and FSG builders (the layouts of
- * Grid::addDatasetToGrid, Grid.cpp:210-316, and FSG::addDatasetToGrid, FSG.cpp:95-143).
+/* Device builders of the Grid (GT-quadtree + FVTable) and FSG indexes, in the layouts of
+ * Grid::addDatasetToGrid (Grid.cpp:210-316, quadtree Grid.cpp:58-94, frequency vectors
+ * Grid.cpp:152-166 / FVTable.cpp:18-30) and FSG::addDatasetToGrid (FSG.cpp:95-143).
  *
  * Both indexes order points by cell, trajectories ascending within a cell and points in
  * trajectory order within a trajectory: a stable sort by cell of the set's points taken in
- * trajectory order. The device computes every point's cell with the builders' float expressions
- * (IEEE single subtract and divide, truncation toward zero), sorts (cell, original position)
- * pairs with a stable LSD radix sort, gathers x / y / trajectory / key in that order, and finds
- * the cell boundaries by binary search over the sorted cells. For the Grid it also forms the
- * frequency vectors: 64-bit (trajectory, virtual cell) keys sorted and run-length counted give
- * each trajectory's (virtual cell, count) list in ascending cell order, which is what merging
- * the runs' (cell >> vparam, count) pairs per trajectory yields (Grid.cpp:152-166).
- *
- * Only the cell boundaries travel to the host, where the quadtree is a walk over them; the host
- * copies of the points are downloaded when first asked for (gat_index_points, snapshots).
- * The sorts and the run-length encoding are CUB's (the CUDA toolkit's header library); an index
- * build runs once per trajectory set and is not on the query path. */
+ * trajectory order. The build runs entirely in HBM:
+ *   1. cells      a warp per trajectory computes each point's cell with the builders' float
+ *                 expressions (IEEE single subtract and divide, truncation toward zero);
+ *   2. sort       a stable LSD radix sort of (cell, position) pairs;
+ *   3. gather     x / y / trajectory / key in sorted order; a point's trajectory comes from a
+ *                 per-1024-point hint table and a short binary search of the offsets (L2-resident);
+ *   4. bounds     cell boundaries by binary search over the sorted cells;
+ *   5. quadtree   (Grid) level by level: split flags, a scan, children written in parents' order,
+ *                 which is the breadth-first order of the reference's queue; node MBBs from the
+ *                 same float expressions as the host builder;
+ *   6. vectors    (Grid) each trajectory's (virtual cell, count) list in ascending cell order: a
+ *                 warp sorts the trajectory's virtual cells in shared memory and counts runs;
+ *                 sets with a trajectory longer than kFvLocal sort (trajectory, virtual cell)
+ *                 keys globally instead.
+ * The host copies of the points are downloaded only when asked for (gat_index_points,
+ * snapshots). The radix sorts, scans and run-length encoding are CUB's (the CUDA toolkit's
+ * header library); an index build runs once per trajectory set and is not on the query path. */
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_run_length_encode.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "internal.h"
 
 namespace gat {
 namespace {
+
+constexpr int kHintShift = 10;  /* one trajectory hint per 1024 points */
+constexpr int kFvLocal = 2048;  /* longest trajectory whose vector a warp sorts in shared memory */
+constexpr int kFvWarps = 4;     /* warps per block of the local vector kernel (8 KB each) */
+constexpr int kMaxLevels = 32;
 
 struct CellParams {
     float rxmin, rymax, cell;
@@ -35,6 +47,14 @@ __device__ __forceinline__ uint32_t spread_bits(uint32_t v) {
     v = (v | (v << 4)) & 0x0F0F0F0F;
     v = (v | (v << 2)) & 0x33333333;
     v = (v | (v << 1)) & 0x55555555;
+    return v;
+}
+__device__ __forceinline__ uint32_t compact_bits(uint32_t v) {
+    v &= 0x55555555;
+    v = (v | (v >> 1)) & 0x33333333;
+    v = (v | (v >> 2)) & 0x0F0F0F0F;
+    v = (v | (v >> 4)) & 0x00FF00FF;
+    v = (v | (v >> 8)) & 0x0000FFFF;
     return v;
 }
 
@@ -60,54 +80,67 @@ __device__ __forceinline__ int point_cell(const CellParams& p, float lon, float 
     return row * p.nx + col;
 }
 
-/* per point (trajectory order): cell, position, trajectory, point index within the trajectory,
- * and for the Grid the frequency-vector key (trajectory << 32 | cell >> vparam) */
-__global__ void k_point_cells(int64_t P, int n, const int64_t* __restrict__ off, const float2* __restrict__ xy,
-                              CellParams p, uint32_t* cell, int32_t* pos, int32_t* tid, int32_t* pidx,
-                              unsigned long long* fvkey, int32_t* flag) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x) {
-        /* the largest t with off[t] <= i is the trajectory holding point i (off[1] = 0; an empty
-         * trajectory shares its successor's offset and so is never the largest) */
-        int lo = 1, hi = n;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (off[mid] <= i)
-                lo = mid;
-            else
-                hi = mid - 1;
+/* 1. a warp per trajectory: cell and position of each point, the trajectory holding every
+ * 1024th point (hint), and for the global vector path the key (trajectory << 32 | vcell) */
+__global__ void k_point_cells(int n, const int64_t* __restrict__ off, const float2* __restrict__ xy, CellParams p,
+                              uint32_t* cell, int32_t* pos, int32_t* hint, unsigned long long* fvkey, int32_t* flag) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t <= n; t += nw) {
+        const int64_t s = off[t], e = off[t + 1];
+        bool bad = false;
+        for (int64_t i = s + lane; i < e; i += 32) {
+            const float2 v = xy[i];
+            int c = point_cell(p, v.x, v.y);
+            if (c < 0) {
+                bad = true;
+                c = 0;
+            }
+            cell[i] = (uint32_t)c;
+            pos[i] = (int32_t)i;
+            if ((i & ((1 << kHintShift) - 1)) == 0) hint[i >> kHintShift] = t;
+            if (fvkey) fvkey[i] = ((unsigned long long)(unsigned)t << 32) | (unsigned)(c >> p.vparam);
         }
-        const float2 v = xy[i];
-        int c = point_cell(p, v.x, v.y);
-        if (c < 0) {
-            atomicCAS(flag, 0, GAT_ERR_ARG);
-            c = 0;
-        }
-        cell[i] = (uint32_t)c;
-        pos[i] = (int32_t)i;
-        tid[i] = lo;
-        pidx[i] = (int32_t)(i - off[lo]);
-        if (fvkey) fvkey[i] = ((unsigned long long)(unsigned)lo << 32) | (unsigned)(c >> p.vparam);
+        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicCAS(flag, 0, GAT_ERR_ARG);
     }
 }
 
-/* index-order arrays from the sorted positions; key = tid << pidx_bits | pidx, or 0 when the
+/* the trajectory holding point s: the largest t with off[t] <= s, searched between the hints of
+ * s's 1024-point block and the next (an empty trajectory shares its successor's offset and so is
+ * never the largest) */
+__device__ __forceinline__ int holder(int64_t s, int n, const int64_t* __restrict__ off, const int32_t* __restrict__ hint,
+                                      int64_t nhint) {
+    const int64_t b = s >> kHintShift;
+    int lo = hint[b], hi = b + 1 < nhint ? hint[b + 1] : n;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= s)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+/* 3. index-order arrays from the sorted positions; key = tid << pidx_bits | pidx, or 0 when the
  * pair does not fit 32 bits (pidx_bits < 0; the point index then goes to pidx) */
-__global__ void k_gather_points(int64_t P, const int32_t* __restrict__ order, const float2* __restrict__ xy,
-                                const int32_t* __restrict__ tid_in, const int32_t* __restrict__ pidx_in, float* x,
+__global__ void k_gather_points(int64_t P, int n, const int32_t* __restrict__ order, const int64_t* __restrict__ off,
+                                const int32_t* __restrict__ hint, int64_t nhint, const float2* __restrict__ xy, float* x,
                                 float* y, int32_t* tid, uint32_t* key, int32_t* pidx, int pidx_bits) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x) {
         const int s = order[i];
         const float2 v = xy[s];
+        const int t = holder(s, n, off, hint, nhint);
+        const int k = (int)(s - off[t]);
         x[i] = v.x;
         y[i] = v.y;
-        const int t = tid_in[s], k = pidx_in[s];
         tid[i] = t;
         key[i] = pidx_bits >= 0 ? ((uint32_t)t << pidx_bits) | (uint32_t)k : 0u;
         if (pidx) pidx[i] = k;
     }
 }
 
-/* bound[j] = the first position p in the sorted keys with keys[p] >= j << shift, j = 0..m */
+/* 4. bound[j] = the first position p in the sorted keys with keys[p] >= j << shift, j = 0..m */
 template <class K>
 __global__ void k_bounds(int64_t P, int64_t m, const K* __restrict__ keys, int shift, int64_t* bound) {
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j <= m; j += (int64_t)gridDim.x * blockDim.x) {
@@ -124,12 +157,171 @@ __global__ void k_bounds(int64_t P, int64_t m, const K* __restrict__ keys, int s
     }
 }
 
-/* frequency-vector cells: the low half of each (trajectory, virtual cell) run key */
+/* FSG cell ranges [cbeg, cend) from the boundaries (FSG.cpp:119-140) */
+__global__ void k_fsg_cells(int64_t ncells, const int64_t* __restrict__ cb, int32_t* cbeg, int32_t* cend) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells; c += (int64_t)gridDim.x * blockDim.x) {
+        cbeg[c] = (int32_t)cb[c];
+        cend[c] = (int32_t)cb[c + 1];
+    }
+}
+
+/* ---------------------------------------------------------------- 5. quadtree */
+struct TreeParams {
+    float rxmin, rymax, cell;
+    int total_level, leaf_cap;
+};
+
+__device__ __forceinline__ int64_t node_span(int level, int total_level) {
+    return (int64_t)1 << (2 * (total_level - level));
+}
+
+/* split flag of each node of one level; flags[m] = 0 closes the scan */
+__global__ void k_tree_split(int64_t m, int level, const int32_t* __restrict__ ids, const int64_t* __restrict__ cb,
+                             TreeParams tp, int32_t* flags) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j <= m; j += (int64_t)gridDim.x * blockDim.x) {
+        if (j == m) {
+            flags[j] = 0;
+            continue;
+        }
+        const int64_t span = node_span(level, tp.total_level);
+        const int64_t first = (int64_t)ids[j] * span, last = first + span - 1;
+        const int64_t pts = cb[last + 1] - cb[first];
+        /* Grid::buildQuadTree (Grid.cpp:58-94): a leaf below the point cap or at the last level */
+        flags[j] = (pts < tp.leaf_cap || level == tp.total_level) ? 0 : 1;
+    }
+}
+
+/* children of the split nodes of one level, in their parents' order (the breadth-first queue) */
+__global__ void k_tree_children(int64_t m, const int32_t* __restrict__ ids, const int32_t* __restrict__ flags,
+                                const int32_t* __restrict__ spos, int64_t base_next, int32_t* next_ids, int32_t* child) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+        if (!flags[j]) {
+            child[j] = -1;
+            continue;
+        }
+        const int64_t c0 = base_next + 4 * (int64_t)spos[j];
+        child[j] = (int32_t)c0;
+        for (int c = 0; c < 4; c++) next_ids[c0 - base_next + c] = (ids[j] << 2) + c;
+    }
+}
+
+struct LevelTable {
+    int64_t base[kMaxLevels + 1];
+    int nlevels;
+};
+
+/* the Morton cell's box (Grid.cpp:121), in the host builder's float expressions */
+__device__ __forceinline__ float4 cell_box(const TreeParams& tp, int c) {
+    const int col = (int)compact_bits((uint32_t)c), row = (int)compact_bits((uint32_t)c >> 1);
+    return make_float4(__fadd_rn(tp.rxmin, __fmul_rn(tp.cell, (float)col)),
+                       __fsub_rn(tp.rymax, __fmul_rn(tp.cell, (float)(row + 1))),
+                       __fadd_rn(tp.rxmin, __fmul_rn(tp.cell, (float)(col + 1))),
+                       __fsub_rn(tp.rymax, __fmul_rn(tp.cell, (float)row)));
+}
+
+/* node arrays in breadth-first order: MBB, first child, point range */
+__global__ void k_tree_nodes(int64_t N, LevelTable lt, const int32_t* __restrict__ ids, const int32_t* __restrict__ child_in,
+                             const int64_t* __restrict__ cb, TreeParams tp, float4* mbb, int32_t* child, int32_t* pbeg,
+                             int32_t* pend) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < N; j += (int64_t)gridDim.x * blockDim.x) {
+        int level = 0;
+        while (level + 1 < lt.nlevels && lt.base[level + 1] <= j) level++;
+        const int64_t span = node_span(level, tp.total_level);
+        const int64_t first = (int64_t)ids[j] * span, last = first + span - 1;
+        const float4 a = cell_box(tp, (int)first), b = cell_box(tp, (int)last);
+        mbb[j] = make_float4(a.x, b.y, b.z, a.w);
+        child[j] = child_in[j];
+        pbeg[j] = (int32_t)cb[first];
+        pend[j] = (int32_t)cb[last + 1];
+    }
+}
+
+/* ---------------------------------------------------------------- 6. frequency vectors */
+/* Sorts the warp's n values in place (bitonic, padded to a power of two with UINT_MAX). */
+__device__ void warp_sort(uint32_t* v, int n, int lane) {
+    int m = 32;
+    while (m < n) m <<= 1;
+    for (int i = n + lane; i < m; i += 32) v[i] = 0xffffffffu;
+    __syncwarp();
+    for (int k = 2; k <= m; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < m; i += 32) {
+                const int p = i ^ j;
+                if (p > i) {
+                    const uint32_t a = v[i], b = v[p];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) {
+                        v[i] = b;
+                        v[p] = a;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+/* a warp per trajectory (length <= kFvLocal): sorted virtual cells, run-length counted into
+ * tmp at the trajectory's own offset; nnz[t] entries; the largest count to max_nnz */
+__global__ void __launch_bounds__(kFvWarps * 32) k_fv_local(int n, const int64_t* __restrict__ off,
+                                                            const uint32_t* __restrict__ cells, int vparam,
+                                                            int32_t* tmp_cell, int32_t* tmp_cnt, int64_t* nnz,
+                                                            int32_t* max_nnz) {
+    __shared__ uint32_t sv[kFvWarps][kFvLocal];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t* v = sv[w];
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    int mx = 0;
+    for (int t = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t <= n; t += nw) {
+        const int64_t s = off[t];
+        const int L = (int)(off[t + 1] - s);
+        for (int i = lane; i < L; i += 32) v[i] = cells[s + i] >> vparam;
+        __syncwarp();
+        warp_sort(v, L, lane);
+        /* run heads: the first index of each distinct value; count = next head - head */
+        int written = 0;
+        for (int base = 0; base < L; base += 32) {
+            const int i = base + lane;
+            const bool head = i < L && (i == 0 || v[i] != v[i - 1]);
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            if (head) {
+                int j = i + 1;
+                while (j < L && v[j] == v[i]) j++;
+                const int r = written + __popc(hm & ((1u << lane) - 1));
+                tmp_cell[s + r] = (int32_t)v[i];
+                tmp_cnt[s + r] = j - i;
+            }
+            written += __popc(hm);
+        }
+        if (lane == 0) nnz[t] = written;
+        mx = max(mx, written);
+        __syncwarp();
+    }
+    if (lane == 0 && mx > 0) atomicMax(max_nnz, mx);
+}
+
+/* entries of trajectory t from tmp (at off[t]) to the CSR (at fv_off[t]) */
+__global__ void k_fv_compact(int n, const int64_t* __restrict__ off, const int64_t* __restrict__ fv_off,
+                             const int32_t* __restrict__ tmp_cell, const int32_t* __restrict__ tmp_cnt, int32_t* fv_cell,
+                             int32_t* fv_cnt) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t <= n; t += nw) {
+        const int64_t s = off[t], d = fv_off[t], k = fv_off[t + 1] - d;
+        for (int64_t i = lane; i < k; i += 32) {
+            fv_cell[d + i] = tmp_cell[s + i];
+            fv_cnt[d + i] = tmp_cnt[s + i];
+        }
+    }
+}
+
+/* frequency-vector cells of the global path: the low half of each (trajectory, vcell) run key */
 __global__ void k_fv_cells(int64_t R, const unsigned long long* __restrict__ runs, int32_t* cell) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x)
         cell[r] = (int32_t)(runs[r] & 0xffffffffull);
 }
 
+/* ---------------------------------------------------------------- host side */
 /* device allocations of one build, freed with it */
 struct Temps {
     std::vector<void*> ptrs;
@@ -138,7 +330,8 @@ struct Temps {
     Temps(const Temps&) = delete;
     Temps& operator=(const Temps&) = delete;
     ~Temps() {
-        for (void* p : ptrs) cudaFree(p);
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
     }
     template <class T>
     T* get(size_t n) {
@@ -149,6 +342,15 @@ struct Temps {
         ptrs.push_back(p);
         return static_cast<T*>(p);
     }
+    /* frees one temporary early (stream-ordered work that reads it must be complete or on the
+     * same stream: cudaFree waits for the device) */
+    void release(void* p) {
+        for (auto& q : ptrs)
+            if (q && q == p) {
+                cudaFree(q);
+                q = nullptr;
+            }
+    }
 };
 
 int bits_to_hold(int64_t v) {
@@ -157,50 +359,62 @@ int bits_to_hold(int64_t v) {
     return b;
 }
 
-int grid_size(const gat_ctx* ctx, int64_t work) {
-    const int64_t want = (work + 255) / 256;
+int grid_size(const gat_ctx* ctx, int64_t work, int per_block = 256) {
+    const int64_t want = (work + per_block - 1) / per_block;
     return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)std::max(1, ctx->sm_count) * 8));
 }
 
-}  // namespace
+/* index array of `count` elements of T plus the host builder's one element of padding, zeroed */
+template <class T>
+T* alloc_padded(gat_index* ix, int64_t count, int* st) {
+    T* p = (T*)index_alloc(ix, (size_t)(count + 1) * sizeof(T), st);
+    if (!p) return nullptr;
+    const cudaError_t e = cudaMemsetAsync(p + count, 0, sizeof(T), ix->ctx->stream);
+    if (e != cudaSuccess) {
+        *st = cuda_fail(ix->ctx, e, "index build");
+        return nullptr;
+    }
+    return p;
+}
 
-/* the Grid's sorted, counted (trajectory, virtual cell) runs between device_place and device_fv */
-struct DeviceFvRuns {
-    Temps tmp;
-    unsigned long long* runs = nullptr;
-    int32_t* cnt = nullptr;
-    int32_t* nruns = nullptr;
+/* Steps 1-4: the points in index order (x, y, tid, key allocated first, as the host builder
+ * uploads them), the cells in trajectory order and the boundaries d_cb[0..ncells]. */
+struct Placement {
+    uint32_t* cells = nullptr; /* trajectory order */
+    int64_t* d_cb = nullptr;
+    unsigned long long* fvkey = nullptr; /* global vector path only */
 };
-void DeviceFvRunsFree::operator()(DeviceFvRuns* r) const { delete r; }
 
-int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& cb, DeviceFvHandle* fv) {
+int place(gat_index* ix, const DevicePlaceArgs& a, bool fv_keys, Temps& tmp, Placement& out) {
     gat_ctx* ctx = ix->ctx;
     const gat_db* db = ix->db;
     cudaStream_t s = ctx->stream;
     const int64_t P = db->npoints;
     const int n = db->n;
     if (P >= ((int64_t)1 << 31) - 1) return fail(ctx, GAT_ERR_ARG, std::string(a.what) + ": more than 2^31 - 2 points");
-    Temps tmp;
+    const int64_t nhint = (P + (1 << kHintShift) - 1) >> kHintShift; /* blocks holding points */
     uint32_t* cells = tmp.get<uint32_t>(P);
     uint32_t* cells_s = tmp.get<uint32_t>(P);
     int32_t* pos = tmp.get<int32_t>(P);
     int32_t* order = tmp.get<int32_t>(P);
-    int32_t* tid0 = tmp.get<int32_t>(P);
-    int32_t* pidx0 = tmp.get<int32_t>(P);
+    int32_t* hint = tmp.get<int32_t>(nhint);
     int64_t* d_cb = tmp.get<int64_t>((size_t)a.ncells + 1);
-    unsigned long long* fvk = fv ? tmp.get<unsigned long long>(P) : nullptr;
+    unsigned long long* fvk = fv_keys ? tmp.get<unsigned long long>(P) : nullptr;
     if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
     CellParams cp{a.rxmin, a.rymax, a.cell, a.morton ? 1 : 0, a.axis, a.nx, a.ny, a.vparam};
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int32_t), s), "index build");
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(hint, 0, (size_t)nhint * 4, s), "index build");
     if (P > 0) {
-        k_point_cells<<<grid_size(ctx, P), 256, 0, s>>>(P, n, db->d_off, db->d_xy, cp, cells, pos, tid0, pidx0, fvk,
-                                                        ctx->d_flag);
+        timed_begin(ctx, GAT_KERNEL_INDEX_BUILD);
+        k_point_cells<<<grid_size(ctx, (int64_t)n * 32), 256, 0, s>>>(n, db->d_off, db->d_xy, cp, cells, pos, hint, fvk,
+                                                                      ctx->d_flag);
+        timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * (16 + (fvk ? 8 : 0)) + (double)n * 16);
         count_launch(ctx);
     }
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (cells)");
     if (check_device_flag(ctx, "index build") != GAT_OK)
         return fail(ctx, GAT_ERR_ARG, std::string(a.what) + ": a point lies outside the grid range");
-    /* stable sort of (cell, position) */
+    /* 2. stable sort of (cell, position) */
     const int end_bit = bits_to_hold(a.ncells);
     size_t tbytes = 0;
     GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tbytes, cells, cells_s, pos, order, (int)P, 0, end_bit, s),
@@ -212,106 +426,262 @@ int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& 
                      "index build sort");
         count_launch(ctx, 2 * ((end_bit + 7) / 8) + 1);
     }
-    /* index-order arrays, allocated in the host builder's upload order (x, y, tid, key) with its
-     * one element of padding, zeroed */
+    /* 3. index-order arrays */
     const int tid_bits = bits_to_hold(n);
     int pidx_bits = bits_to_hold(std::max(1, db->maxlen - 1));
     if (tid_bits + pidx_bits > 32) pidx_bits = -1; /* point-level results unavailable for this set */
     ix->pidx_bits = pidx_bits;
     ix->npoints = P;
     int st = GAT_OK;
-    const size_t pb = (size_t)(P + 1) * 4;
-    float* dx = (float*)index_alloc(ix, pb, &st);
-    float* dy = dx ? (float*)index_alloc(ix, pb, &st) : nullptr;
-    int32_t* dt = dy ? (int32_t*)index_alloc(ix, pb, &st) : nullptr;
-    uint32_t* dk = dt ? (uint32_t*)index_alloc(ix, pb, &st) : nullptr;
+    float* dx = alloc_padded<float>(ix, P, &st);
+    float* dy = dx ? alloc_padded<float>(ix, P, &st) : nullptr;
+    int32_t* dt = dy ? alloc_padded<int32_t>(ix, P, &st) : nullptr;
+    uint32_t* dk = dt ? alloc_padded<uint32_t>(ix, P, &st) : nullptr;
     if (!dk) return st;
     ix->d_x = dx;
     ix->d_y = dy;
     ix->d_tid = dt;
     ix->d_key = dk;
     if (pidx_bits < 0) GAT_CUDA_TRY(ctx, cudaMalloc(&ix->d_pidx, std::max<size_t>((size_t)P, 1) * 4), "index build");
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(dx + P, 0, 4, s), "index build");
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(dy + P, 0, 4, s), "index build");
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(dt + P, 0, 4, s), "index build");
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(dk + P, 0, 4, s), "index build");
     if (P > 0) {
-        k_gather_points<<<grid_size(ctx, P), 256, 0, s>>>(P, order, db->d_xy, tid0, pidx0, dx, dy, dt, dk, ix->d_pidx,
-                                                          pidx_bits);
+        timed_begin(ctx, GAT_KERNEL_INDEX_BUILD);
+        k_gather_points<<<grid_size(ctx, P), 256, 0, s>>>(P, n, order, db->d_off, hint, nhint, db->d_xy, dx, dy, dt, dk,
+                                                          ix->d_pidx, pidx_bits);
+        timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * (28 + (pidx_bits < 0 ? 4 : 0)));
         count_launch(ctx);
     }
+    /* 4. cell boundaries */
     k_bounds<uint32_t><<<grid_size(ctx, a.ncells + 1), 256, 0, s>>>(P, a.ncells, cells_s, 0, d_cb);
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (gather)");
-    cb.resize((size_t)a.ncells + 1);
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cb.data(), d_cb, cb.size() * 8, cudaMemcpyDeviceToHost, s), "index build");
     ix->host_pending = true;
-    if (fv) {
-        /* (trajectory, virtual cell) keys sorted and run-length counted; kept for device_fv */
-        DeviceFvHandle r(new DeviceFvRuns());
-        unsigned long long* fvk_s = r->tmp.get<unsigned long long>(P);
-        r->runs = r->tmp.get<unsigned long long>(P);
-        r->cnt = r->tmp.get<int32_t>(P + 1);
-        r->nruns = r->tmp.get<int32_t>(1);
-        if (r->tmp.err != cudaSuccess) return cuda_fail(ctx, r->tmp.err, "index build (device temporaries)");
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(r->nruns, 0, 4, s), "index build fv");
+    out.cells = cells;
+    out.d_cb = d_cb;
+    out.fvkey = fvk;
+    return GAT_OK;
+}
+
+/* Step 5: quadtree node arrays (node_mbb, node_child, node_pbeg, node_pend) in breadth-first
+ * order. */
+int build_tree(gat_index* ix, const Placement& pl, const TreeParams& tp, Temps& tmp) {
+    gat_ctx* ctx = ix->ctx;
+    cudaStream_t s = ctx->stream;
+    /* node ids and child links in queue order; grown as levels are added */
+    int64_t cap = 1 << 16;
+    int32_t* ids = tmp.get<int32_t>(cap);
+    int32_t* child = tmp.get<int32_t>(cap);
+    int32_t* flags = tmp.get<int32_t>(cap + 1);
+    int32_t* spos = tmp.get<int32_t>(cap + 1);
+    if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+    size_t scan_bytes = 0;
+    void* scan_tmp = nullptr;
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(ids, 0, 4, s), "index build tree");
+    LevelTable lt{};
+    int64_t base = 0, m = 1, splits = 0;
+    for (int level = 0;; level++) {
+        if (level >= kMaxLevels) return fail(ctx, GAT_ERR_ARG, "gat_grid_build: quadtree deeper than supported");
+        lt.base[level] = base;
+        lt.nlevels = level + 1;
+        k_tree_split<<<grid_size(ctx, m + 1), 256, 0, s>>>(m, level, ids + base, pl.d_cb, tp, flags);
+        count_launch(ctx);
+        size_t need = 0;
+        GAT_CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(nullptr, need, flags, spos, (int)(m + 1), s), "index build tree");
+        if (need > scan_bytes) {
+            if (scan_tmp) tmp.release(scan_tmp);
+            scan_tmp = tmp.get<char>(need);
+            if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+            scan_bytes = need;
+        }
+        GAT_CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(scan_tmp, need, flags, spos, (int)(m + 1), s), "index build tree");
+        count_launch(ctx);
+        int32_t S = 0;
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&S, spos + m, 4, cudaMemcpyDeviceToHost, s), "index build tree");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build tree");
+        const int64_t next = base + m + 4 * (int64_t)S;
+        if (next > (int64_t)INT32_MAX) return fail(ctx, GAT_ERR_ARG, "gat_grid_build: quadtree larger than 2^31 nodes");
+        if (next > cap || 4 * (int64_t)S + 1 > cap) {
+            /* grow: room for the next level's nodes, and flags for a level of that size */
+            int64_t ncap = cap;
+            while (ncap < next || ncap < 4 * (int64_t)S + 1) ncap *= 2;
+            int32_t* nids = tmp.get<int32_t>(ncap);
+            int32_t* nchild = tmp.get<int32_t>(ncap);
+            int32_t* nflags = tmp.get<int32_t>(ncap + 1);
+            int32_t* nspos = tmp.get<int32_t>(ncap + 1);
+            if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(nids, ids, (size_t)(base + m) * 4, cudaMemcpyDeviceToDevice, s), "index build tree");
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(nchild, child, (size_t)std::max<int64_t>(base, 1) * 4, cudaMemcpyDeviceToDevice, s),
+                         "index build tree");
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(nflags, flags, (size_t)(m + 1) * 4, cudaMemcpyDeviceToDevice, s), "index build tree");
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(nspos, spos, (size_t)(m + 1) * 4, cudaMemcpyDeviceToDevice, s), "index build tree");
+            GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build tree");
+            tmp.release(ids);
+            tmp.release(child);
+            tmp.release(flags);
+            tmp.release(spos);
+            ids = nids;
+            child = nchild;
+            flags = nflags;
+            spos = nspos;
+            cap = ncap;
+        }
+        k_tree_children<<<grid_size(ctx, m), 256, 0, s>>>(m, ids + base, flags, spos, base + m, ids + base + m, child + base);
+        count_launch(ctx);
+        splits += S;
+        base += m;
+        m = 4 * (int64_t)S;
+        if (m == 0) break;
+    }
+    const int64_t N = base;
+    GridDev& g = ix->grid;
+    g.nnodes = (int)N;
+    ix->nodes = N;
+    ix->leaves = N - splits;
+    int st = GAT_OK;
+    float4* nmbb = alloc_padded<float4>(ix, N, &st);
+    int32_t* nchild = nmbb ? alloc_padded<int32_t>(ix, N, &st) : nullptr;
+    int32_t* npbeg = nchild ? alloc_padded<int32_t>(ix, N, &st) : nullptr;
+    int32_t* npend = npbeg ? alloc_padded<int32_t>(ix, N, &st) : nullptr;
+    if (!npend) return st;
+    g.node_mbb = nmbb;
+    g.node_child = nchild;
+    g.node_pbeg = npbeg;
+    g.node_pend = npend;
+    k_tree_nodes<<<grid_size(ctx, N), 256, 0, s>>>(N, lt, ids, child, pl.d_cb, tp, nmbb, nchild, npbeg, npend);
+    count_launch(ctx);
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build tree");
+    return GAT_OK;
+}
+
+/* Step 6: the frequency-vector CSR (fv_off [n+2], fv_cell, fv_cnt), allocated after the nodes. */
+int build_vectors(gat_index* ix, const Placement& pl, int vparam, Temps& tmp) {
+    gat_ctx* ctx = ix->ctx;
+    cudaStream_t s = ctx->stream;
+    const gat_db* db = ix->db;
+    const int n = db->n;
+    const int64_t P = db->npoints;
+    int st = GAT_OK;
+    int64_t* off = alloc_padded<int64_t>(ix, n + 2, &st);
+    if (!off) return st;
+    ix->d_fv_off = off;
+    int64_t R = 0;
+    if (!pl.fvkey) {
+        /* local: a warp sorts each trajectory's virtual cells */
+        int32_t* tcell = tmp.get<int32_t>(P);
+        int32_t* tcnt = tmp.get<int32_t>(P);
+        int64_t* nnz = tmp.get<int64_t>((size_t)n + 2);
+        int32_t* mx = tmp.get<int32_t>(1);
+        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(nnz, 0, ((size_t)n + 2) * 8, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(mx, 0, 4, s), "index build fv");
+        if (n > 0) {
+            k_fv_local<<<grid_size(ctx, (int64_t)n * 32, kFvWarps * 32), kFvWarps * 32, 0, s>>>(
+                n, db->d_off, pl.cells, vparam, tcell, tcnt, nnz, mx);
+            count_launch(ctx);
+        }
+        size_t need = 0;
+        GAT_CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(nullptr, need, nnz, off, n + 2, s), "index build fv");
+        void* stmp = tmp.get<char>(need);
+        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+        GAT_CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(stmp, need, nnz, off, n + 2, s), "index build fv");
+        count_launch(ctx);
+        int32_t hmx = 0;
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R, off + n + 1, 8, cudaMemcpyDeviceToHost, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&hmx, mx, 4, cudaMemcpyDeviceToHost, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
+        int32_t* cell = alloc_padded<int32_t>(ix, R, &st);
+        int32_t* cnt = cell ? alloc_padded<int32_t>(ix, R, &st) : nullptr;
+        if (!cnt) return st;
+        ix->d_fv_cell = cell;
+        ix->d_fv_cnt = cnt;
+        if (n > 0) {
+            k_fv_compact<<<grid_size(ctx, (int64_t)n * 32), 256, 0, s>>>(n, db->d_off, off, tcell, tcnt, cell, cnt);
+            count_launch(ctx);
+        }
+        ix->fv_max_nnz = hmx;
+    } else {
+        /* global: (trajectory, virtual cell) keys sorted and run-length counted */
+        unsigned long long* fvk_s = tmp.get<unsigned long long>(P);
+        unsigned long long* runs = tmp.get<unsigned long long>(P);
+        int32_t* rcnt = tmp.get<int32_t>(P + 1);
+        int32_t* nruns = tmp.get<int32_t>(1);
+        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(nruns, 0, 4, s), "index build fv");
         if (P > 0) {
             /* keys hold the trajectory above bit 32 and the virtual cell below it */
             const int kbits = 32 + bits_to_hold(n);
             size_t b1 = 0, b2 = 0;
-            GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortKeys(nullptr, b1, fvk, fvk_s, (int)P, 0, kbits, s), "index build fv");
-            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(nullptr, b2, fvk_s, r->runs, r->cnt, r->nruns, (int)P, s),
+            GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortKeys(nullptr, b1, pl.fvkey, fvk_s, (int)P, 0, kbits, s),
+                         "index build fv");
+            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(nullptr, b2, fvk_s, runs, rcnt, nruns, (int)P, s),
                          "index build fv");
             void* t2 = tmp.get<char>(std::max(b1, b2));
             if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-            GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortKeys(t2, b1, fvk, fvk_s, (int)P, 0, kbits, s), "index build fv");
-            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(t2, b2, fvk_s, r->runs, r->cnt, r->nruns, (int)P, s),
+            GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortKeys(t2, b1, pl.fvkey, fvk_s, (int)P, 0, kbits, s), "index build fv");
+            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(t2, b2, fvk_s, runs, rcnt, nruns, (int)P, s),
                          "index build fv");
             count_launch(ctx, 2 * ((kbits + 7) / 8) + 3);
         }
-        *fv = std::move(r);
+        int32_t R32 = 0;
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R32, nruns, 4, cudaMemcpyDeviceToHost, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
+        R = R32;
+        int32_t* cell = alloc_padded<int32_t>(ix, R, &st);
+        int32_t* cnt = cell ? alloc_padded<int32_t>(ix, R, &st) : nullptr;
+        if (!cnt) return st;
+        ix->d_fv_cell = cell;
+        ix->d_fv_cnt = cnt;
+        if (R > 0) {
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, rcnt, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "index build fv");
+            k_fv_cells<<<grid_size(ctx, R), 256, 0, s>>>(R, runs, cell);
+            count_launch(ctx);
+        }
+        /* off[t] = entries of trajectories below t: the first run whose key is >= t << 32 */
+        k_bounds<unsigned long long><<<grid_size(ctx, n + 2), 256, 0, s>>>(R, n + 1, runs, 32, off);
+        count_launch(ctx);
+        std::vector<int64_t> h((size_t)n + 2);
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), off, h.size() * 8, cudaMemcpyDeviceToHost, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
+        int hmx = 0;
+        for (int t = 0; t <= n; t++) hmx = std::max<int>(hmx, (int)(h[(size_t)t + 1] - h[(size_t)t]));
+        ix->fv_max_nnz = hmx;
     }
-    /* the temporaries are freed on return: wait for the work that reads them */
-    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build");
+    ix->fv_entries = R;
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build fv");
     return GAT_OK;
 }
 
-int device_fv(gat_index* ix, DeviceFvRuns* fv) {
+}  // namespace
+
+int device_build_grid(gat_index* ix, const DevicePlaceArgs& a, int total_level, int leaf_cap) {
     gat_ctx* ctx = ix->ctx;
-    cudaStream_t s = ctx->stream;
-    const int n = ix->db->n;
-    int32_t R = 0;
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R, fv->nruns, 4, cudaMemcpyDeviceToHost, s), "index build fv");
-    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
-    /* sizes and order of the host builder's uploads: fv_off [n+2], fv_cell [R], fv_cnt [R], each
-     * with one zeroed element of padding */
+    Temps tmp;
+    Placement pl;
+    const bool global_fv = ix->db->maxlen > kFvLocal;
+    if (int st = place(ix, a, global_fv, tmp, pl)) return st;
+    TreeParams tp{a.rxmin, a.rymax, a.cell, total_level, leaf_cap};
+    if (int st = build_tree(ix, pl, tp, tmp)) return st;
+    if (int st = build_vectors(ix, pl, a.vparam, tmp)) return st;
+    /* the temporaries are freed on return: wait for the work that reads them */
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "gat_grid_build");
+    return GAT_OK;
+}
+
+int device_build_fsg(gat_index* ix, const DevicePlaceArgs& a) {
+    gat_ctx* ctx = ix->ctx;
+    Temps tmp;
+    Placement pl;
+    if (int st = place(ix, a, false, tmp, pl)) return st;
     int st = GAT_OK;
-    int64_t* off = (int64_t*)index_alloc(ix, (size_t)(n + 3) * 8, &st);
-    int32_t* cell = off ? (int32_t*)index_alloc(ix, (size_t)(R + 1) * 4, &st) : nullptr;
-    int32_t* cnt = cell ? (int32_t*)index_alloc(ix, (size_t)(R + 1) * 4, &st) : nullptr;
-    if (!cnt) return st;
-    ix->d_fv_off = off;
-    ix->d_fv_cell = cell;
-    ix->d_fv_cnt = cnt;
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(off + n + 2, 0, 8, s), "index build fv");
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(cell + R, 0, 4, s), "index build fv");
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(cnt + R, 0, 4, s), "index build fv");
-    if (R > 0) {
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, fv->cnt, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "index build fv");
-        k_fv_cells<<<grid_size(ctx, R), 256, 0, s>>>(R, fv->runs, cell);
-        count_launch(ctx);
-    }
-    /* off[t] = entries of trajectories below t: the first run whose key is >= t << 32 */
-    k_bounds<unsigned long long><<<grid_size(ctx, n + 2), 256, 0, s>>>(R, n + 1, fv->runs, 32, off);
+    int32_t* cbeg = alloc_padded<int32_t>(ix, a.ncells, &st);
+    int32_t* cend = cbeg ? alloc_padded<int32_t>(ix, a.ncells, &st) : nullptr;
+    if (!cend) return st;
+    ix->fsg.cbeg = cbeg;
+    ix->fsg.cend = cend;
+    ix->leaves = a.ncells;
+    k_fsg_cells<<<grid_size(ctx, a.ncells), 256, 0, ctx->stream>>>(a.ncells, pl.d_cb, cbeg, cend);
     count_launch(ctx);
-    GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build fv");
-    std::vector<int64_t> h((size_t)n + 2);
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), off, h.size() * 8, cudaMemcpyDeviceToHost, s), "index build fv");
-    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
-    int mx = 0;
-    for (int t = 0; t <= n; t++) mx = std::max<int>(mx, (int)(h[(size_t)t + 1] - h[(size_t)t]));
-    ix->fv_max_nnz = mx;
-    ix->fv_entries = R;
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "gat_fsg_build");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "gat_fsg_build");
     return GAT_OK;
 }
 

@@ -248,11 +248,9 @@ int edr_launch_soa(gat_ctx* ctx, int npairs, const int* d_npairs, const int64_t*
                    const int64_t* b_off, const int32_t* b_len, int rows_hint, int max_cols, const float2* A,
                    const float2* B, float u, int32_t* d_out, unsigned long long* d_cells);
 
-/* Device placement of a Grid or FSG index's points (index_gpu.cu): cells, the stable sort by
- * cell, the index-order arrays (allocated in the host builder's order; host copies deferred) and
- * the cell boundaries cb[0..ncells]. With fv given it also sorts and counts the Grid's
- * (trajectory, virtual cell) pairs and keeps them for device_fv, which allocates and fills the
- * frequency-vector CSR after the quadtree's arrays. */
+/* Device builds of a Grid or FSG index (index_gpu.cu): points, cell boundaries, quadtree and
+ * frequency vectors computed in HBM, allocated in the host builder's order; the host copies of
+ * the points are downloaded on first use. */
 struct DevicePlaceArgs {
     const char* what; /* the API call, for error messages */
     bool morton;      /* Grid (Morton ids on axis x axis) or FSG (row-major nx x ny) */
@@ -260,13 +258,8 @@ struct DevicePlaceArgs {
     int axis, nx, ny, vparam;
     int64_t ncells;
 };
-struct DeviceFvRuns;
-struct DeviceFvRunsFree {
-    void operator()(DeviceFvRuns* r) const;
-};
-using DeviceFvHandle = std::unique_ptr<DeviceFvRuns, DeviceFvRunsFree>;
-int device_place(gat_index* ix, const DevicePlaceArgs& a, std::vector<int64_t>& cb, DeviceFvHandle* fv);
-int device_fv(gat_index* ix, DeviceFvRuns* fv);
+int device_build_grid(gat_index* ix, const DevicePlaceArgs& a, int total_level, int leaf_cap);
+int device_build_fsg(gat_index* ix, const DevicePlaceArgs& a);
 /* downloads the host copies of a device-placed index (no-op otherwise) */
 int index_host_copies(gat_index* ix);
 /* gat_index_points for a device-placed index without host copies: device arrays straight into

@@ -85,7 +85,8 @@ int64_t gat_ctx_scratch_bytes(const gat_ctx* ctx);
  * events on the context stream; gat_ctx_kernel_stats returns their summed device time (ms),
  * launch count and algorithmic work (DP cells for EDR, bytes for the others) since the last
  * reset. Turning timing on resets the counters. */
-enum { GAT_KERNEL_EDR = 0, GAT_KERNEL_BOUNDS = 1, GAT_KERNEL_RANGE_SCAN = 2, GAT_KERNEL_CLASSES = 3 };
+enum { GAT_KERNEL_EDR = 0, GAT_KERNEL_BOUNDS = 1, GAT_KERNEL_RANGE_SCAN = 2, GAT_KERNEL_INDEX_BUILD = 3,
+       GAT_KERNEL_CLASSES = 4 };
 int gat_ctx_set_timing(gat_ctx* ctx, int on);
 int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* launches, double* work);
 /* Tuning knobs (no counterpart in the reference, which has fixed launch shapes).

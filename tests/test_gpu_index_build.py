@@ -152,3 +152,23 @@ def test_point_index_beyond_the_key(gpu_ctx, tmp_path):
     db = G.TrajectorySet(gpu_ctx, t)
     assert_same_index(gpu_ctx, db, "grid", tmp_path, cell=0.01)
     assert_same_index(gpu_ctx, db, "fsg", tmp_path, cell=0.02)
+
+
+def test_long_trajectories_and_deep_trees(gpu_ctx, tmp_path):
+    """Trajectories up to 2048 points (vectors sorted per trajectory in shared memory), one of
+    2049 (the whole set then sorts (trajectory, cell) keys globally), and a leaf cap of 1 over a
+    fine grid, whose quadtree outgrows the builder's first node buffer."""
+    q = D.boxes(200, 1, 0.001, 0.05, 67)
+    for top in (2048, 2049):
+        lens = D.lengths(400, 0, 0, 0, 1, 300, 68).astype(np.int32)
+        lens[[5, 100, 399]] = [top, 2047, 1]
+        t = D.walks(lens, 69)
+        db = G.TrajectorySet(gpu_ctx, t)
+        assert_same_index(gpu_ctx, db, "grid", tmp_path, q, t.subset([6, 101, 400]), cell=0.0025, vparam=2, leaf=64)
+    rng = np.random.default_rng(70)
+    x0, y0, x1, y1 = D.BOX
+    t = D.Trajectories(np.ones(60000, np.int32), rng.uniform(x0, x1, 60000).astype(np.float32),
+                       rng.uniform(y0, y1, 60000).astype(np.float32))
+    db = G.TrajectorySet(gpu_ctx, t)
+    h, d = assert_same_index(gpu_ctx, db, "grid", tmp_path, q, cell=0.001, vparam=3, leaf=1)
+    assert d.info()["nodes"] > 1 << 16
