@@ -7,7 +7,8 @@ Default workload (config 2 of the reference's benchmark set): plain EDR top-k si
 A step is one pass over the 256 queries. Other workloads: --workload c1 (plain GT-quadtree range
 queries), c3 (batched range queries over the three indexes), c4 (batched EDR pairs), c5 (served
 mix of range and top-k requests through the serving loop at three offered loads), c4k (batched
-top-k of 1024 long queries against the 1M-trajectory set).
+top-k of 1024 long queries against the 1M-trajectory set), build (Grid and FSG index builds over
+the 1M-trajectory set).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
 
@@ -29,7 +30,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-OPS_PER_CELL = 12  # int32 / fp32 instructions per DP cell of the EDR recurrence
+OPS_PER_CELL = 12  # int32 / fp32 instructions per DP cell of the EDR recurrence (match test, three-way min, carries)
 
 
 def log(*a):
@@ -1069,8 +1070,156 @@ def run_c5(args, world, rank, local, td):
     return line
 
 
-WORKLOADS = {"c1": run_c1, "c2": None, "c3": run_c3, "c4": run_c4, "c4k": run_c4k, "c5": run_c5}
-REFERENCE = {"c1": run_reference_c1, "c2": None, "c4": run_reference_c4}
+# ---------------------------------------------------------------- workload: index builds
+BUILD = dict(cell=0.001, vparam=2, leaf_cap=512, ref_n=40_000)
+
+
+def build_roofline(st):
+    gbs, src = hbm_peak()
+    if st["launches"] == 0 or st["ms"] <= 0:
+        return None
+    ach = st["work"] / (st["ms"] / 1e3) / 1e9
+    return {"kernel": "k_point_cells + k_gather_points", "bound": "hbm", "achieved": round(ach, 1), "peak": gbs,
+            "unit": "GB/s", "frac": round(ach / gbs, 4), "traffic": None,
+            "work_per_launch": st["work"] / st["launches"],
+            "note": "achieved = algorithmic bytes of both placement kernels / their summed event time; k_point_cells "
+                    "16 B per point (x, y read; cell, position written) + 16 B per trajectory, k_gather_points 28 B "
+                    f"per point (position, x, y read; x, y, trajectory, key written); peak of {src}"}
+
+
+def build_reference_sample():
+    """The reference's own Grid::addDatasetToGrid and FSG::addDatasetToGrid over the first
+    BUILD['ref_n'] trajectories of the set: (points placed per second over both builds, seconds)."""
+    from gat_b200 import data as D
+    from oracle import pyoracle as po
+
+    t, _ = D.config3(seed=0, n=BUILD["ref_n"], nq=1)
+    R = po.RefRunner()
+    r = R.gtq(t, np.zeros((0, 4), np.float32), D.BOX, BUILD["cell"], BUILD["leaf_cap"])
+    f = R.fsg(t, D.BOX, BUILD["cell"])
+    sec = float(r["t_build"][0]) + float(f["t_build"][0])
+    return 2 * len(t.lon) / sec, sec, len(t.lon)
+
+
+def run_build(args, world, rank, local, td):
+    """Index builds over the C3 set (1M walks U[50,350], 200M points): a GT-quadtree Grid with its
+    FVTable (cell 0.001 deg, virtual cells of 4x4 cells, leaf cap 512) and an FSG (cell 0.001 deg),
+    both built in HBM from a resident trajectory set."""
+    import torch
+
+    import gat_b200 as G
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t, _ = D.config3(seed=0, n=args.c3_n, nq=1)
+    P = len(t.lon)
+    ctx = G.Context(local)
+    ctx.set_tuning(L.GAT_TUNE_INDEX_BUILD, 2)
+    db = G.TrajectorySet(ctx, t)
+    H = Harness(ctx, dev)
+
+    def build(dbh):
+        return [G.Grid(ctx, dbh, G.BOX, BUILD["cell"], BUILD["vparam"], BUILD["leaf_cap"]),
+                G.FSG(ctx, dbh, G.BOX, BUILD["cell"])]
+
+    def step():
+        out = []
+        ms = H.time(lambda: out.extend(build(db)))
+        info = [ix.info() for ix in out]
+        for ix in out:
+            ix.close()
+        return ms, info
+
+    for _ in range(args.warmup):
+        step()
+    ctx.set_timing(True)
+    l0 = ctx.launches
+    clocks = ClockSampler(local)
+    barrier(td, dev)
+    clocks.start()
+    ms, info = [], None
+    for _ in range(args.steps):
+        m, info = step()
+        ms.append(m)
+    clk = clocks.stop()
+    st = ctx.kernel_stats(L.GAT_KERNEL_INDEX_BUILD)
+    ctx.set_timing(False)
+    launches = ctx.launches - l0
+    tot = max_over_ranks(td, sum(ms), dev)
+    # end to end through the public API: the trajectory set uploaded from host arrays, both
+    # builds, and each index's counts read back
+    ems = []
+    for _ in range(args.steps):
+        keep = []
+
+        def e2e():
+            dbh = G.TrajectorySet(ctx, t)
+            keep.append(dbh)
+            keep.extend(build(dbh))
+            for ix in keep[1:]:
+                ix.info()
+
+        ems.append(H.time(e2e))
+        for ix in keep[1:]:
+            ix.close()
+        keep[0].close()
+    etot = max_over_ranks(td, sum(ems), dev)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, sec, ps = build_reference_sample()
+        cpu = {"value": round(v, 1), "unit": "points/s", "cores": 1, "kind": "reference",
+               "sample": f"first {BUILD['ref_n']} trajectories ({ps} points): Grid::addDatasetToGrid + "
+                         f"FSG::addDatasetToGrid, {sec:.2f} s on one core"}
+    if rank != 0:
+        ctx.close()
+        return None
+    line = base_line(args, world, "index build points/s (GT-quadtree Grid + FVTable, and FSG)", "points/s",
+                     2 * P * world * args.steps / (tot / 1e3), tot,
+                     {"workload": f"index builds over the C3 set: {t.n} walks U[50,350] ({P} points), Grid cell 0.001 "
+                                  "deg (2048 x 2048 Morton cells), virtual cells 4x4, leaf cap 512; FSG cell 0.001 deg",
+                      "l2": "flushed between steps (256 MiB write); point arrays 1.6 GB in, 3.2 GB out per index",
+                      "parallelism": f"replicas x{world}"}, dtype="fp32-cell/int32")
+    line.update({
+        "e2e": {"value": round(2 * P * world * args.steps / (etot / 1e3), 1), "unit": "points/s",
+                "h2d_bytes_per_step": int(t.lon.nbytes + t.lat.nbytes + t.lengths.nbytes),
+                "d2h_bytes_per_step": 2 * 8 * 8},
+        "gpu_launches": int(launches),
+        "launches_note": "counts this library's kernels and the CUB radix-sort / scan passes it issues",
+        "indexes": {"grid": info[0], "fsg": info[1]},
+        "roofline": build_roofline(st),
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    })
+    ctx.close()
+    return line
+
+
+def run_reference_build(args, world, rank):
+    if rank != 0:
+        return None
+    times, v, ps = [], 0.0, 0
+    for s in range(args.warmup + args.steps):
+        v, sec, ps = build_reference_sample()
+        if s >= args.warmup:
+            times.append(sec)
+    sec = sum(times)
+    v = 2 * ps * args.steps / sec
+    line = base_line(args, world, "index build points/s (GT-quadtree Grid + FVTable, and FSG)", "points/s", v, sec * 1e3,
+                     {"workload": f"index builds: first {BUILD['ref_n']} trajectories of the C3 set ({ps} points), "
+                                  "Grid cell 0.001 deg, leaf cap 512; FSG cell 0.001 deg"}, dtype="fp32-cell/int32")
+    line.update({"impl": "reference",
+                 "cpu_baseline": {"value": round(v, 1), "unit": "points/s", "cores": 1, "kind": "reference",
+                                  "sample": f"first {BUILD['ref_n']} of the 1M trajectories per step (the reference's "
+                                            "Grid build allocates and clears a cell-sized array per trajectory, "
+                                            "Grid.cpp:268-269, so the full set does not finish in minutes)"},
+                 "e2e": {"value": round(v, 1), "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return line
+
+
+WORKLOADS = {"c1": run_c1, "c2": None, "c3": run_c3, "c4": run_c4, "c4k": run_c4k, "c5": run_c5, "build": run_build}
+REFERENCE = {"c1": run_reference_c1, "c2": None, "c4": run_reference_c4, "build": run_reference_build}
 
 
 def main():
@@ -1079,7 +1228,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c4k", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c4k", "c5", "build"])
     ap.add_argument("--cpu-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=0, help="C2: use only the first N of the 256 queries")

@@ -91,7 +91,12 @@ class Context:
 
     @property
     def scratch_bytes(self) -> int:
+        """Device bytes held by the scratch arena and the index-build temporaries kept for reuse."""
         return int(lib.gat_ctx_scratch_bytes(self.h))
+
+    def trim(self) -> None:
+        """Returns the scratch arena and kept index-build temporaries to the device (gat_ctx_trim)."""
+        self.check(lib.gat_ctx_trim(self.h), "gat_ctx_trim")
 
     def close(self) -> None:
         if getattr(self, "h", None):

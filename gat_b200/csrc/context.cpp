@@ -220,6 +220,7 @@ int gat_ctx_trim(gat_ctx* ctx) {
         ctx->slot_ptr[i] = nullptr;
         ctx->slot_bytes[i] = 0;
     }
+    if (ctx->build_pool) cudaMemPoolTrimTo(ctx->build_pool, 0);
     return GAT_OK;
 }
 
@@ -236,6 +237,7 @@ void gat_ctx_destroy(gat_ctx* ctx) {
     for (cudaEvent_t e : ctx->ev_free) cudaEventDestroy(e);
     for (void* p : ctx->slot_ptr)
         if (p) cudaFree(p);
+    if (ctx->build_pool) cudaMemPoolDestroy(ctx->build_pool);
     if (ctx->d_flag) cudaFree(ctx->d_flag);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -341,6 +343,11 @@ int64_t gat_ctx_scratch_bytes(const gat_ctx* ctx) {
     if (!ctx) return 0;
     int64_t s = 0;
     for (size_t b : ctx->slot_bytes) s += (int64_t)b;
+    if (ctx->build_pool) {
+        uint64_t held = 0;
+        if (cudaMemPoolGetAttribute(ctx->build_pool, cudaMemPoolAttrReservedMemCurrent, &held) == cudaSuccess)
+            s += (int64_t)held;
+    }
     return s;
 }
 
@@ -364,22 +371,25 @@ int gat_db_create(gat_ctx* ctx, int n, const int32_t* lengths, const float* lon,
         if (lengths[t - 1] > db->maxlen) db->maxlen = lengths[t - 1];
     }
     db->npoints = db->h_off[n + 1];
-    db->h_x.assign(lon, lon + db->npoints);
-    db->h_y.assign(lat, lat + db->npoints);
     if (ctx->device < 0) {
+        db->h_x.assign(lon, lon + db->npoints);
+        db->h_y.assign(lat, lat + db->npoints);
         *out = db;
         return GAT_OK;
     }
-    std::vector<float2> xy(db->npoints);
-    for (int64_t i = 0; i < db->npoints; i++) xy[i] = make_float2(lon[i], lat[i]);
+    /* the host copies of the points are downloaded when a host builder or a snapshot needs them */
+    db->host_pending = true;
     cudaError_t e;
     if ((e = cudaMalloc(&db->d_len, (n + 1) * sizeof(int32_t))) != cudaSuccess ||
         (e = cudaMalloc(&db->d_off, (n + 2) * sizeof(int64_t))) != cudaSuccess ||
         (e = cudaMalloc(&db->d_xy, (db->npoints + 1) * sizeof(float2))) != cudaSuccess ||
         (e = cudaMemcpy(db->d_len, db->h_len.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(db->d_off, db->h_off.data(), (n + 2) * sizeof(int64_t), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(db->d_xy, xy.data(), db->npoints * sizeof(float2), cudaMemcpyHostToDevice)) != cudaSuccess) {
+        (e = cudaMemcpy(db->d_off, db->h_off.data(), (n + 2) * sizeof(int64_t), cudaMemcpyHostToDevice)) != cudaSuccess) {
         int rc = cuda_fail(ctx, e, "gat_db_create");
+        gat_db_destroy(db);
+        return rc;
+    }
+    if (int rc = upload_set_points(ctx, lon, lat, db->npoints, db->d_xy)) {
         gat_db_destroy(db);
         return rc;
     }

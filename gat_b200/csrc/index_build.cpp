@@ -301,6 +301,7 @@ static int build_grid(gat_index* ix, gat_mbb range, float cell, int vparam, int 
         DevicePlaceArgs a{"gat_grid_build", true, range.xmin, range.ymax, cell, axis, 0, 0, vparam, g.cellnum};
         return device_build_grid(ix, a, g.total_level, leaf_cap);
     }
+    if (int st = db_host_copies(ix->db)) return st;
     std::vector<int64_t> cb;
     std::vector<int64_t> fv_off;
     std::vector<int32_t> fv_cell, fv_cnt;
@@ -439,6 +440,7 @@ void flatten(const SNode* nd, std::vector<const SNode*>& order) {
 
 static int build_stig(gat_index* ix, int block) {
     const gat_db* db = ix->db;
+    if (int st = db_host_copies(db)) return st;
     /* STIG::initial (STIG.cpp:35-66): points in trajectory order */
     std::vector<SP> pts(db->npoints);
     for (int t = 1; t <= db->n; t++)
@@ -531,6 +533,7 @@ static int build_fsg(gat_index* ix, gat_mbb range, float cell) {
         DevicePlaceArgs a{"gat_fsg_build", false, range.xmin, range.ymax, cell, 0, nx, ny, 0, f.cellnum};
         return device_build_fsg(ix, a);
     }
+    if (int st = db_host_copies(ix->db)) return st;
     std::vector<int64_t> cb;
     RunSet rs;
     if (make_runs(ix->db, cell_of, rs) != GAT_OK)

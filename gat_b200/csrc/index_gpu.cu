@@ -5,34 +5,32 @@
  * Both indexes order points by cell, trajectories ascending within a cell and points in
  * trajectory order within a trajectory: a stable sort by cell of the set's points taken in
  * trajectory order. The build runs entirely in HBM:
- *   1. cells      a warp per trajectory computes each point's cell with the builders' float
- *                 expressions (IEEE single subtract and divide, truncation toward zero);
+ *   1. cells      every point's cell from the builders' float expressions (IEEE single
+ *                 subtract and divide, truncation toward zero), four points in flight per thread;
  *   2. sort       a stable LSD radix sort of (cell, position) pairs;
  *   3. gather     x / y / trajectory / key in sorted order; a point's trajectory comes from a
- *                 per-1024-point hint table and a short binary search of the offsets (L2-resident);
+ *                 per-256-point hint table and a short binary search of the offsets (L2-resident);
  *   4. bounds     cell boundaries by binary search over the sorted cells;
  *   5. quadtree   (Grid) level by level: split flags, a scan, children written in parents' order,
  *                 which is the breadth-first order of the reference's queue; node MBBs from the
  *                 same float expressions as the host builder;
- *   6. vectors    (Grid) each trajectory's (virtual cell, count) list in ascending cell order: a
- *                 warp sorts the trajectory's virtual cells in shared memory and counts runs;
- *                 sets with a trajectory longer than kFvLocal sort (trajectory, virtual cell)
- *                 keys globally instead.
+ *   6. vectors    (Grid) each trajectory's (virtual cell, count) list in ascending cell order:
+ *                 runs of equal virtual cells (a walk stays in one for many points) keyed
+ *                 (trajectory, virtual cell), radix-sorted, counts summed per key.
  * The host copies of the points are downloaded only when asked for (gat_index_points,
- * snapshots). The radix sorts, scans and run-length encoding are CUB's (the CUDA toolkit's
+ * snapshots). The radix sorts, scans, selection and reduce-by-key are CUB's (the CUDA toolkit's
  * header library); an index build runs once per trajectory set and is not on the query path. */
 #include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_run_length_encode.cuh>
+#include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 
 #include "internal.h"
 
 namespace gat {
 namespace {
 
-constexpr int kHintShift = 10;  /* one trajectory hint per 1024 points */
-constexpr int kFvLocal = 2048;  /* longest trajectory whose vector a warp sorts in shared memory */
-constexpr int kFvWarps = 4;     /* warps per block of the local vector kernel (8 KB each) */
+constexpr int kHintShift = 8;   /* one trajectory hint per 256 points */
 constexpr int kMaxLevels = 32;
 
 struct CellParams {
@@ -80,34 +78,17 @@ __device__ __forceinline__ int point_cell(const CellParams& p, float lon, float 
     return row * p.nx + col;
 }
 
-/* 1. a warp per trajectory: cell and position of each point, the trajectory holding every
- * 1024th point (hint), and for the global vector path the key (trajectory << 32 | vcell) */
-__global__ void k_point_cells(int n, const int64_t* __restrict__ off, const float2* __restrict__ xy, CellParams p,
-                              uint32_t* cell, int32_t* pos, int32_t* hint, unsigned long long* fvkey, int32_t* flag) {
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int t = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t <= n; t += nw) {
-        const int64_t s = off[t], e = off[t + 1];
-        bool bad = false;
-        for (int64_t i = s + lane; i < e; i += 32) {
-            const float2 v = xy[i];
-            int c = point_cell(p, v.x, v.y);
-            if (c < 0) {
-                bad = true;
-                c = 0;
-            }
-            cell[i] = (uint32_t)c;
-            pos[i] = (int32_t)i;
-            if ((i & ((1 << kHintShift) - 1)) == 0) hint[i >> kHintShift] = t;
-            if (fvkey) fvkey[i] = ((unsigned long long)(unsigned)t << 32) | (unsigned)(c >> p.vparam);
-        }
-        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicCAS(flag, 0, GAT_ERR_ARG);
+/* the trajectory holding every 256th point: hint[b] = the trajectory of point b << kHintShift */
+__global__ void k_hints(int n, const int64_t* __restrict__ off, int32_t* hint) {
+    for (int t = 1 + blockIdx.x * blockDim.x + threadIdx.x; t <= n; t += gridDim.x * blockDim.x) {
+        const int64_t e = off[t + 1];
+        for (int64_t b = (off[t] + (1 << kHintShift) - 1) >> kHintShift; (b << kHintShift) < e; b++) hint[b] = t;
     }
 }
 
 /* the trajectory holding point s: the largest t with off[t] <= s, searched between the hints of
- * s's 1024-point block and the next (an empty trajectory shares its successor's offset and so is
- * never the largest) */
+ * s's block and the next (an empty trajectory shares its successor's offset and so is never the
+ * largest) */
 __device__ __forceinline__ int holder(int64_t s, int n, const int64_t* __restrict__ off, const int32_t* __restrict__ hint,
                                       int64_t nhint) {
     const int64_t b = s >> kHintShift;
@@ -122,21 +103,87 @@ __device__ __forceinline__ int holder(int64_t s, int n, const int64_t* __restric
     return lo;
 }
 
+constexpr int kPerThread = 4; /* points each thread of the placement kernels keeps in flight */
+
+/* 1. cell and position of every point (trajectory order). Each thread loads kPerThread points
+ * before using any. */
+__global__ void k_point_cells(int64_t P, const float2* __restrict__ xy, CellParams p, uint32_t* cell, int32_t* pos,
+                              int32_t* flag) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < P; i0 += stride * kPerThread) {
+        float2 v[kPerThread];
+#pragma unroll
+        for (int k = 0; k < kPerThread; k++) {
+            const int64_t i = i0 + k * stride;
+            v[k] = i < P ? xy[i] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < kPerThread; k++) {
+            const int64_t i = i0 + k * stride;
+            if (i >= P) break;
+            int c = point_cell(p, v[k].x, v[k].y);
+            if (c < 0) {
+                bad = true;
+                c = 0;
+            }
+            cell[i] = (uint32_t)c;
+            pos[i] = (int32_t)i;
+        }
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicCAS(flag, 0, GAT_ERR_ARG);
+}
+
 /* 3. index-order arrays from the sorted positions; key = tid << pidx_bits | pidx, or 0 when the
- * pair does not fit 32 bits (pidx_bits < 0; the point index then goes to pidx) */
+ * pair does not fit 32 bits (pidx_bits < 0; the point index then goes to pidx). Each thread
+ * resolves kPerThread points together so that their loads overlap. */
 __global__ void k_gather_points(int64_t P, int n, const int32_t* __restrict__ order, const int64_t* __restrict__ off,
                                 const int32_t* __restrict__ hint, int64_t nhint, const float2* __restrict__ xy, float* x,
                                 float* y, int32_t* tid, uint32_t* key, int32_t* pidx, int pidx_bits) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x) {
-        const int s = order[i];
-        const float2 v = xy[s];
-        const int t = holder(s, n, off, hint, nhint);
-        const int k = (int)(s - off[t]);
-        x[i] = v.x;
-        y[i] = v.y;
-        tid[i] = t;
-        key[i] = pidx_bits >= 0 ? ((uint32_t)t << pidx_bits) | (uint32_t)k : 0u;
-        if (pidx) pidx[i] = k;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < P; i0 += stride * kPerThread) {
+        int s[kPerThread], lo[kPerThread], hi[kPerThread];
+        float2 v[kPerThread];
+#pragma unroll
+        for (int k = 0; k < kPerThread; k++) {
+            const int64_t i = i0 + k * stride;
+            s[k] = i < P ? order[i] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < kPerThread; k++) {
+            const int64_t b = s[k] >> kHintShift;
+            v[k] = xy[s[k]];
+            lo[k] = hint[b];
+            hi[k] = b + 1 < nhint ? hint[b + 1] : n;
+        }
+        /* the binary searches of the kPerThread points advance in lockstep */
+        for (;;) {
+            bool open = false;
+#pragma unroll
+            for (int k = 0; k < kPerThread; k++) {
+                if (lo[k] < hi[k]) {
+                    const int mid = (lo[k] + hi[k] + 1) >> 1;
+                    if (off[mid] <= s[k])
+                        lo[k] = mid;
+                    else
+                        hi[k] = mid - 1;
+                    open = true;
+                }
+            }
+            if (!open) break;
+        }
+#pragma unroll
+        for (int k = 0; k < kPerThread; k++) {
+            const int64_t i = i0 + k * stride;
+            if (i >= P) break;
+            const int t = lo[k];
+            const int q = (int)(s[k] - off[t]);
+            x[i] = v[k].x;
+            y[i] = v[k].y;
+            tid[i] = t;
+            key[i] = pidx_bits >= 0 ? ((uint32_t)t << pidx_bits) | (uint32_t)q : 0u;
+            if (pidx) pidx[i] = q;
+        }
     }
 }
 
@@ -237,117 +284,95 @@ __global__ void k_tree_nodes(int64_t N, LevelTable lt, const int32_t* __restrict
 }
 
 /* ---------------------------------------------------------------- 6. frequency vectors */
-/* Sorts the warp's n values in place (bitonic, padded to a power of two with UINT_MAX). */
-__device__ void warp_sort(uint32_t* v, int n, int lane) {
-    int m = 32;
-    while (m < n) m <<= 1;
-    for (int i = n + lane; i < m; i += 32) v[i] = 0xffffffffu;
-    __syncwarp();
-    for (int k = 2; k <= m; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = lane; i < m; i += 32) {
-                const int p = i ^ j;
-                if (p > i) {
-                    const uint32_t a = v[i], b = v[p];
-                    const bool up = (i & k) == 0;
-                    if ((a > b) == up) {
-                        v[i] = b;
-                        v[p] = a;
-                    }
-                }
-            }
-            __syncwarp();
-        }
+/* run heads of equal virtual cells: 1 where a point's virtual cell differs from its
+ * predecessor's (trajectory starts are marked by k_fv_starts) */
+__global__ void k_fv_heads(int64_t P, const uint32_t* __restrict__ cells, int vparam, uint8_t* head) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x)
+        head[i] = (i == 0 || (cells[i] >> vparam) != (cells[i - 1] >> vparam)) ? 1 : 0;
+}
+
+__global__ void k_fv_starts(int n, const int64_t* __restrict__ off, uint8_t* head) {
+    for (int t = 1 + blockIdx.x * blockDim.x + threadIdx.x; t <= n; t += gridDim.x * blockDim.x)
+        if (off[t + 1] > off[t]) head[off[t]] = 1;
+}
+
+/* per run: key (trajectory << 32 | virtual cell) and point count */
+__global__ void k_fv_runs(int64_t R, int64_t P, int n, const int32_t* __restrict__ starts, const int64_t* __restrict__ off,
+                          const int32_t* __restrict__ hint, int64_t nhint, const uint32_t* __restrict__ cells, int vparam,
+                          unsigned long long* key, int32_t* cnt) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = starts[r], e = r + 1 < R ? starts[r + 1] : P;
+        const int t = holder(s, n, off, hint, nhint);
+        key[r] = ((unsigned long long)(unsigned)t << 32) | (unsigned)(cells[s] >> vparam);
+        cnt[r] = (int32_t)(e - s);
     }
 }
 
-/* a warp per trajectory (length <= kFvLocal): sorted virtual cells, run-length counted into
- * tmp at the trajectory's own offset; nnz[t] entries; the largest count to max_nnz */
-__global__ void __launch_bounds__(kFvWarps * 32) k_fv_local(int n, const int64_t* __restrict__ off,
-                                                            const uint32_t* __restrict__ cells, int vparam,
-                                                            int32_t* tmp_cell, int32_t* tmp_cnt, int64_t* nnz,
-                                                            int32_t* max_nnz) {
-    __shared__ uint32_t sv[kFvWarps][kFvLocal];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    uint32_t* v = sv[w];
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    int mx = 0;
-    for (int t = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t <= n; t += nw) {
-        const int64_t s = off[t];
-        const int L = (int)(off[t + 1] - s);
-        for (int i = lane; i < L; i += 32) v[i] = cells[s + i] >> vparam;
-        __syncwarp();
-        warp_sort(v, L, lane);
-        /* run heads: the first index of each distinct value; count = next head - head */
-        int written = 0;
-        for (int base = 0; base < L; base += 32) {
-            const int i = base + lane;
-            const bool head = i < L && (i == 0 || v[i] != v[i - 1]);
-            const unsigned hm = __ballot_sync(0xffffffffu, head);
-            if (head) {
-                int j = i + 1;
-                while (j < L && v[j] == v[i]) j++;
-                const int r = written + __popc(hm & ((1u << lane) - 1));
-                tmp_cell[s + r] = (int32_t)v[i];
-                tmp_cnt[s + r] = j - i;
-            }
-            written += __popc(hm);
-        }
-        if (lane == 0) nnz[t] = written;
-        mx = max(mx, written);
-        __syncwarp();
-    }
-    if (lane == 0 && mx > 0) atomicMax(max_nnz, mx);
-}
+struct AddInt {
+    __device__ __forceinline__ int operator()(int a, int b) const { return a + b; }
+};
 
-/* entries of trajectory t from tmp (at off[t]) to the CSR (at fv_off[t]) */
-__global__ void k_fv_compact(int n, const int64_t* __restrict__ off, const int64_t* __restrict__ fv_off,
-                             const int32_t* __restrict__ tmp_cell, const int32_t* __restrict__ tmp_cnt, int32_t* fv_cell,
-                             int32_t* fv_cnt) {
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int t = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); t <= n; t += nw) {
-        const int64_t s = off[t], d = fv_off[t], k = fv_off[t + 1] - d;
-        for (int64_t i = lane; i < k; i += 32) {
-            fv_cell[d + i] = tmp_cell[s + i];
-            fv_cnt[d + i] = tmp_cnt[s + i];
-        }
-    }
-}
-
-/* frequency-vector cells of the global path: the low half of each (trajectory, vcell) run key */
+/* frequency-vector cells: the low half of each (trajectory, virtual cell) key */
 __global__ void k_fv_cells(int64_t R, const unsigned long long* __restrict__ runs, int32_t* cell) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x)
         cell[r] = (int32_t)(runs[r] & 0xffffffffull);
 }
 
 /* ---------------------------------------------------------------- host side */
-/* device allocations of one build, freed with it */
+/* The context's pool for index-build temporaries: stream-ordered, and it keeps freed memory
+ * (release threshold unbounded), so repeated builds do not map and unmap gigabytes each time;
+ * gat_ctx_trim returns it. Null when the device has no memory pools. */
+cudaMemPool_t build_pool(gat_ctx* ctx) {
+    if (ctx->build_pool) return ctx->build_pool;
+    int ok = 0;
+    if (cudaDeviceGetAttribute(&ok, cudaDevAttrMemoryPoolsSupported, ctx->device) != cudaSuccess || !ok) return nullptr;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    ctx->build_pool = pool;
+    return pool;
+}
+
+/* device temporaries of one build, taken from the context's pool in stream order and returned
+ * to it (after the work queued on the stream) when the build ends */
 struct Temps {
+    gat_ctx* ctx;
+    cudaMemPool_t pool;
     std::vector<void*> ptrs;
     cudaError_t err = cudaSuccess;
-    Temps() = default;
+    explicit Temps(gat_ctx* c) : ctx(c), pool(build_pool(c)) {}
     Temps(const Temps&) = delete;
     Temps& operator=(const Temps&) = delete;
     ~Temps() {
         for (void* p : ptrs)
-            if (p) cudaFree(p);
+            if (p) drop(p);
+    }
+    void drop(void* p) {
+        if (pool)
+            cudaFreeAsync(p, ctx->stream);
+        else
+            cudaFree(p);
     }
     template <class T>
     T* get(size_t n) {
         if (err != cudaSuccess) return nullptr;
         void* p = nullptr;
-        err = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+        const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        err = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, ctx->stream) : cudaMalloc(&p, bytes);
         if (err != cudaSuccess) return nullptr;
         ptrs.push_back(p);
         return static_cast<T*>(p);
     }
-    /* frees one temporary early (stream-ordered work that reads it must be complete or on the
-     * same stream: cudaFree waits for the device) */
+    /* returns one temporary early (stream-ordered: after the work already queued) */
     void release(void* p) {
         for (auto& q : ptrs)
             if (q && q == p) {
-                cudaFree(q);
+                drop(q);
                 q = nullptr;
             }
     }
@@ -381,11 +406,13 @@ T* alloc_padded(gat_index* ix, int64_t count, int* st) {
  * uploads them), the cells in trajectory order and the boundaries d_cb[0..ncells]. */
 struct Placement {
     uint32_t* cells = nullptr; /* trajectory order */
+    int32_t* pos = nullptr;    /* 0, 1, 2, ... (the sort's values) */
+    int32_t* hint = nullptr;   /* trajectory of every 256th point */
+    int64_t nhint = 0;
     int64_t* d_cb = nullptr;
-    unsigned long long* fvkey = nullptr; /* global vector path only */
 };
 
-int place(gat_index* ix, const DevicePlaceArgs& a, bool fv_keys, Temps& tmp, Placement& out) {
+int place(gat_index* ix, const DevicePlaceArgs& a, Temps& tmp, Placement& out) {
     gat_ctx* ctx = ix->ctx;
     const gat_db* db = ix->db;
     cudaStream_t s = ctx->stream;
@@ -399,16 +426,16 @@ int place(gat_index* ix, const DevicePlaceArgs& a, bool fv_keys, Temps& tmp, Pla
     int32_t* order = tmp.get<int32_t>(P);
     int32_t* hint = tmp.get<int32_t>(nhint);
     int64_t* d_cb = tmp.get<int64_t>((size_t)a.ncells + 1);
-    unsigned long long* fvk = fv_keys ? tmp.get<unsigned long long>(P) : nullptr;
     if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
     CellParams cp{a.rxmin, a.rymax, a.cell, a.morton ? 1 : 0, a.axis, a.nx, a.ny, a.vparam};
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int32_t), s), "index build");
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(hint, 0, (size_t)nhint * 4, s), "index build");
     if (P > 0) {
+        k_hints<<<grid_size(ctx, n), 256, 0, s>>>(n, db->d_off, hint);
+        count_launch(ctx);
         timed_begin(ctx, GAT_KERNEL_INDEX_BUILD);
-        k_point_cells<<<grid_size(ctx, (int64_t)n * 32), 256, 0, s>>>(n, db->d_off, db->d_xy, cp, cells, pos, hint, fvk,
-                                                                      ctx->d_flag);
-        timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * (16 + (fvk ? 8 : 0)) + (double)n * 16);
+        k_point_cells<<<grid_size(ctx, (P + kPerThread - 1) / kPerThread), 256, 0, s>>>(P, db->d_xy, cp, cells, pos,
+                                                                                       ctx->d_flag);
+        timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * 16);
         count_launch(ctx);
     }
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (cells)");
@@ -445,8 +472,8 @@ int place(gat_index* ix, const DevicePlaceArgs& a, bool fv_keys, Temps& tmp, Pla
     if (pidx_bits < 0) GAT_CUDA_TRY(ctx, cudaMalloc(&ix->d_pidx, std::max<size_t>((size_t)P, 1) * 4), "index build");
     if (P > 0) {
         timed_begin(ctx, GAT_KERNEL_INDEX_BUILD);
-        k_gather_points<<<grid_size(ctx, P), 256, 0, s>>>(P, n, order, db->d_off, hint, nhint, db->d_xy, dx, dy, dt, dk,
-                                                          ix->d_pidx, pidx_bits);
+        k_gather_points<<<grid_size(ctx, (P + kPerThread - 1) / kPerThread), 256, 0, s>>>(
+            P, n, order, db->d_off, hint, nhint, db->d_xy, dx, dy, dt, dk, ix->d_pidx, pidx_bits);
         timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * (28 + (pidx_bits < 0 ? 4 : 0)));
         count_launch(ctx);
     }
@@ -456,8 +483,10 @@ int place(gat_index* ix, const DevicePlaceArgs& a, bool fv_keys, Temps& tmp, Pla
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (gather)");
     ix->host_pending = true;
     out.cells = cells;
+    out.pos = pos;
+    out.hint = hint;
+    out.nhint = nhint;
     out.d_cb = d_cb;
-    out.fvkey = fvk;
     return GAT_OK;
 }
 
@@ -552,7 +581,8 @@ int build_tree(gat_index* ix, const Placement& pl, const TreeParams& tp, Temps& 
     return GAT_OK;
 }
 
-/* Step 6: the frequency-vector CSR (fv_off [n+2], fv_cell, fv_cnt), allocated after the nodes. */
+/* Step 6: the frequency-vector CSR (fv_off [n+2], fv_cell, fv_cnt), allocated after the nodes:
+ * runs of equal virtual cells keyed (trajectory, virtual cell), sorted, and counts summed per key. */
 int build_vectors(gat_index* ix, const Placement& pl, int vparam, Temps& tmp) {
     gat_ctx* ctx = ix->ctx;
     cudaStream_t s = ctx->stream;
@@ -563,89 +593,73 @@ int build_vectors(gat_index* ix, const Placement& pl, int vparam, Temps& tmp) {
     int64_t* off = alloc_padded<int64_t>(ix, n + 2, &st);
     if (!off) return st;
     ix->d_fv_off = off;
-    int64_t R = 0;
-    if (!pl.fvkey) {
-        /* local: a warp sorts each trajectory's virtual cells */
-        int32_t* tcell = tmp.get<int32_t>(P);
-        int32_t* tcnt = tmp.get<int32_t>(P);
-        int64_t* nnz = tmp.get<int64_t>((size_t)n + 2);
-        int32_t* mx = tmp.get<int32_t>(1);
-        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(nnz, 0, ((size_t)n + 2) * 8, s), "index build fv");
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(mx, 0, 4, s), "index build fv");
-        if (n > 0) {
-            k_fv_local<<<grid_size(ctx, (int64_t)n * 32, kFvWarps * 32), kFvWarps * 32, 0, s>>>(
-                n, db->d_off, pl.cells, vparam, tcell, tcnt, nnz, mx);
-            count_launch(ctx);
-        }
+    uint8_t* head = tmp.get<uint8_t>(P);
+    int32_t* starts = tmp.get<int32_t>(P);
+    int32_t* nsel = tmp.get<int32_t>(1);
+    if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+    int32_t R = 0;
+    if (P > 0) {
+        k_fv_heads<<<grid_size(ctx, P), 256, 0, s>>>(P, pl.cells, vparam, head);
+        k_fv_starts<<<grid_size(ctx, n), 256, 0, s>>>(n, db->d_off, head);
+        count_launch(ctx, 2);
         size_t need = 0;
-        GAT_CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(nullptr, need, nnz, off, n + 2, s), "index build fv");
-        void* stmp = tmp.get<char>(need);
+        GAT_CUDA_TRY(ctx, cub::DeviceSelect::Flagged(nullptr, need, pl.pos, head, starts, nsel, (int)P, s), "index build fv");
+        void* t1 = tmp.get<char>(need);
         if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-        GAT_CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(stmp, need, nnz, off, n + 2, s), "index build fv");
-        count_launch(ctx);
-        int32_t hmx = 0;
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R, off + n + 1, 8, cudaMemcpyDeviceToHost, s), "index build fv");
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&hmx, mx, 4, cudaMemcpyDeviceToHost, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cub::DeviceSelect::Flagged(t1, need, pl.pos, head, starts, nsel, (int)P, s), "index build fv");
+        count_launch(ctx, 2);
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R, nsel, 4, cudaMemcpyDeviceToHost, s), "index build fv");
         GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
-        int32_t* cell = alloc_padded<int32_t>(ix, R, &st);
-        int32_t* cnt = cell ? alloc_padded<int32_t>(ix, R, &st) : nullptr;
-        if (!cnt) return st;
-        ix->d_fv_cell = cell;
-        ix->d_fv_cnt = cnt;
-        if (n > 0) {
-            k_fv_compact<<<grid_size(ctx, (int64_t)n * 32), 256, 0, s>>>(n, db->d_off, off, tcell, tcnt, cell, cnt);
-            count_launch(ctx);
-        }
-        ix->fv_max_nnz = hmx;
-    } else {
-        /* global: (trajectory, virtual cell) keys sorted and run-length counted */
-        unsigned long long* fvk_s = tmp.get<unsigned long long>(P);
-        unsigned long long* runs = tmp.get<unsigned long long>(P);
-        int32_t* rcnt = tmp.get<int32_t>(P + 1);
-        int32_t* nruns = tmp.get<int32_t>(1);
-        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(nruns, 0, 4, s), "index build fv");
-        if (P > 0) {
-            /* keys hold the trajectory above bit 32 and the virtual cell below it */
-            const int kbits = 32 + bits_to_hold(n);
-            size_t b1 = 0, b2 = 0;
-            GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortKeys(nullptr, b1, pl.fvkey, fvk_s, (int)P, 0, kbits, s),
-                         "index build fv");
-            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(nullptr, b2, fvk_s, runs, rcnt, nruns, (int)P, s),
-                         "index build fv");
-            void* t2 = tmp.get<char>(std::max(b1, b2));
-            if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-            GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortKeys(t2, b1, pl.fvkey, fvk_s, (int)P, 0, kbits, s), "index build fv");
-            GAT_CUDA_TRY(ctx, cub::DeviceRunLengthEncode::Encode(t2, b2, fvk_s, runs, rcnt, nruns, (int)P, s),
-                         "index build fv");
-            count_launch(ctx, 2 * ((kbits + 7) / 8) + 3);
-        }
-        int32_t R32 = 0;
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R32, nruns, 4, cudaMemcpyDeviceToHost, s), "index build fv");
-        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
-        R = R32;
-        int32_t* cell = alloc_padded<int32_t>(ix, R, &st);
-        int32_t* cnt = cell ? alloc_padded<int32_t>(ix, R, &st) : nullptr;
-        if (!cnt) return st;
-        ix->d_fv_cell = cell;
-        ix->d_fv_cnt = cnt;
-        if (R > 0) {
-            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, rcnt, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "index build fv");
-            k_fv_cells<<<grid_size(ctx, R), 256, 0, s>>>(R, runs, cell);
-            count_launch(ctx);
-        }
-        /* off[t] = entries of trajectories below t: the first run whose key is >= t << 32 */
-        k_bounds<unsigned long long><<<grid_size(ctx, n + 2), 256, 0, s>>>(R, n + 1, runs, 32, off);
-        count_launch(ctx);
-        std::vector<int64_t> h((size_t)n + 2);
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), off, h.size() * 8, cudaMemcpyDeviceToHost, s), "index build fv");
-        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
-        int hmx = 0;
-        for (int t = 0; t <= n; t++) hmx = std::max<int>(hmx, (int)(h[(size_t)t + 1] - h[(size_t)t]));
-        ix->fv_max_nnz = hmx;
     }
-    ix->fv_entries = R;
+    int32_t E = 0;
+    unsigned long long* uk = nullptr;
+    int32_t* sums = nullptr;
+    if (R > 0) {
+        unsigned long long* key = tmp.get<unsigned long long>(R);
+        unsigned long long* key_s = tmp.get<unsigned long long>(R);
+        int32_t* cnt = tmp.get<int32_t>(R);
+        int32_t* cnt_s = tmp.get<int32_t>(R);
+        uk = tmp.get<unsigned long long>(R);
+        sums = tmp.get<int32_t>(R);
+        int32_t* nuniq = tmp.get<int32_t>(1);
+        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+        k_fv_runs<<<grid_size(ctx, R), 256, 0, s>>>(R, P, n, starts, db->d_off, pl.hint, pl.nhint, pl.cells, vparam, key, cnt);
+        count_launch(ctx);
+        /* keys hold the trajectory above bit 32 and the virtual cell below it */
+        const int kbits = 32 + bits_to_hold(n);
+        size_t b1 = 0, b2 = 0;
+        GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(nullptr, b1, key, key_s, cnt, cnt_s, R, 0, kbits, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cub::DeviceReduce::ReduceByKey(nullptr, b2, key_s, uk, cnt_s, sums, nuniq, AddInt(), R, s),
+                     "index build fv");
+        void* t2 = tmp.get<char>(std::max(b1, b2));
+        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+        GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(t2, b1, key, key_s, cnt, cnt_s, R, 0, kbits, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cub::DeviceReduce::ReduceByKey(t2, b2, key_s, uk, cnt_s, sums, nuniq, AddInt(), R, s),
+                     "index build fv");
+        count_launch(ctx, 2 * ((kbits + 7) / 8) + 3);
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&E, nuniq, 4, cudaMemcpyDeviceToHost, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
+    }
+    int32_t* cell = alloc_padded<int32_t>(ix, E, &st);
+    int32_t* cnt = cell ? alloc_padded<int32_t>(ix, E, &st) : nullptr;
+    if (!cnt) return st;
+    ix->d_fv_cell = cell;
+    ix->d_fv_cnt = cnt;
+    if (E > 0) {
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, sums, (size_t)E * 4, cudaMemcpyDeviceToDevice, s), "index build fv");
+        k_fv_cells<<<grid_size(ctx, E), 256, 0, s>>>(E, uk, cell);
+        count_launch(ctx);
+    }
+    /* off[t] = entries of trajectories below t: the first entry whose key is >= t << 32 */
+    k_bounds<unsigned long long><<<grid_size(ctx, n + 2), 256, 0, s>>>(E, n + 1, uk, 32, off);
+    count_launch(ctx);
+    std::vector<int64_t> h((size_t)n + 2);
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), off, h.size() * 8, cudaMemcpyDeviceToHost, s), "index build fv");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
+    int hmx = 0;
+    for (int t = 0; t <= n; t++) hmx = std::max<int>(hmx, (int)(h[(size_t)t + 1] - h[(size_t)t]));
+    ix->fv_max_nnz = hmx;
+    ix->fv_entries = E;
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build fv");
     return GAT_OK;
 }
@@ -654,10 +668,9 @@ int build_vectors(gat_index* ix, const Placement& pl, int vparam, Temps& tmp) {
 
 int device_build_grid(gat_index* ix, const DevicePlaceArgs& a, int total_level, int leaf_cap) {
     gat_ctx* ctx = ix->ctx;
-    Temps tmp;
+    Temps tmp(ctx);
     Placement pl;
-    const bool global_fv = ix->db->maxlen > kFvLocal;
-    if (int st = place(ix, a, global_fv, tmp, pl)) return st;
+    if (int st = place(ix, a, tmp, pl)) return st;
     TreeParams tp{a.rxmin, a.rymax, a.cell, total_level, leaf_cap};
     if (int st = build_tree(ix, pl, tp, tmp)) return st;
     if (int st = build_vectors(ix, pl, a.vparam, tmp)) return st;
@@ -668,9 +681,9 @@ int device_build_grid(gat_index* ix, const DevicePlaceArgs& a, int total_level, 
 
 int device_build_fsg(gat_index* ix, const DevicePlaceArgs& a) {
     gat_ctx* ctx = ix->ctx;
-    Temps tmp;
+    Temps tmp(ctx);
     Placement pl;
-    if (int st = place(ix, a, false, tmp, pl)) return st;
+    if (int st = place(ix, a, tmp, pl)) return st;
     int st = GAT_OK;
     int32_t* cbeg = alloc_padded<int32_t>(ix, a.ncells, &st);
     int32_t* cend = cbeg ? alloc_padded<int32_t>(ix, a.ncells, &st) : nullptr;
@@ -682,6 +695,49 @@ int device_build_fsg(gat_index* ix, const DevicePlaceArgs& a) {
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "gat_fsg_build");
     GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), "gat_fsg_build");
+    return GAT_OK;
+}
+
+namespace {
+__global__ void k_interleave(int64_t P, const float* __restrict__ lon, const float* __restrict__ lat, float2* xy) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x)
+        xy[i] = make_float2(lon[i], lat[i]);
+}
+}  // namespace
+
+int upload_set_points(gat_ctx* ctx, const float* lon, const float* lat, int64_t P, float2* d_xy) {
+    if (P == 0) return GAT_OK;
+    Temps tmp(ctx);
+    float* d_lon = tmp.get<float>(P);
+    float* d_lat = tmp.get<float>(P);
+    if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "gat_db_create");
+    cudaStream_t s = ctx->stream;
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(d_lon, lon, (size_t)P * 4, cudaMemcpyHostToDevice, s), "gat_db_create");
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(d_lat, lat, (size_t)P * 4, cudaMemcpyHostToDevice, s), "gat_db_create");
+    k_interleave<<<grid_size(ctx, P), 256, 0, s>>>(P, d_lon, d_lat, d_xy);
+    count_launch(ctx);
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "gat_db_create");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "gat_db_create");
+    return GAT_OK;
+}
+
+int db_host_copies(const gat_db* cdb) {
+    gat_db* db = const_cast<gat_db*>(cdb);
+    std::lock_guard<std::mutex> lk(db->host_mu);
+    if (!db->host_pending) return GAT_OK;
+    gat_ctx* ctx = db->ctx;
+    const size_t P = (size_t)db->npoints;
+    std::vector<float2> xy(P);
+    cudaSetDevice(ctx->device);
+    if (P > 0) GAT_CUDA_TRY(ctx, cudaMemcpy(xy.data(), db->d_xy, P * 8, cudaMemcpyDeviceToHost), "trajectory set host copy");
+    std::vector<float> x(P), y(P);
+    for (size_t i = 0; i < P; i++) {
+        x[i] = xy[i].x;
+        y[i] = xy[i].y;
+    }
+    db->h_x.swap(x);
+    db->h_y.swap(y);
+    db->host_pending = false;
     return GAT_OK;
 }
 

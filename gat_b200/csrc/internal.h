@@ -98,6 +98,7 @@ struct gat_ctx {
     int edr_form = 0; /* 0 = autotune, 1 = row tiles, 2 = column tiles */
     int topk_chunk = 0, topk_growth = 0; /* 0 = defaults */
     int index_build = 0;                 /* 0 = device when present, 1 = host, 2 = device */
+    cudaMemPool_t build_pool = nullptr;  /* index-build temporaries, kept for reuse until gat_ctx_trim */
     std::map<uint64_t, int> edr_tune; /* worker contexts use their root's table */
     std::mutex tune_mu;
     /* objects that hold device memory of this context's scratch or workers (cached CUDA graphs);
@@ -112,7 +113,9 @@ struct gat_db {
     int maxlen = 0;
     std::vector<int32_t> h_len;  /* [n+1], h_len[0] = 0 */
     std::vector<int64_t> h_off;  /* [n+2] */
-    std::vector<float> h_x, h_y; /* trajectory order */
+    std::vector<float> h_x, h_y; /* trajectory order; on a device context downloaded on first use */
+    bool host_pending = false;
+    std::mutex host_mu;
     int32_t* d_len = nullptr;
     int64_t* d_off = nullptr;
     float2* d_xy = nullptr;
@@ -260,6 +263,10 @@ struct DevicePlaceArgs {
 };
 int device_build_grid(gat_index* ix, const DevicePlaceArgs& a, int total_level, int leaf_cap);
 int device_build_fsg(gat_index* ix, const DevicePlaceArgs& a);
+/* uploads lon / lat (host, trajectory order) into d_xy as interleaved (lon, lat) pairs */
+int upload_set_points(gat_ctx* ctx, const float* lon, const float* lat, int64_t P, float2* d_xy);
+/* downloads the host copies (h_x, h_y) of a device trajectory set (no-op when present) */
+int db_host_copies(const gat_db* db);
 /* downloads the host copies of a device-placed index (no-op otherwise) */
 int index_host_copies(gat_index* ix);
 /* gat_index_points for a device-placed index without host copies: device arrays straight into

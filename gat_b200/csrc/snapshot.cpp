@@ -123,6 +123,7 @@ int gat_index_save(gat_ctx* ctx, const gat_index* index, const char* path) {
     if (ix->allocs.size() != fields(ix).size())
         return fail(ctx, GAT_ERR_STATE, "gat_index_save: the index's arrays do not match its kind");
     if (int st = index_host_copies(ix)) return st;
+    if (int st = db_host_copies(ix->db)) return st;
     FILE* f = fopen(path, "wb");
     if (!f) return fail(ctx, GAT_ERR_ARG, std::string("gat_index_save: cannot open ") + path);
     Out o{f};
@@ -170,6 +171,7 @@ int gat_index_load(gat_ctx* ctx, const gat_db* db, const char* path, gat_index**
     if (db->ctx != ctx) return fail(ctx, GAT_ERR_STATE, "gat_index_load: trajectory set from another context");
     std::lock_guard<std::mutex> lk(ctx->mu);
     if (ctx->device >= 0) cudaSetDevice(ctx->device);
+    if (int st = db_host_copies(db)) return st;
     FILE* f = fopen(path, "rb");
     if (!f) return fail(ctx, GAT_ERR_ARG, std::string("gat_index_load: cannot open ") + path);
     In in{f};

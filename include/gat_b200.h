@@ -72,14 +72,15 @@ const char* gat_last_error(const gat_ctx* ctx);
  * through the parent, so several host threads can drive one device concurrently. Destroy
  * workers before their parent. */
 int gat_ctx_create_worker(gat_ctx* parent, gat_ctx** out);
-/* Frees the context's scratch arena (it grows again on demand). */
+/* Frees the context's scratch arena and the index-build temporaries it keeps for reuse (both
+ * grow again on demand). */
 int gat_ctx_trim(gat_ctx* ctx);
 /* The cudaStream_t all work of the context is issued on (for event timing by callers). */
 void* gat_ctx_stream(gat_ctx* ctx);
 int gat_ctx_sync(gat_ctx* ctx);
 /* Kernel launches issued by the context since creation (all of them are this library's). */
 int64_t gat_ctx_launches(const gat_ctx* ctx);
-/* Device bytes currently held by the context's scratch arena. */
+/* Device bytes currently held by the context's scratch arena and index-build temporaries. */
 int64_t gat_ctx_scratch_bytes(const gat_ctx* ctx);
 /* Per-kernel timing: when on, launches of the kernel classes below are bracketed by CUDA
  * events on the context stream; gat_ctx_kernel_stats returns their summed device time (ms),

@@ -493,12 +493,15 @@ int cmd_fsg(int argc, char** argv) {
     Data d = read_data(argv[2]);
     Writer w(argv[3]);
     load_tradb(d);
+    double t0 = now_s();
     FSG* f = new FSG(MBB((float)atof(argv[5]), (float)atof(argv[6]), (float)atof(argv[7]),
                          (float)atof(argv[8])),
                      (float)atof(argv[4]));
     f->addDatasetToGrid(tradb, d.n);
+    double t_build = now_s() - t0;
     std::vector<int32_t> meta = {f->cell_num_x, f->cell_num_y, f->cellnum, f->totalPointNum};
     w.i32("meta", meta);
+    w.f64("t_build", {t_build});
     std::vector<float> px, py;
     std::vector<int32_t> pt, cs, ce;
     for (int i = 0; i < f->totalPointNum; i++) {

@@ -155,9 +155,8 @@ def test_point_index_beyond_the_key(gpu_ctx, tmp_path):
 
 
 def test_long_trajectories_and_deep_trees(gpu_ctx, tmp_path):
-    """Trajectories up to 2048 points (vectors sorted per trajectory in shared memory), one of
-    2049 (the whole set then sorts (trajectory, cell) keys globally), and a leaf cap of 1 over a
-    fine grid, whose quadtree outgrows the builder's first node buffer."""
+    """Trajectories of 1 to 2049 points (many runs of virtual cells per trajectory), and a leaf
+    cap of 1 over a fine grid, whose quadtree outgrows the builder's first node buffer."""
     q = D.boxes(200, 1, 0.001, 0.05, 67)
     for top in (2048, 2049):
         lens = D.lengths(400, 0, 0, 0, 1, 300, 68).astype(np.int32)
@@ -172,3 +171,17 @@ def test_long_trajectories_and_deep_trees(gpu_ctx, tmp_path):
     db = G.TrajectorySet(gpu_ctx, t)
     h, d = assert_same_index(gpu_ctx, db, "grid", tmp_path, q, cell=0.001, vparam=3, leaf=1)
     assert d.info()["nodes"] > 1 << 16
+
+
+def test_build_temporaries_kept_until_trim(gpu_ctx):
+    """A device build leaves its temporaries in the context's pool for the next build (counted by
+    scratch_bytes); trim returns them, and a build after the trim still gives the same index."""
+    t = D.walks(D.lengths(3000, 0, 0, 0, 1, 250, 71), 71)
+    db = G.TrajectorySet(gpu_ctx, t)
+    a = build(gpu_ctx, db, "grid", DEVICE, cell=0.005)
+    assert gpu_ctx.scratch_bytes > 0
+    gpu_ctx.trim()
+    assert gpu_ctx.scratch_bytes == 0
+    b = build(gpu_ctx, db, "grid", DEVICE, cell=0.005)
+    for x, y in zip(a.points(), b.points()):
+        assert np.array_equal(x, y)
