@@ -1074,17 +1074,21 @@ def run_c5(args, world, rank, local, td):
 BUILD = dict(cell=0.001, vparam=2, leaf_cap=512, ref_n=40_000)
 
 
+BUILD_TRAFFIC_RATIO = None  # dram read+write / algorithmic bytes of the placement kernels (set from an ncu capture)
+
+
 def build_roofline(st):
     gbs, src = hbm_peak()
     if st["launches"] == 0 or st["ms"] <= 0:
         return None
     ach = st["work"] / (st["ms"] / 1e3) / 1e9
-    return {"kernel": "k_point_cells + k_gather_points", "bound": "hbm", "achieved": round(ach, 1), "peak": gbs,
-            "unit": "GB/s", "frac": round(ach / gbs, 4), "traffic": None,
-            "work_per_launch": st["work"] / st["launches"],
+    per = st["work"] / st["launches"]
+    return {"kernel": "k_point_cells + k_expand_runs", "bound": "hbm", "achieved": round(ach, 1), "peak": gbs,
+            "unit": "GB/s", "frac": round(ach / gbs, 4),
+            "traffic": round(BUILD_TRAFFIC_RATIO * per) if BUILD_TRAFFIC_RATIO else None, "work_per_launch": per,
             "note": "achieved = algorithmic bytes of both placement kernels / their summed event time; k_point_cells "
-                    "16 B per point (x, y read; cell, position written) + 16 B per trajectory, k_gather_points 28 B "
-                    f"per point (position, x, y read; x, y, trajectory, key written); peak of {src}"}
+                    "13 B per point (x, y read; cell and run flag written), k_expand_runs 24 B per point (x, y read; "
+                    f"x, y, trajectory, key written) + 20 B per run (packed run, destination); peak of {src}"}
 
 
 def build_reference_sample():

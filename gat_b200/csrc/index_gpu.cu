@@ -4,19 +4,22 @@
  *
  * Both indexes order points by cell, trajectories ascending within a cell and points in
  * trajectory order within a trajectory: a stable sort by cell of the set's points taken in
- * trajectory order. The build runs entirely in HBM:
+ * trajectory order, which is a stable sort of the maximal runs of consecutive points sharing a
+ * cell (a walk stays in one cell for several points). The build runs entirely in HBM:
  *   1. cells      every point's cell from the builders' float expressions (IEEE single
- *                 subtract and divide, truncation toward zero), four points in flight per thread;
- *   2. sort       a stable LSD radix sort of (cell, position) pairs;
- *   3. gather     x / y / trajectory / key in sorted order; a point's trajectory comes from a
- *                 per-256-point hint table and a short binary search of the offsets (L2-resident);
- *   4. bounds     cell boundaries by binary search over the sorted cells;
+ *                 subtract and divide, truncation toward zero) and a flag where a run starts;
+ *   2. runs       run starts compacted; per run its cell, trajectory (from a per-256-point hint
+ *                 table and a short search of the offsets) and length; runs stably radix-sorted
+ *                 by cell, their lengths scanned into destinations;
+ *   3. expand     each block fills 2048 consecutive index positions from the runs covering
+ *                 them (staged in shared memory): x, y, trajectory, key;
+ *   4. bounds     cell boundaries from the sorted runs' cells and destinations;
  *   5. quadtree   (Grid) level by level: split flags, a scan, children written in parents' order,
  *                 which is the breadth-first order of the reference's queue; node MBBs from the
  *                 same float expressions as the host builder;
  *   6. vectors    (Grid) each trajectory's (virtual cell, count) list in ascending cell order:
- *                 runs of equal virtual cells (a walk stays in one for many points) keyed
- *                 (trajectory, virtual cell), radix-sorted, counts summed per key.
+ *                 cell runs merged into runs of equal virtual cells, keyed (trajectory, virtual
+ *                 cell), radix-sorted, counts summed per key.
  * The host copies of the points are downloaded only when asked for (gat_index_points,
  * snapshots). The radix sorts, scans, selection and reduce-by-key are CUB's (the CUDA toolkit's
  * header library); an index build runs once per trajectory set and is not on the query path. */
@@ -24,6 +27,7 @@
 #include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "internal.h"
 
@@ -103,87 +107,160 @@ __device__ __forceinline__ int holder(int64_t s, int n, const int64_t* __restric
     return lo;
 }
 
-constexpr int kPerThread = 4; /* points each thread of the placement kernels keeps in flight */
+constexpr int kPerThread = 4; /* points each lane of k_point_cells keeps in flight */
 
-/* 1. cell and position of every point (trajectory order). Each thread loads kPerThread points
- * before using any. */
-__global__ void k_point_cells(int64_t P, const float2* __restrict__ xy, CellParams p, uint32_t* cell, int32_t* pos,
+/* 1. every point's cell (trajectory order) and the run heads: 1 where a point's cell differs
+ * from its predecessor's (trajectory starts are marked by k_run_starts). Each warp takes chunks
+ * of 32 x kPerThread consecutive points; a point's predecessor is in the lane below, in lane 31
+ * of the previous step, or (for the chunk's first point) recomputed from the point before. */
+__global__ void k_point_cells(int64_t P, const float2* __restrict__ xy, CellParams p, uint32_t* cell, uint8_t* head,
                               int32_t* flag) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    constexpr int kChunk = 32 * kPerThread;
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     bool bad = false;
-    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < P; i0 += stride * kPerThread) {
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kChunk; base < P; base += nw * kChunk) {
         float2 v[kPerThread];
 #pragma unroll
         for (int k = 0; k < kPerThread; k++) {
-            const int64_t i = i0 + k * stride;
+            const int64_t i = base + k * 32 + lane;
             v[k] = i < P ? xy[i] : make_float2(0.f, 0.f);
         }
+        const float2 before = (lane == 0 && base > 0) ? xy[base - 1] : make_float2(0.f, 0.f);
+        int carry = (lane == 0 && base > 0) ? max(point_cell(p, before.x, before.y), 0) : -1;
 #pragma unroll
         for (int k = 0; k < kPerThread; k++) {
-            const int64_t i = i0 + k * stride;
-            if (i >= P) break;
-            int c = point_cell(p, v[k].x, v[k].y);
+            const int64_t i = base + k * 32 + lane;
+            int c = i < P ? point_cell(p, v[k].x, v[k].y) : 0;
             if (c < 0) {
                 bad = true;
                 c = 0;
             }
-            cell[i] = (uint32_t)c;
-            pos[i] = (int32_t)i;
+            int prev = __shfl_up_sync(0xffffffffu, c, 1);
+            if (lane == 0) prev = carry;
+            carry = __shfl_sync(0xffffffffu, c, 31);
+            if (i < P) {
+                cell[i] = (uint32_t)c;
+                head[i] = (i == 0 || c != prev) ? 1 : 0;
+            }
         }
     }
-    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicCAS(flag, 0, GAT_ERR_ARG);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicCAS(flag, 0, GAT_ERR_ARG);
 }
 
-/* 3. index-order arrays from the sorted positions; key = tid << pidx_bits | pidx, or 0 when the
- * pair does not fit 32 bits (pidx_bits < 0; the point index then goes to pidx). Each thread
- * resolves kPerThread points together so that their loads overlap. */
-__global__ void k_gather_points(int64_t P, int n, const int32_t* __restrict__ order, const int64_t* __restrict__ off,
-                                const int32_t* __restrict__ hint, int64_t nhint, const float2* __restrict__ xy, float* x,
-                                float* y, int32_t* tid, uint32_t* key, int32_t* pidx, int pidx_bits) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < P; i0 += stride * kPerThread) {
-        int s[kPerThread], lo[kPerThread], hi[kPerThread];
-        float2 v[kPerThread];
-#pragma unroll
-        for (int k = 0; k < kPerThread; k++) {
-            const int64_t i = i0 + k * stride;
-            s[k] = i < P ? order[i] : 0;
+/* a run never spans two trajectories */
+__global__ void k_run_starts(int n, const int64_t* __restrict__ off, uint8_t* head) {
+    for (int t = 1 + blockIdx.x * blockDim.x + threadIdx.x; t <= n; t += gridDim.x * blockDim.x)
+        if (off[t + 1] > off[t]) head[off[t]] = 1;
+}
+
+/* 2. per run (trajectory order): its cell, index, trajectory and length */
+__global__ void k_runs(int64_t R, int64_t P, int n, const int32_t* __restrict__ starts, const int64_t* __restrict__ off,
+                       const int32_t* __restrict__ hint, int64_t nhint, const uint32_t* __restrict__ cells,
+                       uint32_t* run_cell, int32_t* run_idx, int32_t* run_tid, int32_t* run_len) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = starts[r], e = r + 1 < R ? starts[r + 1] : P;
+        run_cell[r] = cells[s];
+        run_idx[r] = (int32_t)r;
+        run_tid[r] = holder(s, n, off, hint, nhint);
+        run_len[r] = (int32_t)(e - s);
+    }
+}
+
+/* the runs in sorted order, packed (source start, trajectory, point index of the start, length),
+ * and their lengths for the scan into destinations (len[R] = 0 closes it) */
+__global__ void k_sorted_runs(int64_t R, const int32_t* __restrict__ order, const int32_t* __restrict__ starts,
+                              const int32_t* __restrict__ run_tid, const int32_t* __restrict__ run_len,
+                              const int64_t* __restrict__ off, int4* rec, int32_t* len) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j <= R; j += (int64_t)gridDim.x * blockDim.x) {
+        if (j == R) {
+            len[j] = 0;
+            continue;
         }
-#pragma unroll
-        for (int k = 0; k < kPerThread; k++) {
-            const int64_t b = s[k] >> kHintShift;
-            v[k] = xy[s[k]];
-            lo[k] = hint[b];
-            hi[k] = b + 1 < nhint ? hint[b + 1] : n;
+        const int r = order[j];
+        const int st = starts[r], t = run_tid[r], L = run_len[r];
+        rec[j] = make_int4(st, t, (int)(st - off[t]), L);
+        len[j] = L;
+    }
+}
+
+constexpr int kExpandTile = 2048;  /* output positions per block of k_expand_runs */
+constexpr int kExpandThreads = 256;
+
+/* first[b] = the last sorted run whose destination is <= b * kExpandTile */
+__global__ void k_tile_first(int64_t ntiles, int64_t R, const int32_t* __restrict__ dest, int32_t* first) {
+    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < ntiles; b += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t lo = b * kExpandTile;
+        int64_t a = 0, e = R - 1;
+        while (a < e) {
+            const int64_t mid = (a + e + 1) >> 1;
+            if (dest[mid] <= lo)
+                a = mid;
+            else
+                e = mid - 1;
         }
-        /* the binary searches of the kPerThread points advance in lockstep */
-        for (;;) {
-            bool open = false;
-#pragma unroll
-            for (int k = 0; k < kPerThread; k++) {
-                if (lo[k] < hi[k]) {
-                    const int mid = (lo[k] + hi[k] + 1) >> 1;
-                    if (off[mid] <= s[k])
-                        lo[k] = mid;
-                    else
-                        hi[k] = mid - 1;
-                    open = true;
-                }
-            }
-            if (!open) break;
+        first[b] = (int32_t)a;
+    }
+}
+
+/* 3. points to their index positions: block b fills the kExpandTile positions from b * kExpandTile.
+ * It stages the sorted runs covering them in shared memory; each thread finds its position's run
+ * by binary search there and writes x, y, trajectory and key = tid << pidx_bits | pidx (0 when
+ * the pair does not fit 32 bits; pidx_bits < 0, the point index then goes to pidx). */
+__global__ void __launch_bounds__(kExpandThreads) k_expand_runs(
+    int64_t P, int64_t R, int64_t ntiles, const int32_t* __restrict__ first, const int4* __restrict__ rec,
+    const int32_t* __restrict__ dest, const float2* __restrict__ xy, float* x, float* y, int32_t* tid, uint32_t* key,
+    int32_t* pidx, int pidx_bits) {
+    __shared__ int s_dest[kExpandTile + 1], s_src[kExpandTile + 1], s_tid[kExpandTile + 1], s_k0[kExpandTile + 1];
+    const int64_t b = blockIdx.x;
+    const int64_t lo = b * kExpandTile;
+    const int64_t hi = min(P, lo + kExpandTile);
+    const int a0 = first[b];
+    const int a1 = b + 1 < ntiles ? first[b + 1] : (int)(R - 1);
+    /* runs a0 .. a1 cover [lo, hi); each run holds at least one point, so there are at most
+     * kExpandTile + 1 of them */
+    const int m = a1 - a0 + 1;
+    for (int q = threadIdx.x; q < m; q += kExpandThreads) {
+        const int4 v = rec[a0 + q];
+        s_dest[q] = dest[a0 + q];
+        s_src[q] = v.x;
+        s_tid[q] = v.y;
+        s_k0[q] = v.z;
+    }
+    __syncthreads();
+    for (int64_t i = lo + threadIdx.x; i < hi; i += kExpandThreads) {
+        int a = 0, e = m - 1;
+        while (a < e) {
+            const int mid = (a + e + 1) >> 1;
+            if (s_dest[mid] <= i)
+                a = mid;
+            else
+                e = mid - 1;
         }
-#pragma unroll
-        for (int k = 0; k < kPerThread; k++) {
-            const int64_t i = i0 + k * stride;
-            if (i >= P) break;
-            const int t = lo[k];
-            const int q = (int)(s[k] - off[t]);
-            x[i] = v[k].x;
-            y[i] = v[k].y;
-            tid[i] = t;
-            key[i] = pidx_bits >= 0 ? ((uint32_t)t << pidx_bits) | (uint32_t)q : 0u;
-            if (pidx) pidx[i] = q;
+        const int d = (int)(i - s_dest[a]);
+        const float2 v = xy[s_src[a] + d];
+        const int t = s_tid[a], q = s_k0[a] + d;
+        x[i] = v.x;
+        y[i] = v.y;
+        tid[i] = t;
+        key[i] = pidx_bits >= 0 ? ((uint32_t)t << pidx_bits) | (uint32_t)q : 0u;
+        if (pidx) pidx[i] = q;
+    }
+}
+
+/* 4. cell boundaries from the sorted runs: cb[c] = destination of the first run whose cell is >= c */
+__global__ void k_cell_bounds(int64_t R, int64_t ncells, const uint32_t* __restrict__ run_cell_s,
+                              const int32_t* __restrict__ dest, int64_t* cb) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c <= ncells; c += (int64_t)gridDim.x * blockDim.x) {
+        int64_t lo = 0, hi = R;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if ((int64_t)run_cell_s[mid] < c)
+                lo = mid + 1;
+            else
+                hi = mid;
         }
+        cb[c] = dest[lo];
     }
 }
 
@@ -284,27 +361,23 @@ __global__ void k_tree_nodes(int64_t N, LevelTable lt, const int32_t* __restrict
 }
 
 /* ---------------------------------------------------------------- 6. frequency vectors */
-/* run heads of equal virtual cells: 1 where a point's virtual cell differs from its
- * predecessor's (trajectory starts are marked by k_fv_starts) */
-__global__ void k_fv_heads(int64_t P, const uint32_t* __restrict__ cells, int vparam, uint8_t* head) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P; i += (int64_t)gridDim.x * blockDim.x)
-        head[i] = (i == 0 || (cells[i] >> vparam) != (cells[i - 1] >> vparam)) ? 1 : 0;
+/* heads of runs of equal virtual cells: a cell run whose trajectory or virtual cell differs from
+ * the previous run's */
+__global__ void k_vrun_heads(int64_t R, const uint32_t* __restrict__ run_cell, const int32_t* __restrict__ run_tid,
+                             int vparam, uint8_t* vhead) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x)
+        vhead[r] = (r == 0 || run_tid[r] != run_tid[r - 1] || (run_cell[r] >> vparam) != (run_cell[r - 1] >> vparam)) ? 1 : 0;
 }
 
-__global__ void k_fv_starts(int n, const int64_t* __restrict__ off, uint8_t* head) {
-    for (int t = 1 + blockIdx.x * blockDim.x + threadIdx.x; t <= n; t += gridDim.x * blockDim.x)
-        if (off[t + 1] > off[t]) head[off[t]] = 1;
-}
-
-/* per run: key (trajectory << 32 | virtual cell) and point count */
-__global__ void k_fv_runs(int64_t R, int64_t P, int n, const int32_t* __restrict__ starts, const int64_t* __restrict__ off,
-                          const int32_t* __restrict__ hint, int64_t nhint, const uint32_t* __restrict__ cells, int vparam,
-                          unsigned long long* key, int32_t* cnt) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t s = starts[r], e = r + 1 < R ? starts[r + 1] : P;
-        const int t = holder(s, n, off, hint, nhint);
-        key[r] = ((unsigned long long)(unsigned)t << 32) | (unsigned)(cells[s] >> vparam);
-        cnt[r] = (int32_t)(e - s);
+/* per virtual-cell run: key (trajectory << 32 | virtual cell) and point count */
+__global__ void k_vruns(int64_t Rv, int64_t R, int64_t P, const int32_t* __restrict__ vstarts,
+                        const int32_t* __restrict__ starts, const uint32_t* __restrict__ run_cell,
+                        const int32_t* __restrict__ run_tid, int vparam, unsigned long long* key, int32_t* cnt) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < Rv; v += (int64_t)gridDim.x * blockDim.x) {
+        const int a = vstarts[v];
+        const int64_t b = v + 1 < Rv ? vstarts[v + 1] : R;
+        key[v] = ((unsigned long long)(unsigned)run_tid[a] << 32) | (run_cell[a] >> vparam);
+        cnt[v] = (int32_t)((b < R ? (int64_t)starts[b] : P) - starts[a]);
     }
 }
 
@@ -403,13 +476,13 @@ T* alloc_padded(gat_index* ix, int64_t count, int* st) {
 }
 
 /* Steps 1-4: the points in index order (x, y, tid, key allocated first, as the host builder
- * uploads them), the cells in trajectory order and the boundaries d_cb[0..ncells]. */
+ * uploads them), the cell boundaries d_cb[0..ncells] and, for the Grid, the runs' vector keys. */
 struct Placement {
-    uint32_t* cells = nullptr; /* trajectory order */
-    int32_t* pos = nullptr;    /* 0, 1, 2, ... (the sort's values) */
-    int32_t* hint = nullptr;   /* trajectory of every 256th point */
-    int64_t nhint = 0;
     int64_t* d_cb = nullptr;
+    int64_t R = 0;               /* runs of equal cells, in trajectory order: */
+    int32_t* starts = nullptr;   /*   first point */
+    uint32_t* run_cell = nullptr; /*   cell */
+    int32_t* run_tid = nullptr;  /*   trajectory */
 };
 
 int place(gat_index* ix, const DevicePlaceArgs& a, Temps& tmp, Placement& out) {
@@ -421,37 +494,40 @@ int place(gat_index* ix, const DevicePlaceArgs& a, Temps& tmp, Placement& out) {
     if (P >= ((int64_t)1 << 31) - 1) return fail(ctx, GAT_ERR_ARG, std::string(a.what) + ": more than 2^31 - 2 points");
     const int64_t nhint = (P + (1 << kHintShift) - 1) >> kHintShift; /* blocks holding points */
     uint32_t* cells = tmp.get<uint32_t>(P);
-    uint32_t* cells_s = tmp.get<uint32_t>(P);
-    int32_t* pos = tmp.get<int32_t>(P);
-    int32_t* order = tmp.get<int32_t>(P);
+    uint8_t* head = tmp.get<uint8_t>(P);
+    int32_t* starts = tmp.get<int32_t>(P);
+    int32_t* nsel = tmp.get<int32_t>(1);
     int32_t* hint = tmp.get<int32_t>(nhint);
     int64_t* d_cb = tmp.get<int64_t>((size_t)a.ncells + 1);
     if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
     CellParams cp{a.rxmin, a.rymax, a.cell, a.morton ? 1 : 0, a.axis, a.nx, a.ny, a.vparam};
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int32_t), s), "index build");
+    int32_t R = 0;
     if (P > 0) {
+        /* 1. cells and run heads */
         k_hints<<<grid_size(ctx, n), 256, 0, s>>>(n, db->d_off, hint);
         count_launch(ctx);
         timed_begin(ctx, GAT_KERNEL_INDEX_BUILD);
-        k_point_cells<<<grid_size(ctx, (P + kPerThread - 1) / kPerThread), 256, 0, s>>>(P, db->d_xy, cp, cells, pos,
-                                                                                       ctx->d_flag);
-        timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * 16);
-        count_launch(ctx);
-    }
-    GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (cells)");
-    if (check_device_flag(ctx, "index build") != GAT_OK)
-        return fail(ctx, GAT_ERR_ARG, std::string(a.what) + ": a point lies outside the grid range");
-    /* 2. stable sort of (cell, position) */
-    const int end_bit = bits_to_hold(a.ncells);
-    size_t tbytes = 0;
-    GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tbytes, cells, cells_s, pos, order, (int)P, 0, end_bit, s),
-                 "index build sort");
-    void* tstore = tmp.get<char>(tbytes);
-    if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-    if (P > 0) {
-        GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(tstore, tbytes, cells, cells_s, pos, order, (int)P, 0, end_bit, s),
-                     "index build sort");
-        count_launch(ctx, 2 * ((end_bit + 7) / 8) + 1);
+        k_point_cells<<<grid_size(ctx, (P + kPerThread - 1) / kPerThread), 256, 0, s>>>(P, db->d_xy, cp, cells, head,
+                                                                                   ctx->d_flag);
+        timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * 13);
+        k_run_starts<<<grid_size(ctx, n), 256, 0, s>>>(n, db->d_off, head);
+        count_launch(ctx, 2);
+        GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (cells)");
+        if (check_device_flag(ctx, "index build") != GAT_OK)
+            return fail(ctx, GAT_ERR_ARG, std::string(a.what) + ": a point lies outside the grid range");
+        /* run starts, in position order */
+        size_t need = 0;
+        thrust::counting_iterator<int> iota(0);
+        GAT_CUDA_TRY(ctx, cub::DeviceSelect::Flagged(nullptr, need, iota, head, starts, nsel, (int)P, s), "index build runs");
+        void* t0 = tmp.get<char>(need);
+        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+        GAT_CUDA_TRY(ctx, cub::DeviceSelect::Flagged(t0, need, iota, head, starts, nsel, (int)P, s), "index build runs");
+        count_launch(ctx, 2);
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R, nsel, 4, cudaMemcpyDeviceToHost, s), "index build runs");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build runs");
+        tmp.release(t0);
+        tmp.release(head);
     }
     /* 3. index-order arrays */
     const int tid_bits = bits_to_hold(n);
@@ -470,23 +546,58 @@ int place(gat_index* ix, const DevicePlaceArgs& a, Temps& tmp, Placement& out) {
     ix->d_tid = dt;
     ix->d_key = dk;
     if (pidx_bits < 0) GAT_CUDA_TRY(ctx, cudaMalloc(&ix->d_pidx, std::max<size_t>((size_t)P, 1) * 4), "index build");
-    if (P > 0) {
-        timed_begin(ctx, GAT_KERNEL_INDEX_BUILD);
-        k_gather_points<<<grid_size(ctx, (P + kPerThread - 1) / kPerThread), 256, 0, s>>>(
-            P, n, order, db->d_off, hint, nhint, db->d_xy, dx, dy, dt, dk, ix->d_pidx, pidx_bits);
-        timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * (28 + (pidx_bits < 0 ? 4 : 0)));
-        count_launch(ctx);
+    out.R = R;
+    if (R == 0) {
+        GAT_CUDA_TRY(ctx, cudaMemsetAsync(d_cb, 0, ((size_t)a.ncells + 1) * 8, s), "index build");
+        out.d_cb = d_cb;
+        ix->host_pending = true;
+        return GAT_OK;
     }
-    /* 4. cell boundaries */
-    k_bounds<uint32_t><<<grid_size(ctx, a.ncells + 1), 256, 0, s>>>(P, a.ncells, cells_s, 0, d_cb);
+    /* 2. the runs, stably sorted by cell */
+    uint32_t* run_cell = tmp.get<uint32_t>(R);
+    uint32_t* run_cell_s = tmp.get<uint32_t>(R);
+    int32_t* run_idx = tmp.get<int32_t>(R);
+    int32_t* order = tmp.get<int32_t>(R);
+    int32_t* run_tid = tmp.get<int32_t>(R);
+    int32_t* run_len = tmp.get<int32_t>(R);
+    int32_t* len_s = tmp.get<int32_t>(R + 1);
+    int32_t* dest = tmp.get<int32_t>(R + 1);
+    int4* rec = tmp.get<int4>(R);
+    const int64_t ntiles = (P + kExpandTile - 1) / kExpandTile;
+    int32_t* tfirst = tmp.get<int32_t>(ntiles);
+    if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+    k_runs<<<grid_size(ctx, R), 256, 0, s>>>(R, P, n, starts, db->d_off, hint, nhint, cells, run_cell, run_idx, run_tid,
+                                             run_len);
     count_launch(ctx);
-    GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (gather)");
+    const int end_bit = bits_to_hold(a.ncells);
+    size_t b1 = 0, b2 = 0;
+    GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(nullptr, b1, run_cell, run_cell_s, run_idx, order, R, 0, end_bit, s),
+                 "index build sort");
+    GAT_CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(nullptr, b2, len_s, dest, R + 1, s), "index build scan");
+    void* t1 = tmp.get<char>(std::max(b1, b2));
+    if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+    GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(t1, b1, run_cell, run_cell_s, run_idx, order, R, 0, end_bit, s),
+                 "index build sort");
+    k_sorted_runs<<<grid_size(ctx, R + 1), 256, 0, s>>>(R, order, starts, run_tid, run_len, db->d_off, rec, len_s);
+    GAT_CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(t1, b2, len_s, dest, R + 1, s), "index build scan");
+    count_launch(ctx, 2 * ((end_bit + 7) / 8) + 4);
+    /* 3. points to their index positions */
+    timed_begin(ctx, GAT_KERNEL_INDEX_BUILD);
+    k_tile_first<<<grid_size(ctx, ntiles), 256, 0, s>>>(ntiles, R, dest, tfirst);
+    count_launch(ctx);
+    k_expand_runs<<<(unsigned)ntiles, kExpandThreads, 0, s>>>(P, R, ntiles, tfirst, rec, dest, db->d_xy, dx, dy, dt, dk,
+                                                              ix->d_pidx, pidx_bits);
+    timed_end(ctx, GAT_KERNEL_INDEX_BUILD, (double)P * (24 + (pidx_bits < 0 ? 4 : 0)) + (double)R * 20);
+    count_launch(ctx);
+    /* 4. cell boundaries */
+    k_cell_bounds<<<grid_size(ctx, a.ncells + 1), 256, 0, s>>>(R, a.ncells, run_cell_s, dest, d_cb);
+    count_launch(ctx);
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "index build (placement)");
     ix->host_pending = true;
-    out.cells = cells;
-    out.pos = pos;
-    out.hint = hint;
-    out.nhint = nhint;
     out.d_cb = d_cb;
+    out.starts = starts;
+    out.run_cell = run_cell;
+    out.run_tid = run_tid;
     return GAT_OK;
 }
 
@@ -582,59 +693,59 @@ int build_tree(gat_index* ix, const Placement& pl, const TreeParams& tp, Temps& 
 }
 
 /* Step 6: the frequency-vector CSR (fv_off [n+2], fv_cell, fv_cnt), allocated after the nodes:
- * runs of equal virtual cells keyed (trajectory, virtual cell), sorted, and counts summed per key. */
+ * cell runs merged into runs of equal virtual cells, keyed (trajectory, virtual cell), sorted, and
+ * their point counts summed per key. */
 int build_vectors(gat_index* ix, const Placement& pl, int vparam, Temps& tmp) {
     gat_ctx* ctx = ix->ctx;
     cudaStream_t s = ctx->stream;
-    const gat_db* db = ix->db;
-    const int n = db->n;
-    const int64_t P = db->npoints;
+    const int n = ix->db->n;
+    const int64_t P = ix->db->npoints;
+    const int64_t R = pl.R;
     int st = GAT_OK;
     int64_t* off = alloc_padded<int64_t>(ix, n + 2, &st);
     if (!off) return st;
     ix->d_fv_off = off;
-    uint8_t* head = tmp.get<uint8_t>(P);
-    int32_t* starts = tmp.get<int32_t>(P);
-    int32_t* nsel = tmp.get<int32_t>(1);
-    if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-    int32_t R = 0;
-    if (P > 0) {
-        k_fv_heads<<<grid_size(ctx, P), 256, 0, s>>>(P, pl.cells, vparam, head);
-        k_fv_starts<<<grid_size(ctx, n), 256, 0, s>>>(n, db->d_off, head);
-        count_launch(ctx, 2);
-        size_t need = 0;
-        GAT_CUDA_TRY(ctx, cub::DeviceSelect::Flagged(nullptr, need, pl.pos, head, starts, nsel, (int)P, s), "index build fv");
-        void* t1 = tmp.get<char>(need);
-        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-        GAT_CUDA_TRY(ctx, cub::DeviceSelect::Flagged(t1, need, pl.pos, head, starts, nsel, (int)P, s), "index build fv");
-        count_launch(ctx, 2);
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&R, nsel, 4, cudaMemcpyDeviceToHost, s), "index build fv");
-        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
-    }
     int32_t E = 0;
     unsigned long long* uk = nullptr;
     int32_t* sums = nullptr;
     if (R > 0) {
-        unsigned long long* key = tmp.get<unsigned long long>(R);
-        unsigned long long* key_s = tmp.get<unsigned long long>(R);
-        int32_t* cnt = tmp.get<int32_t>(R);
-        int32_t* cnt_s = tmp.get<int32_t>(R);
-        uk = tmp.get<unsigned long long>(R);
-        sums = tmp.get<int32_t>(R);
+        uint8_t* vhead = tmp.get<uint8_t>(R);
+        int32_t* vstarts = tmp.get<int32_t>(R);
+        int32_t* nsel = tmp.get<int32_t>(1);
+        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+        k_vrun_heads<<<grid_size(ctx, R), 256, 0, s>>>(R, pl.run_cell, pl.run_tid, vparam, vhead);
+        count_launch(ctx);
+        size_t need = 0;
+        thrust::counting_iterator<int> iota(0);
+        GAT_CUDA_TRY(ctx, cub::DeviceSelect::Flagged(nullptr, need, iota, vhead, vstarts, nsel, (int)R, s), "index build fv");
+        void* t0 = tmp.get<char>(need);
+        if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
+        GAT_CUDA_TRY(ctx, cub::DeviceSelect::Flagged(t0, need, iota, vhead, vstarts, nsel, (int)R, s), "index build fv");
+        count_launch(ctx, 2);
+        int32_t Rv = 0;
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&Rv, nsel, 4, cudaMemcpyDeviceToHost, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "index build fv");
+        unsigned long long* key = tmp.get<unsigned long long>(Rv);
+        int32_t* cnt = tmp.get<int32_t>(Rv);
+        unsigned long long* key_s = tmp.get<unsigned long long>(Rv);
+        int32_t* cnt_s = tmp.get<int32_t>(Rv);
+        uk = tmp.get<unsigned long long>(Rv);
+        sums = tmp.get<int32_t>(Rv);
         int32_t* nuniq = tmp.get<int32_t>(1);
         if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-        k_fv_runs<<<grid_size(ctx, R), 256, 0, s>>>(R, P, n, starts, db->d_off, pl.hint, pl.nhint, pl.cells, vparam, key, cnt);
+        k_vruns<<<grid_size(ctx, Rv), 256, 0, s>>>(Rv, R, P, vstarts, pl.starts, pl.run_cell, pl.run_tid, vparam, key, cnt);
         count_launch(ctx);
         /* keys hold the trajectory above bit 32 and the virtual cell below it */
         const int kbits = 32 + bits_to_hold(n);
         size_t b1 = 0, b2 = 0;
-        GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(nullptr, b1, key, key_s, cnt, cnt_s, R, 0, kbits, s), "index build fv");
-        GAT_CUDA_TRY(ctx, cub::DeviceReduce::ReduceByKey(nullptr, b2, key_s, uk, cnt_s, sums, nuniq, AddInt(), R, s),
+        GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(nullptr, b1, key, key_s, cnt, cnt_s, Rv, 0, kbits, s),
+                     "index build fv");
+        GAT_CUDA_TRY(ctx, cub::DeviceReduce::ReduceByKey(nullptr, b2, key_s, uk, cnt_s, sums, nuniq, AddInt(), Rv, s),
                      "index build fv");
         void* t2 = tmp.get<char>(std::max(b1, b2));
         if (tmp.err != cudaSuccess) return cuda_fail(ctx, tmp.err, "index build (device temporaries)");
-        GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(t2, b1, key, key_s, cnt, cnt_s, R, 0, kbits, s), "index build fv");
-        GAT_CUDA_TRY(ctx, cub::DeviceReduce::ReduceByKey(t2, b2, key_s, uk, cnt_s, sums, nuniq, AddInt(), R, s),
+        GAT_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(t2, b1, key, key_s, cnt, cnt_s, Rv, 0, kbits, s), "index build fv");
+        GAT_CUDA_TRY(ctx, cub::DeviceReduce::ReduceByKey(t2, b2, key_s, uk, cnt_s, sums, nuniq, AddInt(), Rv, s),
                      "index build fv");
         count_launch(ctx, 2 * ((kbits + 7) / 8) + 3);
         GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&E, nuniq, 4, cudaMemcpyDeviceToHost, s), "index build fv");
