@@ -204,14 +204,20 @@ __global__ void k_tile_first(int64_t ntiles, int64_t R, const int32_t* __restric
 }
 
 /* 3. points to their index positions: block b fills the kExpandTile positions from b * kExpandTile.
- * It stages the sorted runs covering them in shared memory; each thread finds its position's run
- * by binary search there and writes x, y, trajectory and key = tid << pidx_bits | pidx (0 when
- * the pair does not fit 32 bits; pidx_bits < 0, the point index then goes to pidx). */
+ * It stages the sorted runs covering them in shared memory, marks each run's first position
+ * with its index and fills the tile with a block-wide max-scan, so each position reads its run
+ * directly; then writes x, y, trajectory and key = tid << pidx_bits | pidx (0 when the pair does
+ * not fit 32 bits; pidx_bits < 0, the point index then goes to pidx). */
 __global__ void __launch_bounds__(kExpandThreads) k_expand_runs(
     int64_t P, int64_t R, int64_t ntiles, const int32_t* __restrict__ first, const int4* __restrict__ rec,
     const int32_t* __restrict__ dest, const float2* __restrict__ xy, float* x, float* y, int32_t* tid, uint32_t* key,
     int32_t* pidx, int pidx_bits) {
+    constexpr int kPer = kExpandTile / kExpandThreads;
+    constexpr int kWarps = kExpandThreads / 32;
     __shared__ int s_dest[kExpandTile + 1], s_src[kExpandTile + 1], s_tid[kExpandTile + 1], s_k0[kExpandTile + 1];
+    __shared__ int s_run[kExpandTile];
+    __shared__ int s_warp[kWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t b = blockIdx.x;
     const int64_t lo = b * kExpandTile;
     const int64_t hi = min(P, lo + kExpandTile);
@@ -220,23 +226,45 @@ __global__ void __launch_bounds__(kExpandThreads) k_expand_runs(
     /* runs a0 .. a1 cover [lo, hi); each run holds at least one point, so there are at most
      * kExpandTile + 1 of them */
     const int m = a1 - a0 + 1;
+    for (int k = threadIdx.x; k < kExpandTile; k += kExpandThreads) s_run[k] = 0;
+    __syncthreads();
     for (int q = threadIdx.x; q < m; q += kExpandThreads) {
         const int4 v = rec[a0 + q];
-        s_dest[q] = dest[a0 + q];
+        const int d = dest[a0 + q];
+        s_dest[q] = d;
         s_src[q] = v.x;
         s_tid[q] = v.y;
         s_k0[q] = v.z;
+        /* run 0 starts at or before lo and covers position 0 */
+        if (q > 0 && d - lo < kExpandTile) s_run[d - lo] = q;
     }
     __syncthreads();
+    /* inclusive max-scan of s_run: each thread its kPer consecutive entries, then across threads */
+    int loc[kPer];
+    int run = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        run = max(run, s_run[threadIdx.x * kPer + k]);
+        loc[k] = run;
+    }
+    int incl = run;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl = max(incl, o);
+    }
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    int carry = 0;
+    for (int k = 0; k < w; k++) carry = max(carry, s_warp[k]);
+    int excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = 0;
+    carry = max(carry, excl);
+#pragma unroll
+    for (int k = 0; k < kPer; k++) s_run[threadIdx.x * kPer + k] = max(loc[k], carry);
+    __syncthreads();
     for (int64_t i = lo + threadIdx.x; i < hi; i += kExpandThreads) {
-        int a = 0, e = m - 1;
-        while (a < e) {
-            const int mid = (a + e + 1) >> 1;
-            if (s_dest[mid] <= i)
-                a = mid;
-            else
-                e = mid - 1;
-        }
+        const int a = s_run[i - lo];
         const int d = (int)(i - s_dest[a]);
         const float2 v = xy[s_src[a] + d];
         const int t = s_tid[a], q = s_k0[a] + d;
