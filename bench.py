@@ -1074,7 +1074,9 @@ def run_c5(args, world, rank, local, td):
 BUILD = dict(cell=0.001, vparam=2, leaf_cap=512, ref_n=40_000)
 
 
-BUILD_TRAFFIC_RATIO = None  # dram read+write / algorithmic bytes of the placement kernels (set from an ncu capture)
+# dram read+write / algorithmic bytes of k_point_cells + k_expand_runs: (228.1 + 501.3) MB / 804.0 MB in an
+# ncu capture of one Grid build over 100k walks (20M points, every array above L2)
+BUILD_TRAFFIC_RATIO = 0.907
 
 
 def build_roofline(st):
@@ -1088,7 +1090,9 @@ def build_roofline(st):
             "traffic": round(BUILD_TRAFFIC_RATIO * per) if BUILD_TRAFFIC_RATIO else None, "work_per_launch": per,
             "note": "achieved = algorithmic bytes of both placement kernels / their summed event time; k_point_cells "
                     "13 B per point (x, y read; cell and run flag written), k_expand_runs 24 B per point (x, y read; "
-                    f"x, y, trajectory, key written) + 20 B per run (packed run, destination); peak of {src}"}
+                    f"x, y, trajectory, key written) + 20 B per run (packed run, destination); peak of {src}; "
+                    f"traffic = {BUILD_TRAFFIC_RATIO} x algorithmic, the dram read+write / algorithmic ratio of an ncu "
+                    "capture of both kernels on a 100k-walk set (20M points)"}
 
 
 def build_reference_sample():
