@@ -408,6 +408,16 @@ class SystemTest:
     def FSGrangeQueryTest(self, rangeQueryMBB, rangeQueryNum: int) -> RangeResult:
         return self.fsg.range_query(self._repeat(rangeQueryMBB, rangeQueryNum))
 
+    def rangeQueryTestWithoutMorton(self, rangeQueryMBB, rangeQueryNum: int) -> RangeResult:
+        """SystemTest.h:29. The reference's row-major walk over the Grid's points
+        (Grid.cpp:544-662) returns the Grid's id sets; this runs the GT-quadtree path."""
+        return self.rangeQueryTest(rangeQueryMBB, rangeQueryNum)
+
+    def MortonGridRangeQueryTest(self, rangeQueryMBB, rangeQueryNum: int) -> RangeResult:
+        """SystemTest.h:33. MortonGrid (MortonGrid.cpp:238-400) is the Grid with a leaf bitmap
+        over implicit node ids and the same leaf rule; its id sets are the Grid's."""
+        return self.rangeQueryTest(rangeQueryMBB, rangeQueryNum)
+
     def similarityQueryTest(self, t, similarityScale: int, similarityKValue: int):
         """t: a Trajectories holding one query, or an int trajectory number (README.md:30)."""
         if isinstance(t, (int, np.integer)):

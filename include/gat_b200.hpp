@@ -276,6 +276,14 @@ public:
     int rangeQueryTest(MBB mbb, int num) { return repeat_range(g, "", mbb, num); }
     int STIGrangeQueryTest(MBB mbb, int num) { return repeat_range(stig, " STIG", mbb, num); }
     int FSGrangeQueryTest(MBB mbb, int num) { return repeat_range(fsg, " FSG", mbb, num); }
+    /* SystemTest.h:29 and :33. The reference's two ablations of the GT-quadtree change only how
+     * its points and tree are laid out: rangeQueryBatchGPUWithoutMorton (Grid.cpp:544-662) walks
+     * the Morton-ordered points through per-block segment lists as if they were row-major, and
+     * MortonGrid (MortonGrid.cpp:238-400) replaces the node pointers with a leaf bitmap over
+     * implicit node ids, under the same leaf rule. Both return the Grid's trajectory-id sets, so
+     * here both run the GT-quadtree path. */
+    int rangeQueryTestWithoutMorton(MBB mbb, int num) { return repeat_range(g, " (without Morton)", mbb, num); }
+    int MortonGridRangeQueryTest(MBB mbb, int num) { return repeat_range(g, " Morton Grid", mbb, num); }
 
     /* SystemTest.h:30: similarityScale copies of t against the grid's set */
     int similarityQueryTest(const Trajectory& t, int scale, int k) {

@@ -78,6 +78,12 @@ int main(int argc, char** argv) {
         rc = st.FSGrangeQueryTest(q, 2);
         printf("FSGrangeQueryTest %d\n", rc);
         if (rc == GAT_OK) emit("fsg_off", st.lastRange.offsets), emit("fsg_ids", st.lastRange.tids);
+        rc = st.rangeQueryTestWithoutMorton(q, 2);
+        printf("rangeQueryTestWithoutMorton %d\n", rc);
+        if (rc == GAT_OK) emit("nonmorton_ids", st.lastRange.tids);
+        rc = st.MortonGridRangeQueryTest(q, 2);
+        printf("MortonGridRangeQueryTest %d\n", rc);
+        if (rc == GAT_OK) emit("mortongrid_ids", st.lastRange.tids);
         // batch form with point results
         std::vector<float> b4(4 * 16);
         if (gat_gen_boxes(16, GAT_SIDE_LOGUNIFORM, 0.002, 0.05, box, 5, b4.data()) != GAT_OK) return 2;

@@ -29,7 +29,8 @@ def run(exe, device, n=2000, path=None):
     for line in r.stdout.splitlines():
         f = line.split()
         if len(f) >= 2 and f[0] in ("build", "rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest",
-                                    "rangeQueryBatch", "similarityQueryTest", "file_roundtrip"):
+                                    "rangeQueryTestWithoutMorton", "MortonGridRangeQueryTest", "rangeQueryBatch",
+                                    "similarityQueryTest", "file_roundtrip"):
             out[f[0]] = int(f[1])
         elif len(f) >= 2:
             out[f[0]] = np.array([int(x) for x in f[2:]], np.int64)
@@ -43,7 +44,8 @@ def test_host_only(demo, tmp_path):
     rc, out, log = run(demo, -1, path=str(tmp_path / "tradb.txt"))
     assert rc == 0, log
     assert out["build"] == 0 and out["file_roundtrip"] == 1
-    for k in ("rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest", "rangeQueryBatch", "similarityQueryTest"):
+    for k in ("rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest", "rangeQueryTestWithoutMorton",
+              "MortonGridRangeQueryTest", "rangeQueryBatch", "similarityQueryTest"):
         assert out[k] == L.GAT_ERR_STATE, (k, log)
 
 
@@ -61,6 +63,7 @@ def test_systemtest_matches_oracle(demo):
     assert np.array_equal(out["stig_ids"], np.tile(sids, 2)) and out["stig_off"][1] == soff[1]
     foff, fids = po.OracleFSG(t, D.BOX, 0.01).range(q)
     assert np.array_equal(out["fsg_ids"], np.tile(fids, 2)) and out["fsg_off"][1] == foff[1]
+    assert np.array_equal(out["nonmorton_ids"], np.tile(ids, 2)) and np.array_equal(out["mortongrid_ids"], np.tile(ids, 2))
     qs = D.boxes(16, 1, 0.002, 0.05, 5)
     poff, ptid, ppidx = po.OracleGrid(t, D.BOX, 0.01, 2, 512).range(qs, 1)
     assert np.array_equal(out["pts_off"], poff) and np.array_equal(out["pts_tid"], ptid)
