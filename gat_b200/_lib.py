@@ -80,6 +80,8 @@ SIGNATURES = [
     ("gat_fv_lower_bounds", c_int, [c_p, c_p, c_int, P_i32, P_f32, P_f32, P_i32]),
     ("gat_topk", c_int, [c_p, c_p, c_int, P_i32, P_f32, P_f32, c_int, c_d, c_int, P_i32, P_i32, P_i64]),
     ("gat_topk_dev", c_int, [c_p, c_p, c_int, c_p, c_p, c_p, c_int, c_int, c_d, c_int, c_p, c_p, P_i64]),
+    ("gat_topk_merge", c_int, [c_int, c_int, c_int, P_i32, P_i32, P_i32, P_i32]),
+    ("gat_topk_merge_dev", c_int, [c_p, c_int, c_int, c_int, c_p, c_p, c_p, c_p]),
     ("gat_server_create", c_int, [c_p, c_p, c_p, c_p, C.POINTER(ServerConfig), C.POINTER(c_p)]),
     ("gat_server_destroy", None, [c_p]),
     ("gat_server_submit_range", c_int, [c_p, c_int, MBB, c_int, P_i64]),

@@ -213,6 +213,20 @@ int gat_topk_dev(gat_ctx* ctx, const gat_index* grid, int nq, const int32_t* d_q
                  const int64_t* d_q_off, const float* d_q_xy, int max_q_len, int k, double eps,
                  int exec, int32_t* d_ids, int32_t* d_dist, int64_t* stats);
 
+/* ---------------------------------------------------------------- sharded sets (no counterpart in the reference,
+ * whose two-GPU mode splits the queries, Grid.cpp:1758-2332) */
+/* A trajectory set split across GPUs by contiguous id ranges answers top-k as the merge of each
+ * shard's gat_topk (ids made global by adding the shard's first id - 1): the k smallest
+ * (distance, id) of the union, equal to the unsharded result. Inputs are [nparts][nq][k], each
+ * list sorted by (distance, id); id -1 marks padding (a shard with fewer than k trajectories)
+ * and is emitted as (-1, -1). nparts x k must not exceed 8192. gat_topk_merge runs on host
+ * buffers; gat_topk_merge_dev on device buffers (for example after an all-gather), on the
+ * context's stream. */
+int gat_topk_merge(int nq, int k, int nparts, const int32_t* ids, const int32_t* dist, int32_t* out_ids,
+                   int32_t* out_dist);
+int gat_topk_merge_dev(gat_ctx* ctx, int nq, int k, int nparts, const int32_t* d_ids, const int32_t* d_dist,
+                       int32_t* d_out_ids, int32_t* d_out_dist);
+
 /* ---------------------------------------------------------------- serving (no counterpart in the reference) */
 /* A request loop over device-resident indexes with continuous batching: requests are submitted
  * one at a time from any thread; a scheduler thread forms a batch whenever one of `lanes`
