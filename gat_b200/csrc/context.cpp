@@ -308,6 +308,11 @@ int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
         ctx->index_build = value;
         return GAT_OK;
     }
+    if (knob == GAT_TUNE_DEP_LAUNCH) {
+        if (value < 0 || value > 1) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: dependent launch must be 0 or 1");
+        ctx->dep_launch = value;
+        return GAT_OK;
+    }
     if (knob != GAT_TUNE_EDR_ROWS) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: unknown knob");
     if (value != 0 && value != 2 && value != 4 && value != 8)
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR rows per lane must be 0 (autotune), 2, 4 or 8");
@@ -334,6 +339,8 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
         *value = ctx->topk_growth;
     else if (knob == GAT_TUNE_INDEX_BUILD)
         *value = ctx->index_build;
+    else if (knob == GAT_TUNE_DEP_LAUNCH)
+        *value = ctx->dep_launch;
     else
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_get_tuning: unknown knob");
     return GAT_OK;

@@ -24,6 +24,7 @@
 #include <algorithm>
 
 #include "internal.h"
+#include "launch.cuh"
 
 namespace gat {
 namespace edr {
@@ -257,6 +258,7 @@ __device__ __forceinline__ int duration_class(long long d) {
 
 template <int R, bool COL, class Src>
 __global__ void k_sched_count(Src src, int cap, int coop_cap, int* __restrict__ ctr, int2* __restrict__ meta) {
+    dep_wait();
     __shared__ int hist[kClasses];
     for (int i = threadIdx.x; i < kClasses; i += blockDim.x) hist[i] = 0;
     __syncthreads();
@@ -290,6 +292,7 @@ __global__ void k_sched_count(Src src, int cap, int coop_cap, int* __restrict__ 
 template <class Src>
 __global__ void k_sched_write(Src src, int cap, int* __restrict__ ctr, const int2* __restrict__ meta,
                               int4* __restrict__ items, unsigned long long* __restrict__ epochs) {
+    dep_wait();
     __shared__ int off[kClasses];
     __shared__ int lcnt[kClasses];
     __shared__ int lbase[kClasses];
@@ -528,6 +531,7 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
 template <int R, bool COL, class Src>
 __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(Src src, float u, TileCtl ctl, unsigned* __restrict__ work,
                                                            unsigned long long* __restrict__ cells) {
+    dep_wait();
     __shared__ float2 bring[kTileWarps][64];
     __shared__ int cring[kTileWarps][32];
     const unsigned FULL = 0xffffffffu;
@@ -632,17 +636,17 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
         coop > 0 ? (carry_t*)scratch_zeroed(ctx, S_EDR_PCARRY, (size_t)coop * 2 * stride * sizeof(carry_t), &st) : nullptr;
     carry_t* wcarry = (carry_t*)scratch_zeroed(ctx, S_EDR_CARRY, (size_t)grid * kTileWarps * 2 * stride * sizeof(carry_t), &st);
     if (!ctr || !meta || !items || !wcarry || (coop > 0 && !pcarry)) return st;
-    GAT_CUDA_TRY(ctx, cudaMemsetAsync(ctr, 0, kCtrWords * sizeof(int), s), "edr");
+    (void)launch_dep(ctx, k_zero_words, dim3(1), dim3(256), 0, s, ctr, (int)kCtrWords);
     const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->sm_count * 8));
-    k_sched_count<R, COL, Src><<<pgrid, 256, 0, s>>>(src, (int)cap, (int)coop, ctr, meta);
+    (void)launch_dep(ctx, k_sched_count<R, COL, Src>, dim3(pgrid), dim3(256), 0, s, src, (int)cap, (int)coop, ctr, meta);
     count_launch(ctx);
-    k_sched_write<Src><<<pgrid, 256, 0, s>>>(src, (int)cap, ctr, meta, items, edr_epochs(ctx));
+    (void)launch_dep(ctx, k_sched_write<Src>, dim3(pgrid), dim3(256), 0, s, src, (int)cap, ctr, meta, items, edr_epochs(ctx));
     count_launch(ctx);
     TileCtl ctl{items, ctr + 2, pcarry, wcarry, stride, reinterpret_cast<const unsigned long long*>(ctr + kCtrEpoch),
                 ctx->d_flag};
     timed_begin(ctx, GAT_KERNEL_EDR);
     if (ev0) cudaEventRecord(ev0, s);
-    k_edr_tiles<R, COL, Src><<<grid, kTileWarps * 32, 0, s>>>(src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
+    (void)launch_dep(ctx, k_edr_tiles<R, COL, Src>, dim3(grid), dim3(kTileWarps * 32), 0, s, src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
     if (ev1) cudaEventRecord(ev1, s);
     timed_end(ctx, GAT_KERNEL_EDR, 0.0);
     count_launch(ctx);

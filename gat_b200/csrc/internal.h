@@ -98,6 +98,7 @@ struct gat_ctx {
     int edr_form = 0; /* 0 = autotune, 1 = row tiles, 2 = column tiles */
     int topk_chunk = 0, topk_growth = 0; /* 0 = defaults */
     int index_build = 0;                 /* 0 = device when present, 1 = host, 2 = device */
+    int dep_launch = 1;                  /* programmatic dependent launch on the query path */
     cudaMemPool_t build_pool = nullptr;  /* index-build temporaries, kept for reuse until gat_ctx_trim */
     std::map<uint64_t, int> edr_tune; /* worker contexts use their root's table */
     std::mutex tune_mu;

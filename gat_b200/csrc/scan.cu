@@ -1,7 +1,13 @@
 /* Device-wide exclusive scan of int64 counts (CSR offsets for range items and results). */
 #include "internal.h"
+#include "launch.cuh"
 
 namespace gat {
+
+__global__ void k_zero_words(int* p, int n) {
+    dep_wait();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
+}
 namespace {
 
 constexpr int kScanThreads = 512;
@@ -38,6 +44,7 @@ __device__ int64_t block_exclusive_scan(int64_t v, int64_t* total) {
 
 /* out[i] = exclusive prefix of in within the tile; block_sums[b] = tile total */
 __global__ void k_scan_tiles(const int64_t* in, int64_t* out, int64_t n, int64_t* block_sums) {
+    dep_wait();
     int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
     int64_t v[kScanItems];
     int64_t s = 0;
@@ -57,6 +64,7 @@ __global__ void k_scan_tiles(const int64_t* in, int64_t* out, int64_t n, int64_t
 }
 
 __global__ void k_scan_add(int64_t* out, int64_t n, const int64_t* block_prefix) {
+    dep_wait();
     int64_t base = (int64_t)blockIdx.x * kScanTile;
     int64_t add = block_prefix[blockIdx.x];
     for (int k = threadIdx.x; k < kScanTile; k += blockDim.x)
@@ -64,6 +72,7 @@ __global__ void k_scan_add(int64_t* out, int64_t n, const int64_t* block_prefix)
 }
 
 __global__ void k_scan_total(int64_t* out, int64_t n, const int64_t* in_last, const int64_t* out_last_before) {
+    dep_wait();
     /* out[n] = out[n-1] + in[n-1], with both read before out[n-1] changes (captured values) */
     if (threadIdx.x == 0 && blockIdx.x == 0) out[n] = *out_last_before + *in_last;
 }
@@ -74,7 +83,7 @@ __global__ void k_scan_total(int64_t* out, int64_t n, const int64_t* in_last, co
 int scan_i64(gat_ctx* ctx, const int64_t* in, int64_t* out, int64_t n) {
     cudaStream_t s = ctx->stream;
     if (n <= 0) {
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(out, 0, sizeof(int64_t), s), "scan");
+        (void)launch_dep(ctx, k_zero_words, dim3(1), dim3(32), 0, s, reinterpret_cast<int*>(out), 2);
         return GAT_OK;
     }
     /* levels of block sums: level l holds ceil(n_l / tile) values */
@@ -103,7 +112,7 @@ int scan_i64(gat_ctx* ctx, const int64_t* in, int64_t* out, int64_t n) {
         int64_t blocks = (cur_n + kScanTile - 1) / kScanTile;
         int64_t* sums = next;
         next += blocks + 1;
-        k_scan_tiles<<<(unsigned)blocks, kScanThreads, 0, s>>>(cur_in, cur_out, cur_n, sums);
+        (void)launch_dep(ctx, k_scan_tiles, dim3((unsigned)blocks), dim3(kScanThreads), 0, s, cur_in, cur_out, cur_n, sums);
         count_launch(ctx);
         outs.push_back({cur_out, cur_n});
         if (blocks == 1) break;
@@ -114,11 +123,11 @@ int scan_i64(gat_ctx* ctx, const int64_t* in, int64_t* out, int64_t n) {
     /* pass up: add scanned block sums of level l+1 into level l */
     for (int l = (int)outs.size() - 2; l >= 0; l--) {
         int64_t blocks = (outs[l].second + kScanTile - 1) / kScanTile;
-        k_scan_add<<<(unsigned)blocks, kScanThreads, 0, s>>>(outs[l].first, outs[l].second, outs[l + 1].first);
+        (void)launch_dep(ctx, k_scan_add, dim3((unsigned)blocks), dim3(kScanThreads), 0, s, outs[l].first, outs[l].second, outs[l + 1].first);
         count_launch(ctx);
     }
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(last_out, out + (n - 1), sizeof(int64_t), cudaMemcpyDeviceToDevice, s), "scan");
-    k_scan_total<<<1, 32, 0, s>>>(out, n, last_in, last_out);
+    (void)launch_dep(ctx, k_scan_total, dim3(1), dim3(32), 0, s, out, n, last_in, last_out);
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "scan launch");
     return GAT_OK;

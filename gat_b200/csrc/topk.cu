@@ -22,6 +22,7 @@
 
 #include "edr_kernel.cuh"
 #include "internal.h"
+#include "launch.cuh"
 
 namespace gat {
 namespace {
@@ -68,6 +69,7 @@ __device__ __forceinline__ int cell_of(const GridDev& g, float lon, float lat) {
  * qfv rows have stride `stride` (>= longest query); nnz in qfv_n. */
 __global__ void k_query_fv(GridDev g, int nq, const int32_t* q_len, const int64_t* q_off, const float2* Q,
                            int stride, int pow2, int32_t* qfv_cell, int32_t* qfv_cnt, int32_t* qfv_n) {
+    dep_wait();
     extern __shared__ unsigned long long rkey[]; /* pow2 run keys (cell << 32 | count), then pow2 cells */
     int* sk = reinterpret_cast<int*>(rkey + pow2);
     __shared__ int wsum[32];
@@ -202,6 +204,7 @@ __device__ __forceinline__ void set_bit(uint32_t* bm, int words, int c) {
 
 __global__ void k_near_bitmap(int nq, int vbits, const int32_t* qfv_cell, const int32_t* qfv_n, int stride, int words,
                               uint32_t* near) {
+    dep_wait();
     int qi = blockIdx.x;
     uint32_t* bm = near + (size_t)qi * words;
     for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0;
@@ -243,6 +246,7 @@ __global__ void __launch_bounds__(kT) k_lower_bounds(int n, int nq, const int64_
                                                      const int32_t* qfv_cnt, const int32_t* qfv_n, int stride,
                                                      int vbits, const uint32_t* __restrict__ near, int words,
                                                      const int32_t* __restrict__ q_len, int32_t* lb, int32_t* flag) {
+    dep_wait();
     extern __shared__ int sq[];
     int qi = blockIdx.y;
     int qn = qfv_n[qi];
@@ -366,6 +370,7 @@ __global__ void __launch_bounds__(kT) k_lower_bounds(int n, int nq, const int64_
 constexpr int kSortTile = 2048;
 
 __global__ void k_sort_hist(int n, const int32_t* lb, int bins, int ntile, int64_t* H) {
+    dep_wait();
     extern __shared__ int hist[];
     int tile = blockIdx.x, qi = blockIdx.y;
     for (int i = threadIdx.x; i < bins; i += blockDim.x) hist[i] = 0;
@@ -381,6 +386,7 @@ __global__ void k_sort_hist(int n, const int32_t* lb, int bins, int ntile, int64
  * memory (loaded from the scanned histograms), the warp walks its ids in order 32 at a time */
 __global__ void __launch_bounds__(32) k_sort_scatter(int n, const int32_t* lb, int bins, int ntile, const int64_t* H,
                                                      int32_t* cand, int32_t* slb) {
+    dep_wait();
     extern __shared__ long long run[];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x;
@@ -418,6 +424,7 @@ __global__ void __launch_bounds__(32) k_sort_scatter(int n, const int32_t* lb, i
 enum { WS_END = 0, WS_START, WS_CHUNK, WS_W, WS_DONE, WS_WORDS };
 
 __global__ void k_walk_init(int nq, int chunk, int32_t* ws) {
+    dep_wait();
     int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= nq) return;
     int32_t* s = ws + (size_t)qi * WS_WORDS;
@@ -432,6 +439,7 @@ __global__ void k_walk_init(int nq, int chunk, int32_t* ws) {
  * order by up to `chunk` candidates whose bound is at most W; the new slices are numbered
  * consecutively over the queries (wprefix) for the EDR kernel. */
 __global__ void k_walk_plan(int n, int nq, const int32_t* slb, int32_t* ws, int* wprefix) {
+    dep_wait();
     __shared__ int warp_sum[32];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
@@ -530,6 +538,7 @@ struct WalkPairs {
  * candidate with a smaller bound may still be closer. */
 __global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* slb, const int32_t* cand,
                            const int32_t* sdist, int32_t* ws) {
+    dep_wait();
     extern __shared__ int hist[];
     __shared__ int sh_W, cnt;
     int qi = blockIdx.x;
@@ -590,6 +599,7 @@ __global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* sl
 __global__ void k_final(int n, int k, int words, uint32_t* gbitmap, const int32_t* cand, const int32_t* sdist,
                         const int32_t* ws, int32_t* out_ids, int32_t* out_dist, int32_t* flag,
                         unsigned long long* pairs) {
+    dep_wait();
     extern __shared__ uint32_t bm_s[];
     __shared__ unsigned long long lt_keys[1024];
     __shared__ int lt_n;
@@ -730,7 +740,7 @@ int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
     int32_t* qfv_n = (int32_t*)(qfv + 2 * fvb);
     size_t smem_fv = (size_t)pow2 * 12;
     allow_smem(k_query_fv, smem_fv);
-    k_query_fv<<<std::min(nq, ctx->sm_count * 4), 512, smem_fv, s>>>(g->grid, nq, d_q_len, d_q_off, d_q_xy, stride, pow2,
+    (void)launch_dep(ctx, k_query_fv, dim3(std::min(nq, ctx->sm_count * 4)), dim3(512), smem_fv, s, g->grid, nq, d_q_len, d_q_off, d_q_xy, stride, pow2,
                                                                       qfv_cell, qfv_cnt, qfv_n);
     count_launch(ctx);
     /* lower bounds */
@@ -741,13 +751,13 @@ int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
     int nwords = ((1 << vbits) + 31) / 32;
     uint32_t* near = (uint32_t*)scratch(ctx, S_TOPK_NEAR, (size_t)nq * nwords * 4 + 64, &st);
     if (!near) return st;
-    k_near_bitmap<<<nq, kT, 0, s>>>(nq, vbits, qfv_cell, qfv_n, stride, nwords, near);
+    (void)launch_dep(ctx, k_near_bitmap, dim3(nq), dim3(kT), 0, s, nq, vbits, qfv_cell, qfv_n, stride, nwords, near);
     count_launch(ctx);
     size_t smem_lb = (size_t)stride * 8;
     allow_smem(k_lower_bounds, smem_lb);
     dim3 lgrid((n + kT - 1) / kT, nq);
     timed_begin(ctx, GAT_KERNEL_BOUNDS);
-    k_lower_bounds<<<lgrid, kT, smem_lb, s>>>(n, nq, g->d_fv_off, g->d_fv_cell, g->d_fv_cnt, qfv_cell, qfv_cnt, qfv_n, stride,
+    (void)launch_dep(ctx, k_lower_bounds, dim3(lgrid), dim3(kT), smem_lb, s, n, nq, g->d_fv_off, g->d_fv_cell, g->d_fv_cnt, qfv_cell, qfv_cnt, qfv_n, stride,
                                              vbits, near, nwords, d_q_len, lb, ctx->d_flag);
     /* algorithmic bytes: every trajectory's FV (8 B per entry + 8 B offset) and its bound (4 B)
      * per query */
@@ -768,12 +778,12 @@ int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
     R.wprefix = (int*)(ws + (size_t)nq * WS_WORDS);
     size_t smem_h = (size_t)bins_lb * 4;
     allow_smem(k_sort_hist, smem_h);
-    k_sort_hist<<<dim3(ntile, nq), kT, smem_h, s>>>(n, lb, bins_lb, ntile, H);
+    (void)launch_dep(ctx, k_sort_hist, dim3(dim3(ntile, nq)), dim3(kT), smem_h, s, n, lb, bins_lb, ntile, H);
     count_launch(ctx);
     if ((st = scan_i64(ctx, H, H, (int64_t)nq * bins_lb * ntile)) != GAT_OK) return st;
     size_t smem_run = (size_t)bins_lb * 8;
     allow_smem(k_sort_scatter, smem_run);
-    k_sort_scatter<<<dim3(ntile, nq), 32, smem_run, s>>>(n, lb, bins_lb, ntile, H, R.cand, R.slb);
+    (void)launch_dep(ctx, k_sort_scatter, dim3(dim3(ntile, nq)), dim3(32), smem_run, s, n, lb, bins_lb, ntile, H, R.cand, R.slb);
     count_launch(ctx);
     /* the walk: a finished query costs nothing in later rounds and `rounds` covers the whole
      * order with growing chunks. A lone query leaves most of the GPU idle in a small round, so
@@ -789,7 +799,7 @@ int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
         cover += c;
     }
     R.rounds += 1;
-    k_walk_init<<<(nq + 127) / 128, 128, 0, s>>>(nq, R.chunk0, ws);
+    (void)launch_dep(ctx, k_walk_init, dim3((nq + 127) / 128), dim3(128), 0, s, nq, R.chunk0, ws);
     count_launch(ctx);
     R.bins_d = max_q_len + db->maxlen + 2;
     R.smem_d = (size_t)R.bins_d * 4;
@@ -802,7 +812,7 @@ int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
 
 /* Phase 2a: each unfinished query extends its evaluated prefix (pair numbering in wprefix). */
 void topk_plan(gat_ctx* ctx, const TopkRun& R) {
-    k_walk_plan<<<1, 1024, 0, ctx->stream>>>(R.n, R.nq, R.slb, R.ws, R.wprefix);
+    (void)launch_dep(ctx, k_walk_plan, dim3(1), dim3(1024), 0, ctx->stream, R.n, R.nq, R.slb, R.ws, R.wprefix);
     count_launch(ctx);
 }
 
@@ -810,7 +820,7 @@ void topk_plan(gat_ctx* ctx, const TopkRun& R) {
 int topk_round(gat_ctx* ctx, const TopkRun& R, int64_t npairs, unsigned long long* cells) {
     int st = edr::edr_launch(ctx, R.src, npairs, R.rows_hint, R.max_cols, R.u, cells);
     if (st != GAT_OK) return st;
-    k_walk_kth<<<R.nq, kT, R.smem_d, ctx->stream>>>(R.n, R.k, R.bins_d, R.growth, R.slb, R.cand, R.sdist, R.ws);
+    (void)launch_dep(ctx, k_walk_kth, dim3(R.nq), dim3(kT), R.smem_d, ctx->stream, R.n, R.k, R.bins_d, R.growth, R.slb, R.cand, R.sdist, R.ws);
     count_launch(ctx);
     return GAT_OK;
 }
@@ -828,7 +838,7 @@ int topk_post(gat_ctx* ctx, const TopkRun& R, int32_t* d_ids, int32_t* d_dist, u
     } else {
         allow_smem(k_final, smem_final);
     }
-    k_final<<<R.nq, kT, smem_final, ctx->stream>>>(R.n, R.k, words, gbm, R.cand, R.sdist, R.ws, d_ids, d_dist, ctx->d_flag,
+    (void)launch_dep(ctx, k_final, dim3(R.nq), dim3(kT), smem_final, ctx->stream, R.n, R.k, words, gbm, R.cand, R.sdist, R.ws, d_ids, d_dist, ctx->d_flag,
                                                    pairs);
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "top-k launch");
@@ -894,6 +904,7 @@ struct StageDesc {
 
 __global__ void k_stage(const StageDesc* d, int* next, int* cur, int32_t* len1, int64_t* off1, float2* xy1,
                         int32_t* flag) {
+    dep_wait();
     __shared__ int qi_s, len_s;
     __shared__ long long off_s;
     if (threadIdx.x == 0) {
@@ -922,6 +933,7 @@ __global__ void k_stage(const StageDesc* d, int* next, int* cur, int32_t* len1, 
 }
 
 __global__ void k_unstage(const StageDesc* d, const int* cur, const int32_t* ids1, const int32_t* dist1, int k) {
+    dep_wait();
     const int qi = *cur;
     if (qi >= d->nq) return;
     for (int i = threadIdx.x; i < k; i += blockDim.x) {
@@ -933,6 +945,7 @@ __global__ void k_unstage(const StageDesc* d, const int* cur, const int32_t* ids
 /* ends the round loop once the query is done; a bound on the rounds guards the loop */
 __global__ void k_loop_cond(const int32_t* ws, int* iter, int maxit, int32_t* flag, unsigned long long* rounds,
                             cudaGraphConditionalHandle h) {
+    dep_wait();
     const int it = ++(*iter);
     atomicAdd(rounds, 1ull);
     bool more = ws[WS_DONE] == 0;
@@ -947,7 +960,7 @@ struct LoneGraph {
     const gat_index* g = nullptr;
     int max_q_len = 0, k = 0;
     float u = 0.f;
-    int chunk = 0, growth = 0, rows = 0, form = 0; /* the context's knobs when the graph was built */
+    int chunk = 0, growth = 0, rows = 0, form = 0, dep = 1; /* the context's knobs when the graph was built */
     gat_ctx* w = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -980,7 +993,8 @@ int lone_graph_get(gat_ctx* ctx, const gat_index* g, int max_q_len, int k, float
         if (o.second == lone_graph_free) {
             auto* L = static_cast<LoneGraph*>(o.first);
             if (L->g == g && L->max_q_len == max_q_len && L->k == k && L->u == u && L->chunk == ctx->topk_chunk &&
-                L->growth == ctx->topk_growth && L->rows == ctx->edr_rows && L->form == ctx->edr_form) {
+                L->growth == ctx->topk_growth && L->rows == ctx->edr_rows && L->form == ctx->edr_form &&
+                L->dep == ctx->dep_launch) {
                 *out = L;
                 return GAT_OK;
             }
@@ -1009,10 +1023,12 @@ int lone_graph_get(gat_ctx* ctx, const gat_index* g, int max_q_len, int k, float
     L->growth = ctx->topk_growth;
     L->rows = ctx->edr_rows;
     L->form = ctx->edr_form;
+    L->dep = ctx->dep_launch;
     L->w->edr_rows = ctx->edr_rows ? ctx->edr_rows : kLoneRows;
     L->w->edr_form = ctx->edr_form ? ctx->edr_form : kLoneForm;
     L->w->topk_chunk = ctx->topk_chunk;
     L->w->topk_growth = ctx->topk_growth;
+    L->w->dep_launch = ctx->dep_launch;
     if (cudaEventCreateWithFlags(&L->ev, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         lone_graph_free(L);
@@ -1049,9 +1065,9 @@ int lone_graph_get(gat_ctx* ctx, const gat_index* g, int max_q_len, int k, float
 /* the kernels of one query before / inside / after the round loop, on the worker's stream */
 int lone_pre(LoneGraph* L, TopkRun& R) {
     gat_ctx* w = L->w;
-    k_stage<<<1, 256, 0, w->stream>>>(L->d_desc, L->d_next, L->d_cur, L->len1, L->off1, L->xy1, w->d_flag);
+    (void)launch_dep(w, k_stage, dim3(1), dim3(256), 0, w->stream, L->d_desc, L->d_next, L->d_cur, L->len1, L->off1, L->xy1, w->d_flag);
     count_launch(w);
-    GAT_CUDA_TRY(w, cudaMemsetAsync(L->d_iter, 0, sizeof(int), w->stream), "top-k");
+    (void)launch_dep(w, k_zero_words, dim3(1), dim3(32), 0, w->stream, L->d_iter, 1);
     return topk_pre(w, L->g, 1, L->len1, L->off1, L->xy1, L->max_q_len, L->k, L->u, nullptr, R);
 }
 
@@ -1061,7 +1077,7 @@ int lone_round(LoneGraph* L, const TopkRun& R, const cudaGraphConditionalHandle*
     int st = topk_round(w, R, R.n, L->acc);
     if (st != GAT_OK) return st;
     if (h) {
-        k_loop_cond<<<1, 1, 0, w->stream>>>(R.ws, L->d_iter, R.rounds + 1, w->d_flag, L->acc + 2, *h);
+        (void)launch_dep(w, k_loop_cond, dim3(1), dim3(1), 0, w->stream, R.ws, L->d_iter, R.rounds + 1, w->d_flag, L->acc + 2, *h);
         count_launch(w);
     }
     return GAT_OK;
@@ -1071,7 +1087,7 @@ int lone_post(LoneGraph* L, const TopkRun& R) {
     gat_ctx* w = L->w;
     int st = topk_post(w, R, L->ids1, L->dist1, L->acc + 1);
     if (st != GAT_OK) return st;
-    k_unstage<<<1, 256, 0, w->stream>>>(L->d_desc, L->d_cur, L->ids1, L->dist1, L->k);
+    (void)launch_dep(w, k_unstage, dim3(1), dim3(256), 0, w->stream, L->d_desc, L->d_cur, L->ids1, L->dist1, L->k);
     count_launch(w);
     return GAT_OK;
 }

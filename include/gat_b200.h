@@ -108,9 +108,12 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  * GAT_TUNE_INDEX_BUILD: where gat_grid_build and gat_fsg_build place the points. 0 (default) =
  *   on the device for a context with one, 1 = on the host, 2 = on the device (GAT_ERR_STATE on a
  *   host-only context). Both give the same index, array for array; STIG is always built on the
- *   host (its median splits follow std::sort's order among equal coordinates). */
+ *   host (its median splits follow std::sort's order among equal coordinates).
+ * GAT_TUNE_DEP_LAUNCH: 1 (default) launches the kernels of the top-k and EDR paths as
+ *   programmatic dependent launches (each kernel is set up while the one before it drains; the
+ *   order of their work is unchanged), 0 launches them plainly. Same results. */
 enum { GAT_TUNE_EDR_ROWS = 1, GAT_TUNE_EDR_TUNED = 2, GAT_TUNE_TOPK_CHUNK = 3, GAT_TUNE_TOPK_GROWTH = 4,
-       GAT_TUNE_EDR_FORM = 5, GAT_TUNE_INDEX_BUILD = 6 };
+       GAT_TUNE_EDR_FORM = 5, GAT_TUNE_INDEX_BUILD = 6, GAT_TUNE_DEP_LAUNCH = 7 };
 int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value);
 int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value);
 

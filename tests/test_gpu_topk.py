@@ -106,3 +106,26 @@ def test_plain_graph_matches_stream_path(gpu_ctx, small):
     one = t.subset(qids[:1])
     i1, d1, _ = g.topk(one, 5, 5e-4, execution="plain")
     assert np.array_equal(i1[0], b_ids[0, :5]) and np.array_equal(d1[0], b_d[0, :5])
+
+
+def test_dependent_launch_does_not_change_results(gpu_ctx, small):
+    """GAT_TUNE_DEP_LAUNCH 0 (plain launches) and 1 (programmatic dependent launches) give the
+    same top-k lists in the plain graph and batched forms, and the same EDR of pairs."""
+    from gat_b200 import _lib as L
+
+    t, g, o, qids = small
+    q = t.subset(qids)
+    res = {}
+    try:
+        for dep in (0, 1):
+            gpu_ctx.set_tuning(L.GAT_TUNE_DEP_LAUNCH, dep)
+            assert gpu_ctx.tuning(L.GAT_TUNE_DEP_LAUNCH) == dep
+            res[dep] = [g.topk(q, 16, 5e-4, execution=e)[:2] for e in ("plain", "batched", "plain")]
+            la, a, lb, b = D.config4_pairs(seed=3, npairs=64, lo=16, hi=600)
+            res[dep].append((G.api.edr_pairs(gpu_ctx, la, a, lb, b, 5e-4),))
+    finally:
+        gpu_ctx.set_tuning(L.GAT_TUNE_DEP_LAUNCH, 1)
+    for x, y in zip(res[0], res[1]):
+        for u, v in zip(x, y):
+            assert np.array_equal(u, v)
+

@@ -163,6 +163,19 @@ def test_index_build_knob(host_ctx):
         host_ctx.set_tuning(L.GAT_TUNE_INDEX_BUILD, 0)
 
 
+def test_dependent_launch_knob(host_ctx):
+    """GAT_TUNE_DEP_LAUNCH takes 0 or 1 (default 1)."""
+    assert host_ctx.tuning(L.GAT_TUNE_DEP_LAUNCH) == 1
+    try:
+        host_ctx.set_tuning(L.GAT_TUNE_DEP_LAUNCH, 0)
+        assert host_ctx.tuning(L.GAT_TUNE_DEP_LAUNCH) == 0
+        for v in (-1, 2):
+            with pytest.raises(G.GatError):
+                host_ctx.set_tuning(L.GAT_TUNE_DEP_LAUNCH, v)
+    finally:
+        host_ctx.set_tuning(L.GAT_TUNE_DEP_LAUNCH, 1)
+
+
 def test_snapshot_errors(host_ctx, tmp_path):
     """Saving needs a device context; loading refuses missing and foreign files."""
     t = D.walks(D.lengths(50, 0, 0, 0, 1, 20, 25), 25)
