@@ -787,12 +787,13 @@ int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
     count_launch(ctx);
     /* the walk: a finished query costs nothing in later rounds and `rounds` covers the whole
      * order with growing chunks. A lone query leaves most of the GPU idle in a small round, so
-     * it starts with a larger chunk and grows faster; a batch keeps rounds tight to limit
-     * surplus evaluations. */
+     * it starts with a larger chunk; every walk doubles its chunk per round, which keeps the
+     * surplus evaluations of the last round small (C2 plain: 2191 pairs per query with doubling
+     * against 2832 when quadrupling, 12% more queries per second). */
     R.lone = nq <= 4;
     R.chunk0 = ctx->topk_chunk ? ctx->topk_chunk : (R.lone ? 1024 : 128);
     R.chunk0 = std::max(R.chunk0, R.lone ? 8 * k : 4 * k);
-    R.growth = ctx->topk_growth ? ctx->topk_growth : (R.lone ? 4 : 2);
+    R.growth = ctx->topk_growth ? ctx->topk_growth : 2;
     R.rounds = 1;
     for (int64_t cover = R.chunk0, c = R.chunk0; cover < n; R.rounds++) {
         c *= R.growth;

@@ -102,9 +102,9 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  *   side, steps walk the longer side), 2 = column tiles (lanes own columns, steps walk the
  *   shorter side: a shorter critical path for pairs of uneven length). Same results.
  * GAT_TUNE_TOPK_CHUNK / GAT_TUNE_TOPK_GROWTH: candidates a query evaluates in the first round
- *   of the top-k walk, and the factor each later round grows by (0 = defaults: 1024 and 4 for up
- *   to 4 queries per batch, 128 and 2 for larger batches; the first round is never below 8k
- *   or 4k). Results never depend on them; they trade rounds against surplus evaluations.
+ *   of the top-k walk, and the factor each later round grows by (0 = defaults: a first round of
+ *   1024 for up to 4 queries per batch and 128 for larger batches, never below 8k or 4k;
+ *   growth 2). Results never depend on them; they trade rounds against surplus evaluations.
  * GAT_TUNE_INDEX_BUILD: where gat_grid_build and gat_fsg_build place the points. 0 (default) =
  *   on the device for a context with one, 1 = on the host, 2 = on the device (GAT_ERR_STATE on a
  *   host-only context). Both give the same index, array for array; STIG is always built on the
