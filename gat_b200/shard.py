@@ -13,12 +13,10 @@ queries needs no exchange and is what `bench.py --gpus N` runs (replicas).
 """
 from __future__ import annotations
 
-import ctypes as C
-
 import numpy as np
 
 from . import _lib as L
-from .api import Context, Grid, RangeResult, TrajectorySet, _c, _p
+from .api import Context, Grid, RangeResult, TrajectorySet, _p
 from .data import Trajectories
 
 lib = L.lib
@@ -111,17 +109,12 @@ def gather_ranges(offsets: np.ndarray, tids: np.ndarray, group=None, device=None
     all_ids = [torch.empty_like(mine) for _ in range(world)]
     td.all_gather(all_ids, mine, group=group)
     cnt = np.stack([c.cpu().numpy() for c in all_counts])  # [world, nq]
-    ids = [a.cpu().numpy() for a in all_ids]
-    starts = [np.concatenate([[0], np.cumsum(cnt[r])]) for r in range(world)]
+    ids = np.concatenate([all_ids[r].cpu().numpy()[: totals[r]] for r in range(world)])
+    query = np.concatenate([np.repeat(np.arange(nq), cnt[r]) for r in range(world)])
+    # a stable sort by query keeps the ranks in order within each query
+    out = ids[np.argsort(query, kind="stable")].astype(np.int32)
     out_off = np.zeros(nq + 1, np.int64)
     out_off[1:] = np.cumsum(cnt.sum(axis=0))
-    out = np.empty(int(out_off[-1]), np.int32)
-    for q in range(nq):
-        w = out_off[q]
-        for r in range(world):
-            s, e = starts[r][q], starts[r][q + 1]
-            out[w:w + e - s] = ids[r][s:e]
-            w += e - s
     return RangeResult(out_off, out, None)
 
 
