@@ -788,10 +788,11 @@ int topk_pre(gat_ctx* ctx, const gat_index* g, int nq, const int32_t* d_q_len, c
     /* the walk: a finished query costs nothing in later rounds and `rounds` covers the whole
      * order with growing chunks. A lone query leaves most of the GPU idle in a small round, so
      * it starts with a larger chunk; every walk doubles its chunk per round, which keeps the
-     * surplus evaluations of the last round small (C2 plain: 2191 pairs per query with doubling
-     * against 2832 when quadrupling, 12% more queries per second). */
+     * surplus evaluations of the last round small. On the C2 set (100k walks, k = 32), first
+     * rounds of 768 / 1024 / 1280 / 1536 candidates with doubling ran 3.21k / 3.29k / 3.40k /
+     * 3.28k queries per second, quadrupling from 1024 2.9k. */
     R.lone = nq <= 4;
-    R.chunk0 = ctx->topk_chunk ? ctx->topk_chunk : (R.lone ? 1024 : 128);
+    R.chunk0 = ctx->topk_chunk ? ctx->topk_chunk : (R.lone ? 1280 : 128);
     R.chunk0 = std::max(R.chunk0, R.lone ? 8 * k : 4 * k);
     R.growth = ctx->topk_growth ? ctx->topk_growth : 2;
     R.rounds = 1;

@@ -103,7 +103,7 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  *   shorter side: a shorter critical path for pairs of uneven length). Same results.
  * GAT_TUNE_TOPK_CHUNK / GAT_TUNE_TOPK_GROWTH: candidates a query evaluates in the first round
  *   of the top-k walk, and the factor each later round grows by (0 = defaults: a first round of
- *   1024 for up to 4 queries per batch and 128 for larger batches, never below 8k or 4k;
+ *   1280 for up to 4 queries per batch and 128 for larger batches, never below 8k or 4k;
  *   growth 2). Results never depend on them; they trade rounds against surplus evaluations.
  * GAT_TUNE_INDEX_BUILD: where gat_grid_build and gat_fsg_build place the points. 0 (default) =
  *   on the device for a context with one, 1 = on the host, 2 = on the device (GAT_ERR_STATE on a
