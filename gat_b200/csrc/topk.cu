@@ -541,26 +541,60 @@ __global__ void k_walk_kth(int n, int k, int bins, int growth, const int32_t* sl
     dep_wait();
     extern __shared__ int hist[];
     __shared__ int sh_W, cnt;
+    __shared__ int warp_tot[kT / 32];
     int qi = blockIdx.x;
     int32_t* s = ws + (size_t)qi * WS_WORDS;
     if (s[WS_DONE]) return;
     const int end = s[WS_END];
     const int32_t* dist = sdist + (size_t)qi * n;
     for (int i = threadIdx.x; i < bins; i += blockDim.x) hist[i] = 0;
-    if (threadIdx.x == 0) cnt = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < end; i += blockDim.x) atomicAdd(&hist[min(dist[i], bins - 1)], 1);
-    __syncthreads();
     if (threadIdx.x == 0) {
-        int run = 0, W = INT_MAX;
-        for (int i = 0; i < bins; i++) {
-            if (run + hist[i] >= k) {
-                W = i;
-                break;
-            }
-            run += hist[i];
+        cnt = 0;
+        sh_W = INT_MAX;
+    }
+    __syncthreads();
+    /* histogram of the evaluated distances, four loads in flight per thread (a negative
+     * distance marks a pair whose wait gave up; the call then fails, it is not counted) */
+    for (int i0 = threadIdx.x; i0 < end; i0 += 4 * blockDim.x) {
+        int d[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = i0 + u * blockDim.x;
+            d[u] = i < end ? dist[i] : -1;
         }
-        sh_W = W;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (d[u] >= 0) atomicAdd(&hist[min(d[u], bins - 1)], 1);
+    }
+    __syncthreads();
+    /* W = the first bin where the running count reaches k: each thread sums a slice of bins,
+     * a block-wide scan gives the slice's starting count, and the one thread whose slice
+     * crosses k walks it */
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int per = (bins + blockDim.x - 1) / blockDim.x;
+        const int b0 = min(bins, threadIdx.x * per), b1 = min(bins, b0 + per);
+        int local = 0;
+        for (int b = b0; b < b1; b++) local += hist[b];
+        int incl = local;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        int before = incl - local;
+        for (int w = 0; w < warp; w++) before += warp_tot[w];
+        if (before < k && before + local >= k) {
+            int run = before;
+            for (int b = b0; b < b1; b++) {
+                if (run + hist[b] >= k) {
+                    sh_W = b;
+                    break;
+                }
+                run += hist[b];
+            }
+        }
     }
     __syncthreads();
     const int W = sh_W;
