@@ -176,6 +176,21 @@ def test_dependent_launch_knob(host_ctx):
         host_ctx.set_tuning(L.GAT_TUNE_DEP_LAUNCH, 1)
 
 
+def test_topk_merge_arguments(host_ctx):
+    """gat_topk_merge validates its sizes; the device form needs a device context."""
+    ids = np.array([[[3, 7]], [[1, -1]]], np.int32)
+    dist = np.array([[[2, 5]], [[2, -1]]], np.int32)
+    oi, od = np.zeros((1, 2), np.int32), np.zeros((1, 2), np.int32)
+    P = lambda a: a.ctypes.data_as(L.P_i32)
+    assert L.lib.gat_topk_merge(1, 2, 2, P(ids), P(dist), P(oi), P(od)) == L.GAT_OK
+    assert oi.tolist() == [[1, 3]] and od.tolist() == [[2, 2]]  # (distance, id) order
+    for nq, k, parts in ((-1, 2, 2), (1, 0, 2), (1, 2, 0), (1, 1025, 1), (1, 1024, 9)):
+        assert L.lib.gat_topk_merge(nq, k, parts, P(ids), P(dist), P(oi), P(od)) == L.GAT_ERR_ARG
+    assert L.lib.gat_topk_merge_dev(host_ctx.h, 1, 2, 2, None, None, None, None) == L.GAT_ERR_ARG
+    assert L.lib.gat_topk_merge_dev(host_ctx.h, 1, 2, 2, ids.ctypes.data, dist.ctypes.data, oi.ctypes.data,
+                                    od.ctypes.data) == L.GAT_ERR_STATE
+
+
 def test_snapshot_errors(host_ctx, tmp_path):
     """Saving needs a device context; loading refuses missing and foreign files."""
     t = D.walks(D.lengths(50, 0, 0, 0, 1, 20, 25), 25)
