@@ -6,8 +6,8 @@
  * Handles are opaque and owned by the library (destroy indexes, then trajectory sets, then the
  * context they were made on): a gat_db holds a trajectory set resident in
  * device memory, a gat_index holds one of the reference's three range indexes (GT-quadtree
- * "Grid" with its FVTable, STIG, FSG) built on the host in the reference's exact layout and
- * resident in device memory. Host output buffers are owned by the caller; calls whose output
+ * "Grid" with its FVTable, STIG, FSG) in the reference's exact layout, resident in device
+ * memory (Grid and FSG are built on the device by default, STIG on the host). Host output buffers are owned by the caller; calls whose output
  * size is data-dependent take a capacity and report the size needed (GAT_ERR_TRUNCATED when
  * it did not fit, with nothing written beyond the capacity).
  *
@@ -23,6 +23,10 @@
  *   Grid::Grid + addDatasetToGrid    Grid.h:39,42     -> gat_grid_build
  *   STIG::initial                    STIG.h:57        -> gat_stig_build
  *   FSG::FSG + addDatasetToGrid      FSG.h:35,38      -> gat_fsg_build
+ *   PreProcess::readTraFromFormatedFile / writeTraDataToFile
+ *                                    PreProcess.cpp:203-315 -> gat_traj_file_read / _write
+ * Additions without a counterpart: index snapshots, the serving loop, the top-k merge of sets
+ * sharded across GPUs, tuning knobs, and an allocation-free EDR entry point.
  */
 #ifndef GAT_B200_H
 #define GAT_B200_H
