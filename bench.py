@@ -1221,7 +1221,7 @@ def run_reference_build(args, world, rank):
                  "cpu_baseline": {"value": round(v, 1), "unit": "points/s", "cores": 1, "kind": "reference",
                                   "sample": f"first {BUILD['ref_n']} of the 1M trajectories per step (the reference's "
                                             "Grid build allocates and clears a cell-sized array per trajectory, "
-                                            "Grid.cpp:268-269, so the full set does not finish in minutes)"},
+                                            "Grid.cpp:268-269, so the full set takes about 3 minutes per build)"},
                  "e2e": {"value": round(v, 1), "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     return line
 
@@ -1253,15 +1253,16 @@ def main():
     if args.impl == "reference":
         fn = REFERENCE.get(args.workload) or run_reference_c2
         if args.workload == "c3":
-            line = {"impl": "reference", "unavailable": "the reference's Grid build is O(trajectories x cells) in memset "
-                    "(Grid.cpp:268-269); at 1M trajectories and 1M cells it does not finish in minutes"}
+            line = {"impl": "reference", "unavailable": "the reference's Grid build clears a cell-sized array per "
+                    "trajectory (Grid.cpp:268-269): about 3 minutes on one core for the 1M-trajectory set before any "
+                    "query, and its 100k queries then scan on one core; a bench step cannot hold that"}
         elif args.workload == "c4k":
-            line = {"impl": "reference", "unavailable": "the reference's Grid build over the 1M-trajectory set does not "
-                    "finish in minutes (Grid.cpp:268-269), and its GPU EDR kernel stops at 1024 points per side "
+            line = {"impl": "reference", "unavailable": "the reference's Grid build over the 1M-trajectory set takes about "
+                    "3 minutes on one core (Grid.cpp:268-269), and its GPU EDR kernel stops at 1024 points per side "
                     "(kernel.cu:249-501) while these queries reach 4096"}
         elif args.workload == "c5":
             line = {"impl": "reference", "unavailable": "the reference has no serving loop, and its Grid build over the "
-                    "1M-trajectory set does not finish in minutes (Grid.cpp:268-269)"}
+                    "1M-trajectory set takes about 3 minutes on one core (Grid.cpp:268-269)"}
         else:
             line = fn(args, world, rank)
         if line is not None:
