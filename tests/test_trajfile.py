@@ -58,3 +58,21 @@ def test_empty_trajectories_and_errors(tmp_path):
         D.read_trajectory_file(str(bad))
     with pytest.raises(RuntimeError):
         D.read_trajectory_file(str(tmp_path / "missing.txt"))
+
+
+def test_reader_accepts_what_strtod_accepts(tmp_path):
+    """Fields parse as the reference's strtod / strtol parse them: leading blanks and '+', an
+    exponent, hexadecimal floats, inf and nan, integers beyond the int range (saturated, then
+    converted to int32 as the old reader did)."""
+    p = tmp_path / "odd.txt"
+    p.write_text("2\n121,30.7,122,31.7\n2;2;\n"
+                 " +31.5, 121.25,1, +7;3.15e1,0x1.e4p+6,1,-8;\n"
+                 "inf,-nan,2,99999999999999;1.0,2.0,2,99999999999999999999999;\n")
+    r, _, times = D.read_trajectory_file(str(p))
+    assert r.lengths.tolist() == [2, 2]
+    assert r.lat[0] == np.float32(31.5) and r.lon[0] == np.float32(121.25)
+    assert r.lat[1] == np.float32(31.5) and r.lon[1] == np.float32(float.fromhex("0x1.e4p+6"))
+    assert np.isinf(r.lat[2]) and np.isnan(r.lon[2])
+    assert times[0] == 7 and times[1] == -8
+    assert times[2] == np.int64(99999999999999).astype(np.int32)  # a long, converted to int32
+    assert times[3] == np.int64(2**63 - 1).astype(np.int32)  # beyond a long: strtol saturates
