@@ -87,6 +87,22 @@ public:
     }
     Context(const Context&) = delete;
     Context& operator=(const Context&) = delete;
+    /* tuning knobs (GAT_TUNE_*); results never depend on them */
+    void setTuning(int knob, int value) {
+        int rc = gat_ctx_set_tuning(h, knob, value);
+        if (rc != GAT_OK) throw Error(rc, gat_last_error(h));
+    }
+    int tuning(int knob) const {
+        int v = 0;
+        int rc = gat_ctx_get_tuning(h, knob, &v);
+        if (rc != GAT_OK) throw Error(rc, gat_last_error(h));
+        return v;
+    }
+    /* returns the scratch arena and kept index-build temporaries to the device */
+    void trim() {
+        int rc = gat_ctx_trim(h);
+        if (rc != GAT_OK) throw Error(rc, gat_last_error(h));
+    }
     gat_ctx* h = nullptr;
 };
 

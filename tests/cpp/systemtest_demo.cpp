@@ -56,6 +56,9 @@ int main(int argc, char** argv) {
     }
     try {
         gat::Context ctx(device);
+        ctx.setTuning(GAT_TUNE_TOPK_GROWTH, 3);
+        printf("tuning %d\n", ctx.tuning(GAT_TUNE_TOPK_GROWTH));
+        ctx.setTuning(GAT_TUNE_TOPK_GROWTH, 0);
         const gat::MBB range(box[0], box[1], box[2], box[3]);
         gat::Grid g(ctx, range, 0.01f, 2, 512);
         gat::STIG stig(ctx);

@@ -30,7 +30,7 @@ def run(exe, device, n=2000, path=None):
         f = line.split()
         if len(f) >= 2 and f[0] in ("build", "rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest",
                                     "rangeQueryTestWithoutMorton", "MortonGridRangeQueryTest", "rangeQueryBatch",
-                                    "similarityQueryTest", "file_roundtrip"):
+                                    "similarityQueryTest", "file_roundtrip", "tuning"):
             out[f[0]] = int(f[1])
         elif len(f) >= 2:
             out[f[0]] = np.array([int(x) for x in f[2:]], np.int64)
@@ -43,7 +43,7 @@ def test_host_only(demo, tmp_path):
     GAT_ERR_STATE instead of aborting; the trajectory file helpers round-trip."""
     rc, out, log = run(demo, -1, path=str(tmp_path / "tradb.txt"))
     assert rc == 0, log
-    assert out["build"] == 0 and out["file_roundtrip"] == 1
+    assert out["build"] == 0 and out["file_roundtrip"] == 1 and out["tuning"] == 3
     for k in ("rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest", "rangeQueryTestWithoutMorton",
               "MortonGridRangeQueryTest", "rangeQueryBatch", "similarityQueryTest"):
         assert out[k] == L.GAT_ERR_STATE, (k, log)
