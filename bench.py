@@ -136,11 +136,16 @@ def measured_peaks() -> dict:
 C2 = dict(n=100_000, nq=256, k=32, eps=5e-4, cell=0.0025, vparam=2, leaf_cap=512)
 
 
-def c2_workload(seed: int):
-    from gat_b200 import data as D
+def c2_workload(seed: int, lib: bool = True):
+    """The config 2 set and query ids, from the library's generator (lib) or the oracle's copy of
+    it (the reference arm loads no part of the library); both give the same arrays."""
+    if lib:
+        from gat_b200 import data as D
 
-    t, qids = D.config2(seed=seed, n=C2["n"], nq=C2["nq"])
-    return t, qids
+        return D.config2(seed=seed, n=C2["n"], nq=C2["nq"])
+    from oracle import pyoracle as po
+
+    return po.config2(seed=seed, n=C2["n"], nq=C2["nq"])
 
 
 def run_c2(args, world, rank, local, td):
@@ -354,7 +359,7 @@ def run_reference_c2(args, world, rank):
         return None
     from oracle import pyoracle as po
 
-    t, qids = c2_workload(seed=0)
+    t, qids = c2_workload(seed=0, lib=False)
     sample = args.cpu_sample
     # evenly spaced over the query sample, so light and heavy queries are both represented
     qs = np.asarray(qids[::max(1, len(qids) // sample)][:sample], np.int32)
@@ -566,10 +571,9 @@ def run_c1(args, world, rank, local, td):
 def run_reference_c1(args, world, rank):
     if rank != 0:
         return None
-    from gat_b200 import data as D
     from oracle import pyoracle as po
 
-    t, q = D.config1(seed=0, n=C1["n"], nq=C1["nq"])
+    t, q = po.config1(seed=0, n=C1["n"], nq=C1["nq"])
     threads = os.cpu_count() or 1
     times = []
     R = po.RefRunner()
@@ -785,10 +789,9 @@ def run_c4(args, world, rank, local, td):
 def run_reference_c4(args, world, rank):
     if rank != 0:
         return None
-    from gat_b200 import data as D
     from oracle import pyoracle as po
 
-    la, a, lb, b = D.config4_pairs(seed=0, npairs=4096)
+    la, a, lb, b = po.config4_pairs(seed=0, npairs=4096)
     n = len(la)
     oa = np.zeros(n, np.int64)
     ob = np.zeros(n, np.int64)
@@ -928,12 +931,9 @@ def run_c5(args, world, rank, local, td):
     (continuous batching, 4 lanes, 40 GiB budget). First a burst of all requests gives the
     saturation throughput; then three offered loads (fractions of it) give the achieved
     throughput and p50/p99 latency (arrival to completion, host clock)."""
-    import threading
-
     import torch
 
     import gat_b200 as G
-    from gat_b200 import _lib as L
     from gat_b200 import data as D
 
     dev = torch.device("cuda", local)
@@ -946,7 +946,45 @@ def run_c5(args, world, rank, local, td):
     stig = G.STIG(ctx, db, C3["stig_block"])
     fsg = G.FSG(ctx, db, G.BOX, C3["cell"])
     log("c5 set and indexes", t.n, round(time.time() - t0, 1))
+    clocks = ClockSampler(local)
+    r = served_mix(ctx, grid, stig, fsg, args.c5_requests, args.warmup, rank, clocks)
+    if rank != 0:
+        ctx.close()
+        return None
+    top = r["loads"][-1]
     n = args.c5_requests
+    line = base_line(args, world, "served mixed requests/s (continuous batching; 70% range / 30% top-k)", "requests/s",
+                     top["achieved_per_s"] * world, 1e3 * n / max(top["achieved_per_s"], 1e-9) * args.steps,
+                     {"workload": f"C5 served mix: {t.n} walks U[50,350] resident with GT-quadtree (cell 0.001, leaf 512), "
+                                  f"STIG (block 10240) and FSG (cell 0.001); {n} requests per load: 70% range "
+                                  "(log-U[0.001,0.05] deg rectangles over the three indexes, id sets), 30% top-k "
+                                  "(query lengths log-U[16,2048], k U[8,64], eps 5e-4); open-loop Poisson arrivals",
+                      "server": r["server"], "l2": "inputs (3.2 GB per index) larger than L2",
+                      "parallelism": f"replicas x{world}"})
+    line.update({
+        "e2e": {"value": round(top["achieved_per_s"] * world, 1), "unit": "requests/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": int(top["result_entries"] * 4 * 2),
+                "timer": "host clock from each request's submission to its completion (the serving path is end to end)"},
+        "saturation": r["saturation"],
+        "loads": r["loads"],
+        "server_stats": r["server_stats"],
+        "results_equal_direct_calls": r["results_equal_direct_calls"],
+        "clocks": r["clocks"],
+    })
+    ctx.close()
+    return line
+
+
+def served_mix(ctx, grid, stig, fsg, n, warmup, rank, clocks):
+    """The C5 measurement on indexes already resident: n requests (70% range over the three
+    indexes, 30% top-k) through a G.Server; a burst for the saturation rate, then the offered
+    loads of C5['loads'] (fractions of it), then a sample of requests against the direct calls."""
+    import threading
+
+    import gat_b200 as G
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
     rng = np.random.default_rng(500 + rank)
     is_range = rng.random(n) < C5["range_frac"]
     ikind = rng.integers(0, 3, n)
@@ -1008,9 +1046,8 @@ def run_c5(args, world, rank, local, td):
                 "topk_p50_ms": pct(lat[~rg], 50), "topk_p99_ms": pct(lat[~rg], 99), "result_entries": entries}
 
     # warm-up: every lane sees both request kinds (first launches tune the EDR tiles)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         run(np.arange(0, min(n, 400)))
-    clocks = ClockSampler(local)
     clocks.start()
     allidx = np.arange(n)
     times, entries = run(allidx)
@@ -1042,32 +1079,10 @@ def run_c5(args, world, rank, local, td):
             ok &= bool(np.array_equal(got[0], wi[0]) and np.array_equal(got[1], wd[0]))
         srv.release(r)
     srv.close()
-    if rank != 0:
-        ctx.close()
-        return None
-    top = loads[-1]
-    h2d = int(sum(32 if is_range[i] else 8 * qlen[i] + 16 for i in range(n)))
-    line = base_line(args, world, "served mixed requests/s (continuous batching; 70% range / 30% top-k)", "requests/s",
-                     top["achieved_per_s"] * world, 1e3 * n / max(top["achieved_per_s"], 1e-9) * args.steps,
-                     {"workload": f"C5 served mix: {t.n} walks U[50,350] resident with GT-quadtree (cell 0.001, leaf 512), "
-                                  f"STIG (block 10240) and FSG (cell 0.001); {n} requests per load: 70% range "
-                                  "(log-U[0.001,0.05] deg rectangles over the three indexes, id sets), 30% top-k "
-                                  "(query lengths log-U[16,2048], k U[8,64], eps 5e-4); open-loop Poisson arrivals",
-                      "server": {"lanes": C5["lanes"], "budget_bytes": C5["budget"], "max_range_batch": 4096,
-                                 "max_topk_batch": 32},
-                      "l2": "inputs (3.2 GB per index) larger than L2", "parallelism": f"replicas x{world}"})
-    line.update({
-        "e2e": {"value": round(top["achieved_per_s"] * world, 1), "unit": "requests/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": int(top["result_entries"] * 4 * 2),
-                "timer": "host clock from each request's submission to its completion (the serving path is end to end)"},
-        "saturation": sat,
-        "loads": loads,
-        "server_stats": st,
-        "results_equal_direct_calls": ok,
-        "clocks": clk,
-    })
-    ctx.close()
-    return line
+    return {"saturation": sat, "loads": loads, "server_stats": st, "results_equal_direct_calls": ok, "clocks": clk,
+            "checked_requests": int(len(chk)),
+            "h2d": int(sum(32 if is_range[i] else 8 * qlen[i] + 16 for i in range(n))),
+            "server": {"lanes": C5["lanes"], "budget_bytes": C5["budget"], "max_range_batch": 4096, "max_topk_batch": 32}}
 
 
 # ---------------------------------------------------------------- workload: index builds
@@ -1098,13 +1113,12 @@ def build_roofline(st):
 def build_reference_sample():
     """The reference's own Grid::addDatasetToGrid and FSG::addDatasetToGrid over the first
     BUILD['ref_n'] trajectories of the set: (points placed per second over both builds, seconds)."""
-    from gat_b200 import data as D
     from oracle import pyoracle as po
 
-    t, _ = D.config3(seed=0, n=BUILD["ref_n"], nq=1)
+    t, _ = po.config3(seed=0, n=BUILD["ref_n"], nq=1)
     R = po.RefRunner()
-    r = R.gtq(t, np.zeros((0, 4), np.float32), D.BOX, BUILD["cell"], BUILD["leaf_cap"])
-    f = R.fsg(t, D.BOX, BUILD["cell"])
+    r = R.gtq(t, np.zeros((0, 4), np.float32), po.BOX, BUILD["cell"], BUILD["leaf_cap"])
+    f = R.fsg(t, po.BOX, BUILD["cell"])
     sec = float(r["t_build"][0]) + float(f["t_build"][0])
     return 2 * len(t.lon) / sec, sec, len(t.lon)
 
@@ -1226,8 +1240,356 @@ def run_reference_build(args, world, rank):
     return line
 
 
-WORKLOADS = {"c1": run_c1, "c2": None, "c3": run_c3, "c4": run_c4, "c4k": run_c4k, "c5": run_c5, "build": run_build}
-REFERENCE = {"c1": run_reference_c1, "c2": None, "c4": run_reference_c4, "build": run_reference_build}
+# ---------------------------------------------------------------- workload: the range and EDR suite (default)
+SUITE = dict(n=1_000_000, nq=100_000, cell=0.001, vparam=2, leaf_cap=512, stig_block=10240, plain_queries=2000,
+             parity_queries=1000, pairs=4096, eps=5e-4, c5_requests=2000, ref_per_step=2000, ref_pair_every=32)
+SUITE_METRIC = "range queries/s & EDR GCUPS, batched vs plain, 1 B200, bit-exact; p50/p99 ms"
+
+
+def host_cpu() -> tuple[int, str]:
+    """(host cores this process may run on, CPU model name)."""
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        cores = os.cpu_count() or 1
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return cores, model
+
+
+def suite_config(world: int, n: int) -> dict:
+    """The configuration both arms print (the reference arm times the same workload on the host)."""
+    return {"workload": f"C3 batched range queries over the GT-quadtree, STIG and FSG: {n} random walks U[50,350] "
+                        "points, 100k rectangles with log-U[0.001,0.05] deg sides, cell 0.001 deg, leaf cap 512, STIG "
+                        "block 10240, trajectory-id sets; value = GT-quadtree batched queries/s. Beside it: the plain "
+                        "form (one query per launch sequence), C4 batched EDR (4096 pairs, both sides log-U[16,4096], "
+                        "eps 5e-4 deg) and its plain form (one pair per launch), and the C5 served mix (p50/p99)",
+            "l2": "flushed between steps (256 MiB write); point arrays 3.2 GB per index",
+            "parallelism": f"replicas x{world}"}
+
+
+def sample_rows(off: np.ndarray, vals: np.ndarray, rows: np.ndarray):
+    """CSR rows `rows` of (off, vals) as a new CSR."""
+    counts = off[rows + 1] - off[rows]
+    o = np.zeros(len(rows) + 1, np.int64)
+    np.cumsum(counts, out=o[1:])
+    v = np.concatenate([vals[off[r]:off[r + 1]] for r in rows]) if len(rows) else np.zeros(0, vals.dtype)
+    return o, v
+
+
+def oracle_range_parallel(o, q, threads: int):
+    """The oracle's id sets for q on `threads` host threads (query slices); (off, ids, seconds)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    nq = len(q)
+    per = max(1, (nq + threads - 1) // threads)
+    slices = [(s, min(nq, s + per)) for s in range(0, nq, per)]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        parts = list(ex.map(lambda se: o.range(q[se[0]:se[1]]), slices))
+    sec = time.perf_counter() - t0
+    counts = np.concatenate([np.diff(p[0]) for p in parts])
+    off = np.zeros(nq + 1, np.int64)
+    np.cumsum(counts, out=off[1:])
+    return off, np.concatenate([p[1] for p in parts]), sec
+
+
+def run_suite(args, world, rank, local, td):
+    """Config 3 batched range queries (the line's value) with their plain form, config 4 batched and
+    plain EDR, and the config 5 served mix, on one resident 1M-walk set and its three indexes."""
+    import ctypes as C
+
+    import torch
+
+    import gat_b200 as G
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    n, nq = args.c3_n, SUITE["nq"]
+    t, q = D.config3(seed=0, n=n, nq=nq)
+    if rank > 0:  # replicas: each rank its own rectangles over the same set
+        q = D.boxes(nq, L.GAT_SIDE_LOGUNIFORM, 0.001, 0.05, 1000 + rank)
+    log("suite data", t.n, len(t.lon), round(time.time() - t0, 1))
+    ctx = G.Context(local)
+    db = G.TrajectorySet(ctx, t)
+    t0 = time.time()
+    idx = {"grid": G.Grid(ctx, db, G.BOX, SUITE["cell"], SUITE["vparam"], SUITE["leaf_cap"]),
+           "fsg": G.FSG(ctx, db, G.BOX, SUITE["cell"])}
+    log("grid + fsg built", round(time.time() - t0, 1))
+    t0 = time.time()
+    idx["stig"] = G.STIG(ctx, db, SUITE["stig_block"])
+    log("stig built", round(time.time() - t0, 1))
+    H = Harness(ctx, dev)
+    cap = 64 * 1024 * 1024
+    d_q = torch.from_numpy(q).to(dev)
+    d_off = torch.empty(nq + 1, dtype=torch.int64, device=dev)
+    d_tid = torch.empty(cap, dtype=torch.int32, device=dev)
+    need = C.c_int64(0)
+
+    def call(ix, dq=d_q, m=nq, execution=L.GAT_EXEC_BATCHED):
+        ctx.check(L.lib.gat_range_query_dev(ctx.h, ix.h, dq.data_ptr(), m, L.GAT_RESULT_IDS, execution, d_off.data_ptr(),
+                                            d_tid.data_ptr(), None, cap, C.byref(need)), "gat_range_query_dev")
+
+    # ---- timed: batched range steps on each index (the GT-quadtree's are the line's value)
+    res = {}
+    clk = None
+    for name in ("grid", "fsg", "stig"):
+        ix = idx[name]
+        for _ in range(args.warmup):
+            H.time(lambda: call(ix))
+        ctx.set_timing(True)
+        l0 = ctx.launches
+        clocks = ClockSampler(local)
+        barrier(td, dev)
+        clocks.start()
+        ms = [H.time(lambda: call(ix)) for _ in range(args.steps)]
+        c = clocks.stop()
+        st = ctx.kernel_stats(L.GAT_KERNEL_RANGE_SCAN)
+        ctx.set_timing(False)
+        res[name] = dict(ms=max_over_ranks(td, sum(ms), dev), launches=ctx.launches - l0, ids=int(need.value), scan=st)
+        if name == "grid":
+            clk = c
+        log(name, [round(x, 3) for x in ms], res[name]["ids"])
+    # ---- plain form: one query per launch sequence, on an evenly spaced sample of the rectangles
+    ps = min(nq, SUITE["plain_queries"])
+    sel = np.arange(0, nq, nq // ps)[:ps]
+    d_qs = d_q[torch.from_numpy(sel).to(dev)].contiguous()
+    H.time(lambda: call(idx["grid"], d_qs, ps, L.GAT_EXEC_PLAIN))
+    pms = [H.time(lambda: call(idx["grid"], d_qs, ps, L.GAT_EXEC_PLAIN)) for _ in range(max(1, min(args.steps, 5)))]
+    plain_off = d_off[:ps + 1].cpu().numpy()
+    plain_ids = d_tid[:int(plain_off[-1])].cpu().numpy()
+    ptot = max_over_ranks(td, sum(pms), dev)
+    plain_qps = ps * world * len(pms) / (ptot / 1e3)
+    # ---- end to end through the host-buffer call (pinned host rectangles in, id sets out)
+    h_q = torch.from_numpy(q).pin_memory()
+    h_off = torch.empty(nq + 1, dtype=torch.int64).pin_memory()
+    h_tid = torch.empty(cap, dtype=torch.int32).pin_memory()
+
+    def call_e2e():
+        ctx.check(L.lib.gat_range_query(ctx.h, idx["grid"].h, h_q.data_ptr(), nq, L.GAT_RESULT_IDS, L.GAT_EXEC_BATCHED,
+                                        h_off.numpy().ctypes.data_as(L.P_i64), h_tid.numpy().ctypes.data_as(L.P_i32), None,
+                                        cap, C.byref(need)), "gat_range_query")
+
+    H.time(call_e2e)
+    ems = [H.time(call_e2e) for _ in range(args.steps)]
+    etot = max_over_ranks(td, sum(ems), dev)
+    grid_off = h_off.numpy().copy()
+    grid_ids = h_tid.numpy()[:int(grid_off[-1])].copy()
+    # FSG id sets of the parity sample
+    pq = min(nq, SUITE["parity_queries"])
+    psel = np.arange(0, nq, nq // pq)[:pq]
+    fsg_r = idx["fsg"].range_query(q[psel])
+    # ---- config 4: batched EDR pairs and their plain form
+    edr = measure_edr_pairs(ctx, H, args, td, rank, local, dev)
+    # ---- config 5: served mix on the same resident set
+    c5 = served_mix(ctx, idx["grid"], idx["stig"], idx["fsg"], args.c5_requests, min(args.warmup, 3), rank,
+                    ClockSampler(local))
+    if rank != 0:
+        ctx.close()
+        return None
+    g = res["grid"]
+    value = nq * world * args.steps / (g["ms"] / 1e3)
+    line = base_line(args, world, SUITE_METRIC, "queries/s", value, g["ms"], suite_config(world, t.n))
+    line.update({
+        "e2e": {"value": round(nq * world * args.steps / (etot / 1e3), 3), "unit": "queries/s",
+                "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int((nq + 1) * 8 + len(grid_ids) * 4),
+                "call": "gat_range_query (pinned host rectangles in, CSR id sets out), GT-quadtree, batched"},
+        "gpu_launches": int(g["launches"]),
+        "roofline": range_roofline(g["scan"], "k_range_hash"),
+        "clocks": clk,
+        "range": {
+            "indexes": {k: {"queries_per_s": round(nq * world * args.steps / (v["ms"] / 1e3), 1), "result_ids": v["ids"],
+                            "ms_per_step": round(v["ms"] / args.steps, 4),
+                            "roofline": range_roofline(v["scan"], "k_range_hash")} for k, v in res.items()},
+            "plain": {"queries": ps, "steps": len(pms), "queries_per_s": round(plain_qps, 1),
+                      "form": "gat_range_query_dev with GAT_EXEC_PLAIN: one query per launch sequence",
+                      "sample": f"every {nq // ps}th of the 100k rectangles"},
+            "batched_over_plain": round(value / plain_qps, 1),
+        },
+        "edr": edr,
+        "served": {"requests_per_load": args.c5_requests, "saturation": c5["saturation"], "loads": c5["loads"],
+                   "server": c5["server"], "server_stats": c5["server_stats"],
+                   "results_equal_direct_calls": c5["results_equal_direct_calls"], "clocks": c5["clocks"]},
+    })
+    # ---- parity against the oracle and the CPU baseline (rank 0, one GPU)
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import pyoracle as po
+
+        cores, model = host_cpu()
+        t0 = time.time()
+        og = po.OracleGrid(t, G.BOX, SUITE["cell"], SUITE["vparam"], SUITE["leaf_cap"])
+        of = po.OracleFSG(t, G.BOX, SUITE["cell"])
+        log("oracle grid + fsg built", round(time.time() - t0, 1))
+        o_off, o_ids, sec = oracle_range_parallel(og, q[psel], cores)
+        g_off, g_ids = sample_rows(grid_off, grid_ids, psel)
+        f_off, f_ids = of.range(q[psel])
+        p_off, p_ids = sample_rows(plain_off, plain_ids, np.arange(0, ps, max(1, ps // pq))[:pq])
+        po_off, po_ids = og.range(q[sel][np.arange(0, ps, max(1, ps // pq))[:pq]])
+        checks = {"grid_batched": bool(np.array_equal(g_off, o_off) and np.array_equal(g_ids, o_ids)),
+                  "fsg_batched": bool(np.array_equal(fsg_r.offsets, f_off) and np.array_equal(fsg_r.tids, f_ids)),
+                  "grid_plain": bool(np.array_equal(p_off, po_off) and np.array_equal(p_ids, po_ids)),
+                  "edr_batched": edr.pop("_parity_ok")}
+        line["parity"] = {"checked": {"range_queries": int(pq), "edr_pairs": int(edr["pairs"])},
+                          "against": "oracle restatement (pinned to the reference's compiled CPU code by the CPU tests)",
+                          "stig": "checked against the oracle by tests/test_gpu_configs.py (its oracle build takes minutes)",
+                          "cases": checks, "equal": all(checks.values())}
+        line["cpu_baseline"] = {"value": round(pq / sec, 1), "unit": "queries/s", "cores": cores, "cpu": model,
+                                "kind": "port",
+                                "sample": f"{pq} of the 100k rectangles (every {nq // pq}th), the oracle's GT-quadtree "
+                                          f"range query on {cores} threads (query slices)"}
+        line["edr"]["cpu_baseline"]["cpu"] = model
+    else:
+        edr.pop("_parity_ok", None)
+    ctx.close()
+    return line
+
+
+def measure_edr_pairs(ctx, H, args, td, rank, local, dev):
+    """Config 4: 4096 pairs, both lengths log-U[16, 4096], eps 5e-4. Batched (one launch for all
+    pairs) timed steps with the tile kernel's own event time; plain (one pair per launch); the
+    oracle's distances on every pair as the parity check and the CPU baseline (rank 0)."""
+    import torch
+
+    import gat_b200.api as A
+    from gat_b200 import _lib as L
+    from gat_b200 import data as D
+
+    la, a, lb, b = D.config4_pairs(seed=rank, npairs=SUITE["pairs"])
+    n = len(la)
+    cells = float(np.sum(la.astype(np.float64) * lb.astype(np.float64)))
+    oa = np.zeros(n, np.int64)
+    ob = np.zeros(n, np.int64)
+    oa[1:] = np.cumsum(la)[:-1]
+    ob[1:] = np.cumsum(lb)[:-1]
+    T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    d_la, d_oa, d_a, d_lb, d_ob, d_b = T(la.astype(np.int32)), T(oa), T(a), T(lb.astype(np.int32)), T(ob), T(b)
+    d_out = torch.empty(n, dtype=torch.int32, device=dev)
+    eps = SUITE["eps"]
+
+    def call(lo=0, hi=n):
+        ctx.check(L.lib.gat_edr_pairs_dev(ctx.h, hi - lo, d_la.data_ptr() + 4 * lo, d_oa.data_ptr() + 8 * lo, d_a.data_ptr(),
+                                          d_lb.data_ptr() + 4 * lo, d_ob.data_ptr() + 8 * lo, d_b.data_ptr(), eps,
+                                          d_out.data_ptr() + 4 * lo), "gat_edr_pairs_dev")
+
+    for _ in range(args.warmup):
+        H.time(call)
+    ctx.set_timing(True)
+    l0 = ctx.launches
+    clocks = ClockSampler(local)
+    barrier(td, dev)
+    clocks.start()
+    ms = [H.time(call) for _ in range(args.steps)]
+    clk = clocks.stop()
+    st = ctx.kernel_stats(L.GAT_KERNEL_EDR)
+    st["work"] = cells * args.steps
+    ctx.set_timing(False)
+    launches = ctx.launches - l0
+    tot = max_over_ranks(td, sum(ms), dev)
+    got = d_out.cpu().numpy().copy()
+
+    def plain():
+        for i in range(n):
+            call(i, i + 1)
+
+    H.time(lambda: [call(i, i + 1) for i in range(0, n, 64)])  # warm the one-pair shape class
+    pms = [H.time(plain)]
+    ptot = max_over_ranks(td, sum(pms), dev)
+    plain_ok = bool(np.array_equal(d_out.cpu().numpy(), got))
+    ems = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_out = A.edr_pairs(ctx, la, a, lb, b, eps)
+        ems.append((time.perf_counter() - t0) * 1e3)
+    etot = max_over_ranks(td, sum(ems), dev)
+    gcups = cells * args.steps / (tot / 1e3) / 1e9
+    pg = cells / (ptot / 1e3) / 1e9
+    out = {"workload": f"{n} pairs, both lengths log-U[16,4096], eps 5e-4 deg, {cells:.4g} DP cells per step",
+           "batched": {"gcups": round(gcups, 3), "ms_per_step": round(tot / args.steps, 4), "gpu_launches": int(launches)},
+           "plain": {"gcups": round(pg, 3), "ms_per_step": round(ptot, 3), "form": "one pair per gat_edr_pairs_dev call",
+                     "results_equal_batched": plain_ok},
+           "batched_over_plain": round(gcups / pg, 1),
+           "e2e": {"gcups": round(cells * args.steps / (etot / 1e3) / 1e9, 3), "timer": "host clock around gat_edr_pairs "
+                   "(synchronous; host arrays in, distances out)", "h2d_bytes_per_step": int(a.nbytes + b.nbytes + 24 * n),
+                   "d2h_bytes_per_step": int(4 * n), "results_equal_batched": bool(np.array_equal(e2e_out, got))},
+           "roofline": edr_roofline(st, clk),
+           "clocks": clk, "pairs": n, "_parity_ok": True}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import pyoracle as po
+
+        cores, _ = host_cpu()
+        t0 = time.perf_counter()
+        want = po.edr_batch(la, a, lb, b, eps, threads=cores)
+        sec = time.perf_counter() - t0
+        out["_parity_ok"] = bool(np.array_equal(want, got))
+        out["cpu_baseline"] = {"value": round(cells / sec / 1e9, 4), "unit": "GCUPS", "cores": cores, "kind": "port",
+                               "sample": f"all {n} pairs, the oracle's EDR on {cores} threads"}
+    return out
+
+
+def run_reference_suite(args, world, rank):
+    """The reference's own CPU code on the suite's workload (rank 0): gatref rangebench builds the
+    reference's Grid over the same generated set and times Grid::rangeQueryBatch on strided samples
+    of the same rectangles on every host core; gatref edr times Grid::SimilarityExecuter on a
+    sample of the config 4 pairs. No part of this library is loaded."""
+    if rank != 0:
+        return None
+    from oracle import pyoracle as po
+
+    cores, model = host_cpu()
+    n, nq = args.c3_n, SUITE["nq"]
+    cfg = suite_config(world, n)
+    if not po.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/gatref (the reference's CPU code compiled from its "
+                "sources) was not built in this tree", "config": cfg}
+    steps = args.warmup + args.steps
+    per_step = min(SUITE["ref_per_step"], nq // steps)
+    R = po.RefRunner()
+    t0 = time.time()
+    r = R.rangebench(n, 50, 350, 0, nq, 0.001, 0.05, SUITE["cell"], SUITE["leaf_cap"], po.BOX, per_step, steps, cores)
+    log("reference rangebench", round(time.time() - t0, 1), "build", float(r["t_build"][0]))
+    ts = [float(x) for x in r["t_step"][args.warmup:]]
+    sec = sum(ts)
+    value = per_step * args.steps / sec
+    la, a, lb, b = po.config4_pairs(seed=0, npairs=SUITE["pairs"])
+    sel = np.arange(0, len(la), SUITE["ref_pair_every"])
+    oa = np.concatenate([[0], np.cumsum(la)]).astype(np.int64)
+    ob = np.concatenate([[0], np.cumsum(lb)]).astype(np.int64)
+    sa = np.concatenate([a[oa[i]:oa[i + 1]] for i in sel])
+    sb = np.concatenate([b[ob[i]:ob[i + 1]] for i in sel])
+    sc = float(np.sum(la[sel].astype(np.float64) * lb[sel]))
+    e = R.edr(la[sel], sa, lb[sel], sb, SUITE["eps"], threads=cores)
+    edr_gcups = sc / float(e["t_query"][0]) / 1e9
+    line = base_line(args, world, SUITE_METRIC, "queries/s", value, sec * 1e3, cfg)
+    line.update({
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 3), "unit": "queries/s", "cores": cores, "cpu": model, "kind": "reference",
+                         "sample": f"per step {per_step} of the 100k rectangles (every {nq // per_step}th, a different "
+                                   f"offset each step), Grid::rangeQueryBatch on {cores} threads (query slices), over "
+                                   f"the reference's Grid of the same {n} walks (built in {float(r['t_build'][0]):.1f} s)"},
+        "e2e": {"value": round(value, 3), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "result_ids_per_step": int(np.mean(r["ids_step"][args.warmup:])),
+        "edr": {"gcups": round(edr_gcups, 4), "unit": "GCUPS", "cores": cores,
+                "sample": f"{len(sel)} of the {len(la)} config 4 pairs (every {SUITE['ref_pair_every']}th), "
+                          f"Grid::SimilarityExecuter on {cores} threads"},
+        "served": {"unavailable": "the reference has no serving loop"},
+    })
+    return line
+
+
+WORKLOADS = {"suite": run_suite, "c1": run_c1, "c2": run_c2, "c3": run_c3, "c4": run_c4, "c4k": run_c4k, "c5": run_c5,
+             "build": run_build}
+REFERENCE = {"suite": run_reference_suite, "c1": run_reference_c1, "c2": run_reference_c2, "c4": run_reference_c4,
+             "build": run_reference_build}
 
 
 def main():
@@ -1236,7 +1598,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c4k", "c5", "build"])
+    ap.add_argument("--workload", default="suite", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--queries", type=int, default=0, help="C2: use only the first N of the 256 queries")
@@ -1244,14 +1606,16 @@ def main():
     ap.add_argument("--c3-indexes", default="grid,fsg,stig")
     ap.add_argument("--c3-n", type=int, default=C3["n"])
     ap.add_argument("--c3-plain-sample", type=int, default=2000)
-    ap.add_argument("--c5-requests", type=int, default=C5["requests"])
+    ap.add_argument("--c5-requests", type=int, default=0, help="C5 requests per load (default 4000; 2000 in the suite)")
     ap.add_argument("--c4k-queries", type=int, default=C4K["nq"])
     ap.add_argument("--c4k-check", type=int, default=C4K["check"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if not args.c5_requests:
+        args.c5_requests = SUITE["c5_requests"] if args.workload == "suite" else C5["requests"]
     world, rank, local = dist_env()
     if args.impl == "reference":
-        fn = REFERENCE.get(args.workload) or run_reference_c2
+        fn = REFERENCE.get(args.workload)
         if args.workload == "c3":
             line = {"impl": "reference", "unavailable": "the reference's Grid build clears a cell-sized array per "
                     "trajectory (Grid.cpp:268-269): about 3 minutes on one core for the 1M-trajectory set before any "
@@ -1270,7 +1634,7 @@ def main():
         return
     td = init_dist(world)
     try:
-        fn = WORKLOADS.get(args.workload) or run_c2
+        fn = WORKLOADS[args.workload]
         line = fn(args, world, rank, local, td)
         if line is not None:
             print(json.dumps(line), flush=True)

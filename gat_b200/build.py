@@ -85,10 +85,15 @@ def build_library(force: bool = False, jobs: int = 8) -> str:
     return LIB
 
 
+# checkout of the reference whose CPU sources oracle/Makefile compiles into oracle/_ref/gatref
+REFERENCE_DIR = os.environ.get("GAT_REFERENCE_DIR", "/root/reference")
+
+
 def build_oracle() -> None:
     """Test oracles: oracle/liboracle.so always; oracle/_ref/gatref when the reference sources
     are present (elsewhere the prebuilt binary is kept)."""
-    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "-j8"], capture_output=True, text=True)
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "-j8", f"REF={REFERENCE_DIR}"],
+                       capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
 

@@ -313,6 +313,11 @@ int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
         ctx->dep_launch = value;
         return GAT_OK;
     }
+    if (knob == GAT_TUNE_TEST_STALL_CARRY) {
+        if (value < 0) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: stall pair must be >= 0");
+        ctx->test_stall_pair = value;
+        return GAT_OK;
+    }
     if (knob != GAT_TUNE_EDR_ROWS) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: unknown knob");
     if (value != 0 && value != 2 && value != 4 && value != 8)
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR rows per lane must be 0 (autotune), 2, 4 or 8");
@@ -339,6 +344,8 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
         *value = ctx->topk_growth;
     else if (knob == GAT_TUNE_INDEX_BUILD)
         *value = ctx->index_build;
+    else if (knob == GAT_TUNE_TEST_STALL_CARRY)
+        *value = ctx->test_stall_pair;
     else if (knob == GAT_TUNE_DEP_LAUNCH)
         *value = ctx->dep_launch;
     else

@@ -234,6 +234,8 @@ struct TileCtl {
     int stride;
     const unsigned long long* epoch; /* written by the schedule's write pass */
     int32_t* flag;
+    int spin_limit;  /* polls before a carry wait gives up (kSpinLimit) */
+    int stall_pair;  /* tests of the bounded wait: this pair's first pipelined tile writes no carries (-1: none) */
 };
 
 /* The carry word is the only datum exchanged, so neither access needs to order other memory
@@ -420,7 +422,8 @@ __device__ __forceinline__ int cf_step(const float (&bx)[R], const float (&by)[R
 template <int R, bool COL = false>
 __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const float2* __restrict__ cols, int len1,
                                          int len2, int t, const carry_t* cin, carry_t* cout, carry_t tag_in,
-                                         carry_t tag_out, float u, float2* sb, int* sc, int& result) {
+                                         carry_t tag_out, float u, float2* sb, int* sc, int& result,
+                                         int spin_limit = kSpinLimit) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const bool lane0 = lane == 0;
@@ -470,7 +473,7 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
                         ok = (nw >> 16) == tag_in;
                     }
                     if (__all_sync(FULL, ok)) break;
-                    if (polls >= kSpinLimit) return false;
+                    if (polls >= spin_limit) return false;
                     if (polls >= 16) __nanosleep(64); /* each poll is an L2 round trip already */
                 }
                 cv = (int)(short)(nw & 0xffffu);
@@ -581,13 +584,14 @@ __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(S
             for (int tt = 0; tt < T && ok; tt++)
                 ok = edr_tile<R, COL>(lpts, spts, nlane, nstep, tt, tt > 0 ? ((tt - 1) & 1 ? wc1 : wc0) : nullptr,
                                       tt + 1 < T ? ((tt & 1) ? wc1 : wc0) : nullptr, ep | ((tt - 1) & 0xff),
-                                      ep | (tt & 0xff), u, bring[wib], cring[wib], result);
+                                      ep | (tt & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit);
             finished = true;
         } else {
             carry_t* pc = ctl.pair_carry + (size_t)it.z * 2 * ctl.stride;
+            const bool stalled = p == ctl.stall_pair && t == 0;
             ok = edr_tile<R, COL>(lpts, spts, nlane, nstep, t, t > 0 ? pc + ((t - 1) & 1) * ctl.stride : nullptr,
-                                  t + 1 < T ? pc + (t & 1) * ctl.stride : nullptr, ep | ((t - 1) & 0xff),
-                                  ep | (t & 0xff), u, bring[wib], cring[wib], result);
+                                  t + 1 < T && !stalled ? pc + (t & 1) * ctl.stride : nullptr, ep | ((t - 1) & 0xff),
+                                  ep | (t & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit);
             finished = t == T - 1;
         }
         if (!ok) {
@@ -642,8 +646,10 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     count_launch(ctx);
     (void)launch_dep(ctx, k_sched_write<Src>, dim3(pgrid), dim3(256), 0, s, src, (int)cap, ctr, meta, items, edr_epochs(ctx));
     count_launch(ctx);
+    /* the stall knob (tests of the bounded wait) also shortens the wait to ~2^12 polls */
+    const int stall = ctx->test_stall_pair - 1;
     TileCtl ctl{items, ctr + 2, pcarry, wcarry, stride, reinterpret_cast<const unsigned long long*>(ctr + kCtrEpoch),
-                ctx->d_flag};
+                ctx->d_flag, stall >= 0 ? (1 << 12) : kSpinLimit, stall};
     timed_begin(ctx, GAT_KERNEL_EDR);
     if (ev0) cudaEventRecord(ev0, s);
     (void)launch_dep(ctx, k_edr_tiles<R, COL, Src>, dim3(grid), dim3(kTileWarps * 32), 0, s, src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);

@@ -8,11 +8,12 @@
  * of one 256-row tile to the next, plus a work counter) lives in the file-scope device array
  * below. Its size is fixed: kMaxLen points per trajectory side, kWarps resident warps.
  *
- * Every GPU that loads the library holds the array until the process exits. Every call uses the
- * same array: calls that overlap on the GPU (on different streams, or from several host threads)
- * race on it and must be serialised by the caller. The work counter is cleared at the start of
- * each call; the carry rows need no clearing (each tile reads only rows its predecessor wrote
- * in the same call).
+ * With CUDA's lazy module loading (the default), the first call on a device loads this file's
+ * module there, and that reserves the array on that device until the process exits; later calls
+ * allocate nothing. Every call uses the same array: calls that overlap on the GPU (on different
+ * streams, or from several host threads) race on it and must be serialised by the caller. The
+ * work counter is cleared at the start of each call; the carry rows need no clearing (each tile
+ * reads only rows its predecessor wrote in the same call).
  */
 #include <mutex>
 
@@ -66,16 +67,25 @@ struct NoAllocPairs {
 std::mutex g_setup_mu;
 int* g_scratch_addr[64] = {nullptr};
 
-/* Device address of the scratch array for the current device, looked up once per device
- * (cudaGetSymbolAddress with that device current). */
-int scratch_address(int** out) {
+/* Device address of the scratch array on the current device. Host code cannot use the array's
+ * name as an address (it names a host-side shadow), so the address comes from
+ * cudaGetSymbolAddress with the device current. Outside a stream capture it is looked up again
+ * on every call (cheap), so the address stays right after a cudaDeviceReset or a re-created
+ * primary context; inside a capture the address of the last call outside one is used, and a
+ * device that has never seen such a call gets GAT_ERR_STATE. */
+int scratch_address(cudaStream_t s, int** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
         return GAT_ERR_CUDA;
     }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return GAT_ERR_CUDA;
+    }
     std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -84,6 +94,7 @@ int scratch_address(int** out) {
         }
         g_scratch_addr[dev] = static_cast<int*>(p);
     }
+    if (!g_scratch_addr[dev]) return GAT_ERR_STATE;
     *out = g_scratch_addr[dev];
     return GAT_OK;
 }
@@ -100,10 +111,10 @@ extern "C" int gat_edr_pairs_dev_noalloc(void* stream, int npairs, int max_len, 
     if (max_len < 1 || max_len > kMaxLen) return GAT_ERR_ARG; /* beyond the fixed scratch */
     if (npairs == 0) return GAT_OK;
     if (!d_q_len || !d_q_off || !d_q_xy || !d_c_len || !d_c_off || !d_c_xy || !d_out) return GAT_ERR_ARG;
-    int* scratch = nullptr;
-    int rc = scratch_address(&scratch);
-    if (rc != GAT_OK) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int* scratch = nullptr;
+    int rc = scratch_address(s, &scratch);
+    if (rc != GAT_OK) return rc;
     unsigned* work = reinterpret_cast<unsigned*>(scratch + kCarryInts);
     if (cudaMemsetAsync(work, 0, sizeof(unsigned), s) != cudaSuccess) {
         cudaGetLastError();

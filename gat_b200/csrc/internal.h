@@ -99,6 +99,7 @@ struct gat_ctx {
     int topk_chunk = 0, topk_growth = 0; /* 0 = defaults */
     int index_build = 0;                 /* 0 = device when present, 1 = host, 2 = device */
     int dep_launch = 1;                  /* programmatic dependent launch on the query path */
+    int test_stall_pair = 0;             /* GAT_TUNE_TEST_STALL_CARRY (tests of the bounded wait) */
     cudaMemPool_t build_pool = nullptr;  /* index-build temporaries, kept for reuse until gat_ctx_trim */
     std::map<uint64_t, int> edr_tune; /* worker contexts use their root's table */
     std::mutex tune_mu;

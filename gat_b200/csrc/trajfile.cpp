@@ -77,6 +77,8 @@ bool parse_double(const char*& p, const char* e, double* v) {
         neg = *q == '-';
         q++;
     }
+    /* strtod takes one sign; from_chars would accept a second '-' after the one stripped here */
+    if (q < e && (*q == '+' || *q == '-')) return false;
     if (q + 1 < e && q[0] == '0' && (q[1] == 'x' || q[1] == 'X')) {
         /* hexadecimal: strtod itself, on a terminated copy of the token */
         const char* t = q;

@@ -115,9 +115,14 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  *   host (its median splits follow std::sort's order among equal coordinates).
  * GAT_TUNE_DEP_LAUNCH: 1 (default) launches the kernels of the top-k and EDR paths as
  *   programmatic dependent launches (each kernel is set up while the one before it drains; the
- *   order of their work is unchanged), 0 launches them plainly. Same results. */
+ *   order of their work is unchanged), 0 launches them plainly. Same results.
+ * GAT_TUNE_TEST_STALL_CARRY: for tests of the bounded wait between pipelined EDR tiles, never
+ *   for production. v > 0 makes the first tile of pair v - 1 of every later pipelined launch
+ *   skip its carry stores and shortens each wait to about 4096 polls, so the next tile of that
+ *   pair gives up: the pair gets -1, the call returns GAT_ERR_TIMEOUT, every other pair keeps
+ *   its exact distance and the context stays usable. 0 (default) turns it off. */
 enum { GAT_TUNE_EDR_ROWS = 1, GAT_TUNE_EDR_TUNED = 2, GAT_TUNE_TOPK_CHUNK = 3, GAT_TUNE_TOPK_GROWTH = 4,
-       GAT_TUNE_EDR_FORM = 5, GAT_TUNE_INDEX_BUILD = 6, GAT_TUNE_DEP_LAUNCH = 7 };
+       GAT_TUNE_EDR_FORM = 5, GAT_TUNE_INDEX_BUILD = 6, GAT_TUNE_DEP_LAUNCH = 7, GAT_TUNE_TEST_STALL_CARRY = 8 };
 int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value);
 int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value);
 
@@ -187,13 +192,18 @@ int gat_edr_pairs_dev(gat_ctx* ctx, int npairs, const int32_t* d_q_len, const in
                       const float* d_q_xy, const int32_t* d_c_len, const int64_t* d_c_off,
                       const float* d_c_xy, double eps, int32_t* d_out);
 /* gat_edr_pairs_dev without any allocation (no counterpart in the reference). For callers that
- * cannot call cudaMalloc (inside someone else's graph capture, under a no-allocation policy, or
- * with a fixed device footprint): no context, only the caller's stream and device arrays. The
- * kernel's working memory is a file-scope device array of fixed size (16.8 MB, held by every GPU
- * that loads the library until exit), which bounds every trajectory side to
- * GAT_EDR_NOALLOC_MAX_LEN points: max_len (the longest side the caller passes, host value) above
- * it returns GAT_ERR_ARG, and a pair whose side exceeds max_len gets -1. The first call on a
- * device looks the array up (cudaGetSymbolAddress) and should come before any stream capture.
+ * cannot call cudaMalloc: code running inside a CUDA-graph capture that someone else owns (an
+ * allocation there fails or ends up in their graph), runtimes and allocators that forbid device
+ * allocations, and programs that must keep a fixed device footprint. There is no context: the
+ * caller passes a stream and device arrays. The kernel's working memory is a file-scope device
+ * array of fixed size (16.8 MB), which bounds every trajectory side to GAT_EDR_NOALLOC_MAX_LEN
+ * points: max_len (the longest side the caller passes, a host value) above it returns
+ * GAT_ERR_ARG, and a pair whose side exceeds max_len gets -1. With CUDA's default lazy module
+ * loading, the first call on each device loads the module holding the array, which reserves the
+ * 16.8 MB there until the process exits: make that first call outside any capture or
+ * no-allocation region; later calls allocate nothing. A call outside a capture looks the
+ * array's address up again, so a cudaDeviceReset between calls is harmless; a call inside a
+ * capture uses the address of the last call outside one (GAT_ERR_STATE before any).
  * Asynchronous on `stream`; calls that overlap on the GPU share the array and race, so the
  * caller serialises them. */
 #define GAT_EDR_NOALLOC_MAX_LEN 4096

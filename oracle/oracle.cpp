@@ -382,7 +382,7 @@ struct orc_stig {
     static bool cmp_x(const P& a, const P& b) { return a.x < b.x; }
     static bool cmp_y(const P& a, const P& b) { return a.y < b.y; }
 
-    int make_leaf(int depth, int s, int e) {
+    Node make_leaf(int depth, int s, int e) const {
         /* STIG::createIndex(LeafNode*) (STIG.cpp:71-93) */
         float xmin = 999, xmax = -999, ymin = 999, ymax = -999;
         for (int i = s; i <= e; i++) {
@@ -397,35 +397,56 @@ struct orc_stig {
         nd.l = s;
         nd.r = e;
         nd.mbb = Box{xmin, ymin, xmax, ymax};
-        nodes.push_back(nd);
-        return (int)nodes.size() - 1;
+        return nd;
     }
-    int make_internal(int depth, int s, int e) {
-        /* STIG::createIndex(InternalNode*) (STIG.cpp:96-168): std::sort over [s, e), the last
-         * element excluded; left child [s, m] as a leaf or [s, m-1] as an inner node, right [m, e] */
+    /* The subtree over [s, e] as a node list in depth-first order (its root first), children
+     * as indices into the list.
+     * STIG::createIndex(InternalNode*) (STIG.cpp:96-168): std::sort over [s, e), the last
+     * element excluded; left child [s, m] as a leaf or [s, m-1] as an inner node, right [m, e].
+     * A left leaf [s, m] shares index m with the right subtree, so its MBB is taken before the
+     * right subtree sorts, as in the reference; an inner left child [s, m-1] is disjoint from
+     * [m, e], so the two are built on separate threads for the first `spawn` levels. Every
+     * std::sort call sees the same range and contents as in the sequential order, so the
+     * result is the same. */
+    std::vector<Node> make_internal(int depth, int s, int e, int spawn) {
         if (depth % 2 == 0)
             std::sort(&pts[s], &pts[e], cmp_x);
         else
             std::sort(&pts[s], &pts[e], cmp_y);
-        int m = (s + e) / 2;
+        const int m = (s + e) / 2;
         Node nd{};
         nd.leaf = false;
         nd.depth = depth;
         nd.median = depth % 2 == 0 ? pts[m].x : pts[m].y;
-        int me = (int)nodes.size();
-        nodes.push_back(nd);
-        int lc, rc;
+        std::vector<Node> lt, rt;
+        std::thread worker;
         if (m - s <= block)
-            lc = make_leaf(depth + 1, s, m);
+            lt.push_back(make_leaf(depth + 1, s, m));
+        else if (spawn > 0)
+            worker = std::thread([&, spawn]() { lt = make_internal(depth + 1, s, m - 1, spawn - 1); });
         else
-            lc = make_internal(depth + 1, s, m - 1);
+            lt = make_internal(depth + 1, s, m - 1, 0);
         if (e - m + 1 <= block)
-            rc = make_leaf(depth + 1, m, e);
+            rt.push_back(make_leaf(depth + 1, m, e));
         else
-            rc = make_internal(depth + 1, m, e);
-        nodes[me].left = lc;
-        nodes[me].right = rc;
-        return me;
+            rt = make_internal(depth + 1, m, e, spawn > 0 ? spawn - 1 : 0);
+        if (worker.joinable()) worker.join();
+        std::vector<Node> out;
+        out.reserve(1 + lt.size() + rt.size());
+        nd.left = 1;
+        nd.right = 1 + (int)lt.size();
+        out.push_back(nd);
+        for (const auto* part : {&lt, &rt}) {
+            const int base = (int)out.size();
+            for (Node c : *part) {
+                if (!c.leaf) {
+                    c.left += base;
+                    c.right += base;
+                }
+                out.push_back(c);
+            }
+        }
+        return out;
     }
     static bool slab(float amin, float amax, float bmin, float bmax) {
         /* STIG::intersectBlock (STIG.cpp:340-347) */
@@ -467,9 +488,9 @@ extern "C" orc_stig* orc_stig_build(int n, const int32_t* lengths, const float* 
     int total = (int)s->pts.size();
     s->root_leaf = total <= block_size;
     if (s->root_leaf)
-        s->make_leaf(0, 0, total - 1);
+        s->nodes.push_back(s->make_leaf(0, 0, total - 1));
     else
-        s->make_internal(0, 0, total - 1);
+        s->nodes = s->make_internal(0, 0, total - 1, 5);
     return s;
 }
 

@@ -66,6 +66,11 @@ def lib():
             "orc_grid_query_fv": (C.c_int, [c_p, P_f32, P_f32, C.c_int, P_i32, P_i32]),
             "orc_grid_fv_lb": (None, [c_p, C.c_int, P_i32, P_i32, P_i32]),
             "orc_grid_topk": (None, [c_p, P_f32, P_f32, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, P_i32, P_i32, P_i64]),
+            "orc_gen_lengths": (None, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_uint64, P_i32]),
+            "orc_gen_walks": (None, [C.c_int, P_i32, P_f32, C.c_double, C.c_uint64, P_f32, P_f32]),
+            "orc_gen_boxes": (None, [C.c_int, C.c_int, C.c_double, C.c_double, P_f32, C.c_uint64, P_f32]),
+            "orc_gen_sample_ids": (None, [C.c_int, C.c_int, C.c_uint64, P_i32]),
+            "orc_gen_pairs": (None, [C.c_int, P_i32, P_i32, P_f32, C.c_double, C.c_double, C.c_uint64, P_f32, P_f32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -261,6 +266,97 @@ class OracleFSG(_RangeMixin):
         return c
 
 
+# ---------------------------------------------------------------- seeded workloads (oracle/datagen.cpp)
+BOX = (121.0, 30.7, 122.0, 31.7)
+STEP = 1e-4
+LEN_UNIFORM, LEN_LOGNORMAL, LEN_LOGUNIFORM = 0, 1, 2
+SIDE_FIXED, SIDE_LOGUNIFORM = 0, 1
+
+
+class Walks:
+    """A trajectory set (ids 1..n) with the attributes the oracle classes and RefRunner read."""
+
+    def __init__(self, lengths, lon, lat):
+        self.lengths, self.lon, self.lat = lengths, lon, lat
+
+    @property
+    def n(self) -> int:
+        return int(self.lengths.shape[0])
+
+    @property
+    def offsets(self):
+        off = np.zeros(self.n + 1, dtype=np.int64)
+        np.cumsum(self.lengths, out=off[1:])
+        return off
+
+    def points(self, tid: int):
+        off = self.offsets
+        return self.lon[off[tid - 1]:off[tid]], self.lat[off[tid - 1]:off[tid]]
+
+
+def gen_lengths(n, kind, p0, p1, lo, hi, seed):
+    out = np.empty(n, np.int32)
+    lib().orc_gen_lengths(n, kind, p0, p1, lo, hi, seed, _p(out, P_i32))
+    return out
+
+
+def gen_walks(lens, seed, box=BOX, step=STEP):
+    lens = _c(lens, np.int32)
+    total = int(lens.astype(np.int64).sum())
+    lon, lat = np.empty(total, np.float32), np.empty(total, np.float32)
+    b = np.asarray(box, np.float32)
+    lib().orc_gen_walks(len(lens), _p(lens, P_i32), _p(b, P_f32), step, seed, _p(lon, P_f32), _p(lat, P_f32))
+    return Walks(lens, lon, lat)
+
+
+def gen_boxes(n, kind, s0, s1, seed, box=BOX):
+    out = np.empty((n, 4), np.float32)
+    b = np.asarray(box, np.float32)
+    lib().orc_gen_boxes(n, kind, s0, s1, _p(b, P_f32), seed, _p(out, P_f32))
+    return out
+
+
+def gen_sample_ids(k, n, seed):
+    out = np.empty(k, np.int32)
+    lib().orc_gen_sample_ids(k, n, seed, _p(out, P_i32))
+    return out
+
+
+def gen_pairs(la, lb, seed, jitter=2.5e-4, box=BOX, step=STEP):
+    la, lb = _c(la, np.int32), _c(lb, np.int32)
+    a = np.empty((int(la.astype(np.int64).sum()), 2), np.float32)
+    bb = np.empty((int(lb.astype(np.int64).sum()), 2), np.float32)
+    b = np.asarray(box, np.float32)
+    lib().orc_gen_pairs(len(la), _p(la, P_i32), _p(lb, P_i32), _p(b, P_f32), step, jitter, seed, _p(a, P_f32), _p(bb, P_f32))
+    return a, bb
+
+
+def config1(seed=0, n=10_000, nq=1_000):
+    """10k walks of U[20, 200] points; nq squares of side 0.01 deg."""
+    t = gen_walks(gen_lengths(n, LEN_UNIFORM, 0, 0, 20, 200, seed), seed)
+    return t, gen_boxes(nq, SIDE_FIXED, 0.01, 0.01, seed)
+
+
+def config2(seed=0, n=100_000, nq=256):
+    """100k walks, lengths lognormal(ln 200, 0.6) clipped to [32, 1024]; nq query ids from the set."""
+    t = gen_walks(gen_lengths(n, LEN_LOGNORMAL, float(np.log(200.0)), 0.6, 32, 1024, seed), seed)
+    return t, gen_sample_ids(nq, n, seed)
+
+
+def config3(seed=0, n=1_000_000, nq=100_000):
+    """1M walks of U[50, 350] points; nq rectangles with sides log-U[0.001, 0.05] deg."""
+    t = gen_walks(gen_lengths(n, LEN_UNIFORM, 0, 0, 50, 350, seed), seed)
+    return t, gen_boxes(nq, SIDE_LOGUNIFORM, 0.001, 0.05, seed)
+
+
+def config4_pairs(seed=0, npairs=4096, lo=16, hi=4096):
+    """EDR pairs with both lengths log-uniform in [lo, hi]."""
+    la = gen_lengths(npairs, LEN_LOGUNIFORM, 0, 0, lo, hi, seed)
+    lb = gen_lengths(npairs, LEN_LOGUNIFORM, 0, 0, lo, hi, seed + 1)
+    a, b = gen_pairs(la, lb, seed)
+    return la, a, lb, b
+
+
 def edr(a_xy, b_xy, eps: float) -> int:
     a, b = _c(a_xy, np.float32).reshape(-1, 2), _c(b_xy, np.float32).reshape(-1, 2)
     return int(lib().orc_edr(_p(a, P_f32), a.shape[0], _p(b, P_f32), b.shape[0], eps))
@@ -412,6 +508,16 @@ class RefRunner:
         r["ids"] = r["ids"].reshape(len(qids), k)
         r["dist"] = r["dist"].reshape(len(qids), k)
         return r
+
+    def rangebench(self, n, len_lo, len_hi, seed, nq, side_lo, side_hi, cell, leaf_cap, box, per_step, steps,
+                   threads, timeout=3600):
+        """The reference's Grid over n generated walks and Grid::rangeQueryBatch over `steps`
+        strided samples of per_step of the nq generated rectangles, on `threads` threads
+        (ref_driver.cpp cmd_rangebench)."""
+        o = self._path("o.bin")
+        self._run(["rangebench", o, n, len_lo, len_hi, seed, nq, repr(float(side_lo)), repr(float(side_hi)),
+                   repr(float(cell)), leaf_cap, *[repr(float(v)) for v in box], per_step, steps, threads], timeout=timeout)
+        return read_out(o)
 
     def nbr(self, cells, vcells):
         i, o = self._path("i.bin"), self._path("o.bin")

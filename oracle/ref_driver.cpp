@@ -6,7 +6,7 @@
  * the product: tests use it to pin the restated oracle (oracle/oracle.cpp) and to write golden
  * fixtures, and bench.py times it as the CPU baseline of the reference.
  *
- * Input files use one small binary format, written by oracle/refio.py:
+ * Input files use one small binary format, written by oracle/pyoracle.py:
  *   data file    : "GATD", int32 n_traj, int64 n_points, int32 lengths[n_traj],
  *                  float lon[n_points], float lat[n_points]   (trajectory ids are 1..n_traj)
  *   query file   : "GATQ", int32 n, float[n][4] (xmin, ymin, xmax, ymax)
@@ -14,7 +14,7 @@
  *                  float B[sum lenB][2]        (x = lon, y = lat)
  *   id file      : "GATI", int32 n, int32 ids[n]
  * Output is a sequence of named arrays (int32 name length, name, char dtype, int64 count, data),
- * read by oracle/refio.py.
+ * read by oracle/pyoracle.py.
  *
  * Two facts of the reference are handled here rather than patched in its sources:
  *  - FVTable::formPriorityQueue (FVTable.cpp:141-152, 171-183) erases the std::map node that its
@@ -34,6 +34,8 @@
 #include <STIG.h>
 #include <FSG.h>
 #include <CalcInAxis.h>
+
+#include "datagen.h"
 
 #include <atomic>
 #include <chrono>
@@ -584,6 +586,93 @@ int cmd_edr(int argc, char** argv) {
     return 0;
 }
 
+/* rangebench OUT n len_lo len_hi seed nq side_lo side_hi cell leafcap bx0 by0 bx1 by1 per_step steps threads
+ * The batched range workload timed through the reference's own CPU query: n random walks with
+ * lengths uniform in [len_lo, len_hi] and nq rectangles with log-uniform sides in
+ * [side_lo, side_hi], generated with seed by oracle/datagen.cpp (the library's streams, so the
+ * arrays equal the GPU run's); the reference's Grid (Grid::Grid + addDatasetToGrid) over them;
+ * then `steps` steps. Step s takes the rectangles s, s + stride, s + 2 stride, ... (per_step of
+ * them, stride = nq / per_step, so every step is a different sample spread over the whole
+ * query set) and runs them on `threads` threads, each calling Grid::rangeQueryBatch
+ * (Grid.cpp:341-405) on a contiguous slice. Writes the per-step seconds, the build seconds, the
+ * number of ids per step and the id sets of step 0 (its rectangle indices in q_index). */
+int cmd_rangebench(int argc, char** argv) {
+    if (argc < 19) die("usage: rangebench OUT n len_lo len_hi seed nq side_lo side_hi cell leafcap bx0 by0 bx1 by1 per_step steps threads");
+    Writer w(argv[2]);
+    const int n = atoi(argv[3]), len_lo = atoi(argv[4]), len_hi = atoi(argv[5]);
+    const uint64_t seed = (uint64_t)atoll(argv[6]);
+    const int nq = atoi(argv[7]);
+    const double side_lo = atof(argv[8]), side_hi = atof(argv[9]);
+    const float cell = (float)atof(argv[10]);
+    gat_ref_leaf_cap = atoi(argv[11]);
+    const float box[4] = {(float)atof(argv[12]), (float)atof(argv[13]), (float)atof(argv[14]), (float)atof(argv[15])};
+    const int per_step = atoi(argv[16]), steps = atoi(argv[17]);
+    const int threads = std::max(1, atoi(argv[18]));
+    if (n < 1 || nq < 1 || per_step < 1 || per_step > nq || steps < 1) die("rangebench: bad sizes");
+    const int stride = nq / per_step;
+    if (steps > stride) die("rangebench: more steps than distinct samples");
+    Data d;
+    d.n = n;
+    d.len.resize(n);
+    orc_gen_lengths(n, ORC_LEN_UNIFORM, 0.0, 0.0, len_lo, len_hi, seed, d.len.data());
+    int64_t np = 0;
+    for (int v : d.len) np += v;
+    d.lon.resize(np);
+    d.lat.resize(np);
+    orc_gen_walks(n, d.len.data(), box, 1e-4, seed, d.lon.data(), d.lat.data());
+    std::vector<float> q4((size_t)nq * 4);
+    orc_gen_boxes(nq, ORC_SIDE_LOGUNIFORM, side_lo, side_hi, box, seed, q4.data());
+    load_tradb(d);
+    std::vector<float>().swap(d.lon);
+    std::vector<float>().swap(d.lat);
+    double t0 = now_s();
+    Grid* g = build_grid(d, cell, box[0], box[1], box[2], box[3]);
+    const double t_build = now_s() - t0;
+    std::vector<double> t_step;
+    std::vector<int64_t> ids_step, id_off(1, 0);
+    std::vector<int32_t> ids0, qidx0;
+    for (int s = 0; s < steps; s++) {
+        std::vector<MBB> q(per_step);
+        for (int j = 0; j < per_step; j++) {
+            const float* b = &q4[(size_t)(s + (int64_t)j * stride) * 4];
+            q[j] = MBB(b[0], b[1], b[2], b[3]);
+        }
+        std::vector<CPURangeQueryResult> res(per_step);
+        t0 = now_s();
+        std::vector<std::thread> th;
+        const int per = (per_step + threads - 1) / threads;
+        for (int b = 0; b < per_step; b += per) {
+            const int c = std::min(per, per_step - b);
+            th.emplace_back([g, &q, &res, b, c]() { g->rangeQueryBatch(&q[b], c, &res[b], nullptr); });
+        }
+        for (auto& t : th) t.join();
+        t_step.push_back(now_s() - t0);
+        int64_t cnt = 0;
+        for (int j = 0; j < per_step; j++) {
+            const CPURangeQueryResult& r = res[j];
+            for (int t = 0; t <= n && t < (int)r.size(); t++)
+                if (r[t]) {
+                    cnt++;
+                    if (s == 0) ids0.push_back(t);
+                }
+            if (s == 0) {
+                id_off.push_back((int64_t)ids0.size());
+                qidx0.push_back(s + j * stride);
+            }
+        }
+        ids_step.push_back(cnt);
+    }
+    w.f64("t_build", {t_build});
+    w.f64("t_step", t_step);
+    w.i64("ids_step", ids_step);
+    w.i64("id_off", id_off);
+    w.i32("ids", ids0);
+    w.i32("q_index", qidx0);
+    std::vector<int64_t> meta = {n, np, nq, per_step, stride, threads};
+    w.i64("meta", meta);
+    return 0;
+}
+
 /* Query frequency vector exactly as Grid::SimilarityQueryBatch builds it (Grid.cpp:860-877). */
 std::map<int, int> query_fv(Grid* g, const Trajectory& t) {
     std::map<int, int> fv;
@@ -726,12 +815,13 @@ int cmd_wfile(int argc, char** argv) {
 }
 
 int main(int argc, char** argv) {
-    if (argc < 2) die("usage: gatref {gtq|stig|fsg|edr|fvlb|topk} ...");
+    if (argc < 2) die("usage: gatref {gtq|stig|fsg|edr|rangebench|fvlb|topk|nbr|wfile} ...");
     std::string c = argv[1];
     if (c == "gtq") return cmd_gtq(argc, argv);
     if (c == "stig") return cmd_stig(argc, argv);
     if (c == "fsg") return cmd_fsg(argc, argv);
     if (c == "edr") return cmd_edr(argc, argv);
+    if (c == "rangebench") return cmd_rangebench(argc, argv);
     if (c == "fvlb") return cmd_fvlb(argc, argv);
     if (c == "topk") return cmd_topk(argc, argv);
     if (c == "nbr") return cmd_nbr(argc, argv);

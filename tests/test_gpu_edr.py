@@ -179,3 +179,46 @@ def test_device_api_rejects_bad_lengths(gpu_ctx):
     assert np.array_equal(got[ok], po.edr_batch(la_ok, sa, lb[ok], sb, 5e-4))
     # the context stays usable
     assert np.array_equal(G.edr_pairs(gpu_ctx, la_ok, sa, lb[ok], sb, 5e-4), got[ok])
+
+
+def test_bounded_carry_wait_gives_up(gpu_ctx):
+    """The wait of a pipelined tile for its predecessor's carry words is bounded: with the test
+    knob, the first tile of one pair writes no carries, the next tile gives up after ~4096
+    polls, the call returns GAT_ERR_TIMEOUT and that pair -1; every other pair is exact, and the
+    same context then answers exactly with the knob off. No fault, no hang: the wait ends by
+    itself and the kernel returns."""
+    from gat_b200 import _lib as L
+
+    ctx = G.Context(0)
+    try:
+        ctx.set_tuning(L.GAT_TUNE_EDR_ROWS, 4)  # one tile shape: no autotune launches
+        ctx.set_tuning(L.GAT_TUNE_EDR_FORM, 1)  # row tiles of 128 rows
+        la = np.array([600, 40, 900, 300], np.int32)
+        lb = np.array([700, 50, 800, 2000], np.int32)
+        a, b = D.pairs(la, lb, 61)
+        want = po.edr_batch(la, a, lb, b, 5e-4)
+        ctx.set_tuning(L.GAT_TUNE_TEST_STALL_CARRY, 3)  # pair 2 (900 x 800: 7 pipelined tiles)
+        assert ctx.tuning(L.GAT_TUNE_TEST_STALL_CARRY) == 3
+        with pytest.raises(G.GatError) as e:
+            G.edr_pairs(ctx, la, a, lb, b, 5e-4)
+        assert e.value.status == L.GAT_ERR_TIMEOUT
+        # the device arrays of the failed call: pair 2 is -1, the others exact
+        import torch
+
+        dev = torch.device("cuda", 0)
+        T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+        oa = np.concatenate([[0], np.cumsum(la)[:-1]]).astype(np.int64)
+        ob = np.concatenate([[0], np.cumsum(lb)[:-1]]).astype(np.int64)
+        d = [T(la), T(oa), T(a), T(lb), T(ob), T(b)]
+        out = torch.full((4,), -7, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        rc = L.lib.gat_edr_pairs_dev(ctx.h, 4, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(),
+                                     d[4].data_ptr(), d[5].data_ptr(), 5e-4, out.data_ptr())
+        assert rc == L.GAT_ERR_TIMEOUT
+        got = out.cpu().numpy()
+        assert got[2] == -1
+        assert np.array_equal(got[[0, 1, 3]], want[[0, 1, 3]])
+        ctx.set_tuning(L.GAT_TUNE_TEST_STALL_CARRY, 0)
+        assert np.array_equal(G.edr_pairs(ctx, la, a, lb, b, 5e-4), want)
+    finally:
+        ctx.close()

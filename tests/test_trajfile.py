@@ -56,6 +56,9 @@ def test_empty_trajectories_and_errors(tmp_path):
     bad.write_text("2\n121,30.7,122\n1;1;\n")  # short box line
     with pytest.raises(RuntimeError):
         D.read_trajectory_file(str(bad))
+    bad.write_text("1\n121,30.7,122,31.7\n1;\n--31.5,121.0,1,0;\n")  # two signs: strtod converts nothing
+    with pytest.raises(RuntimeError):
+        D.read_trajectory_file(str(bad))
     with pytest.raises(RuntimeError):
         D.read_trajectory_file(str(tmp_path / "missing.txt"))
 
