@@ -224,6 +224,7 @@ enum Slot {
     S_RANGE_CURSOR,
     S_RANGE_OVF,
     S_RANGE_CSR,
+    S_RANGE_ORDER,
     S_EDR_PAIRS,
     S_EDR_CARRY,
     S_EDR_COUNTERS,

@@ -23,6 +23,7 @@
 #include <climits>
 
 #include "internal.h"
+#include "launch.cuh"
 
 namespace gat {
 namespace {
@@ -153,15 +154,13 @@ __device__ void fsg_walk(const FsgDev& f, const Box& q, Emit emit, int first = 0
  * thread order the items are the sequential traversal's, cut at subtree boundaries. */
 constexpr int kGridDepth = 3, kStigDepth = 6, kSub = 64;
 
+/* The candidate ranges of sub-thread `sub` of a query, joined and cut into items. Writes them
+ * to items[0..] when items is non-NULL; returns how many there are. Sets GAT_ERR_ARG in flag when
+ * a walk's stack overflows. */
 template <int KIND>
-__global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, int nq, const int64_t* ioff,
-                        int64_t* icnt, int2* items, int32_t* flag) {
-    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= (int64_t)nq * kSub) return;
-    const int qi = (int)(tid / kSub), sub = (int)(tid % kSub);
-    Box q = load_box(queries, qi);
+__device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& f, const Box& q, int sub, int2* items,
+                              int32_t* flag) {
     int64_t cnt = 0;
-    int64_t w = ioff ? ioff[tid] : 0;
     /* Ranges that continue the previous one (neighbouring leaves / cells are contiguous in the
      * index's point order) are joined, and everything is cut into chunks of at most kChunk
      * points ending on multiples of 4, so the warps of the scan get balanced, 16-byte-aligned
@@ -171,7 +170,7 @@ __global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, 
         while (cur_b < cur_e) {
             int e = cur_e;
             if (e - cur_b > kChunk) e = (cur_b + kChunk) & ~3;
-            if (ioff) items[w + cnt] = make_int2(cur_b, e);
+            if (items) items[cnt] = make_int2(cur_b, e);
             cnt++;
             cur_b = e;
         }
@@ -229,7 +228,75 @@ __global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, 
     if (KIND == GAT_INDEX_FSG) fsg_walk(f, q, emit, sub, kSub);
     flush();
     if (!ok) set_flag(flag, GAT_ERR_ARG);
+    return cnt;
+}
+
+template <int KIND>
+__global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, int nq, const int64_t* ioff,
+                        int64_t* icnt, int2* items, int32_t* flag) {
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (int64_t)nq * kSub) return;
+    const int qi = (int)(tid / kSub), sub = (int)(tid % kSub);
+    const Box q = load_box(queries, qi);
+    const int64_t cnt = walk_items<KIND>(g, s, f, q, sub, ioff ? items + ioff[tid] : nullptr, flag);
     if (!ioff) icnt[tid] = cnt;
+}
+
+/* Plain execution, step 1 of 4 for query qi (one CTA of kSub threads): counts every
+ * sub-thread's items, lays out the query's item offsets ioff[0..kSub] (the layout of a batch of
+ * one), writes the items and clears the scan's counters. item_cap bounds the items of any
+ * single query; a query beyond it (impossible with the bound the host computes) raises
+ * GAT_ERR_ARG and scans nothing. */
+template <int KIND>
+__global__ void __launch_bounds__(kSub) k_plain_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, int qi,
+                                                      int64_t* ioff, int2* items, int64_t item_cap,
+                                                      unsigned long long* ctr, int32_t* flag) {
+    dep_wait();
+    __shared__ int64_t pre[kSub + 1];
+    const Box q = load_box(queries, qi);
+    const int sub = threadIdx.x;
+    pre[sub] = walk_items<KIND>(g, s, f, q, sub, nullptr, flag);
+    if (sub < 4) ctr[sub] = 0ull;
+    __syncthreads();
+    if (sub == 0) {
+        int64_t run = 0;
+        for (int i = 0; i < kSub; i++) {
+            const int64_t c = pre[i];
+            pre[i] = run;
+            run += c;
+        }
+        pre[kSub] = run;
+    }
+    __syncthreads();
+    const bool fits = pre[kSub] <= item_cap;
+    ioff[sub] = fits ? pre[sub] : 0;
+    if (sub == 0) ioff[kSub] = fits ? pre[kSub] : 0;
+    if (!fits) {
+        if (sub == 0) set_flag(flag, GAT_ERR_ARG);
+        return;
+    }
+    walk_items<KIND>(g, s, f, q, sub, items + pre[sub], flag);
+}
+
+/* Plain execution, step 4 of 4: the query's sorted ids (arena[segbase[0]..], segcnt[0] of them)
+ * go to out_tid[off[qi]..] and off[qi + 1] = off[qi] + count. When they do not fit `capacity`,
+ * nothing is written and trunc[0] is set; the offsets keep counting. */
+__global__ void k_plain_emit(int qi, const int64_t* __restrict__ segbase, const int64_t* __restrict__ segcnt,
+                             const uint32_t* __restrict__ arena, int64_t* off, int32_t* out_tid, int64_t capacity,
+                             int32_t* trunc) {
+    dep_wait();
+    const int64_t o = qi == 0 ? 0 : off[qi];
+    const int64_t n = segcnt[0];
+    if (threadIdx.x == 0) {
+        if (qi == 0) off[0] = 0;
+        off[qi + 1] = o + n;
+    }
+    if (o + n > capacity) {
+        if (threadIdx.x == 0) *trunc = 1;
+        return;
+    }
+    const uint32_t* src = arena + segbase[0];
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) out_tid[o + i] = (int32_t)src[i];
 }
 
 /* ---------------------------------------------------------------- block helpers */
@@ -301,13 +368,15 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
                                                         const int32_t* tid, int words, uint32_t* gbitmap,
                                                         uint32_t* arena, int64_t cap, unsigned long long* cursor,
                                                         int64_t* segbase, int64_t* segcnt, unsigned long long* work,
-                                                        const int* qlist) {
+                                                        const int* qlist, const unsigned long long* nq_dev) {
+    dep_wait();
     extern __shared__ uint32_t smem_bm[];
     __shared__ int sh[kThreads / 32 + 1];
     __shared__ unsigned long long base_sh;
     uint32_t* bm = gbitmap ? gbitmap + (size_t)blockIdx.x * words : smem_bm;
     int per = (words + kThreads - 1) / kThreads;
     unsigned long long my_work = 0; /* added once at exit */
+    if (nq_dev) nq = (int)*nq_dev; /* plain execution: the overflowed queries counted by the hash scan */
     for (int j = blockIdx.x; j < nq; j += gridDim.x) {
         const int qi = qlist ? qlist[j] : j;
         for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
@@ -357,6 +426,35 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
     }
 }
 
+/* ---------------------------------------------------------------- locality order */
+/* A batch's queries are scanned in the order of the index position of their first candidate
+ * point, bucketed: queries that start near each other in the index's point order (Morton-cell
+ * order for the Grid, row-major cells for FSG, KD-leaf order for STIG) read overlapping point
+ * ranges, and the CTAs working at one time then share those ranges in L2 instead of each
+ * fetching them from HBM. The order only changes which CTA scans a query and when; every
+ * query's result lands in its own slot, so results are the same. Queries without candidates
+ * go last. */
+constexpr int kOrderBuckets = 1 << 16;
+constexpr int kOrderMin = 256; /* smaller batches keep the given order */
+
+__global__ void k_order_keys(int nq, const int64_t* __restrict__ ioff, const int2* __restrict__ items, int64_t npoints,
+                             unsigned long long* __restrict__ hist, int* __restrict__ bucket) {
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= nq) return;
+    const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
+    int b = kOrderBuckets - 1;
+    if (i0 < i1) b = (int)min((long long)kOrderBuckets - 2, (long long)items[i0].x * (kOrderBuckets - 1) / (npoints + 1));
+    bucket[qi] = b;
+    atomicAdd(&hist[b], 1ull);
+}
+
+__global__ void k_order_scatter(int nq, const int* __restrict__ bucket, unsigned long long* __restrict__ base,
+                                int* __restrict__ order) {
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= nq) return;
+    order[atomicAdd(&base[bucket[qi]], 1ull)] = qi;
+}
+
 /* ---------------------------------------------------------------- id sets, hash form */
 /* Queries are taken from a counter by persistent CTAs. Each warp scans one candidate point
  * range at a time (128 points per step as float4 x / y / tid), tests MBB::pInBox, and inserts
@@ -392,7 +490,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
                                                          const float* __restrict__ Y, const int32_t* __restrict__ tid,
                                                          uint32_t* arena, int64_t cap, unsigned long long* ctr,
                                                          int64_t* segbase, int64_t* segcnt, int* ovf_list,
-                                                         unsigned long long* work) {
+                                                         unsigned long long* work, const int* __restrict__ order) {
+    dep_wait();
     extern __shared__ int hs_smem[];
     int* tab = hs_smem;              /* kHashSize */
     int* buf = hs_smem + kHashSize;  /* kHashMax sorted ids */
@@ -406,7 +505,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
     /* ctr: [0] arena cursor, [1] work bytes, [2] query counter, [3] overflow count */
     for (;;) {
         if (threadIdx.x == 0) {
-            q_sh = (int)atomicAdd(&ctr[2], 1ull);
+            const int j = (int)atomicAdd(&ctr[2], 1ull);
+            q_sh = j >= nq ? nq : (order ? order[j] : j);
             cnt_sh = 0;
             ovf_sh = 0;
         }
@@ -729,6 +829,25 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
     if (!items) return st;
     launch_items(ioff, nullptr, items);
     if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
+    int* order = nullptr;
+    if (mode == GAT_RESULT_IDS && nq >= kOrderMin) {
+        /* [order nq | bucket nq | hist kOrderBuckets + 1 (u64, 8-byte aligned; the scan writes the
+         * total into the last entry)] */
+        const size_t qwords = ((size_t)2 * nq + 1) & ~(size_t)1;
+        int* ob = (int*)scratch(ctx, S_RANGE_ORDER, qwords * sizeof(int) + (size_t)(kOrderBuckets + 1) * 8, &st);
+        if (!ob) return st;
+        order = ob;
+        int* bucket = ob + nq;
+        auto* hist = reinterpret_cast<unsigned long long*>(ob + qwords);
+        (void)launch_dep(ctx, k_zero_words, dim3(64), dim3(256), 0, s, reinterpret_cast<int*>(hist), 2 * kOrderBuckets);
+        const int ob_grid = (nq + 255) / 256;
+        k_order_keys<<<ob_grid, 256, 0, s>>>(nq, ioff, items, ix->npoints, hist, bucket);
+        if ((st = scan_i64(ctx, reinterpret_cast<int64_t*>(hist), reinterpret_cast<int64_t*>(hist), kOrderBuckets)) != GAT_OK)
+            return st;
+        k_order_scatter<<<ob_grid, 256, 0, s>>>(nq, bucket, hist, order);
+        count_launch(ctx, 3);
+        GAT_CUDA_TRY(ctx, cudaGetLastError(), "range order");
+    }
 
     int64_t* segbase = (int64_t*)scratch(ctx, S_RANGE_SEGBASE, (nq + 1) * sizeof(int64_t), &st);
     int64_t* segcnt = (int64_t*)scratch(ctx, S_RANGE_SEGCNT, (nq + 1) * sizeof(int64_t), &st);
@@ -764,7 +883,7 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
         if (mode == GAT_RESULT_IDS)
             k_range_hash<<<grid_hs, kThreads, smem_hs, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap,
-                                                           cursor, segbase, segcnt, ovf_list, work);
+                                                           cursor, segbase, segcnt, ovf_list, work, order);
         else
             k_range_points<<<grid_pts, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits,
                                                          arena, cap, cursor, segbase, segcnt);
@@ -788,7 +907,7 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
             timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
             k_range_ids<<<grid, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, (int)n_ovf, ioff, items, ix->d_x, ix->d_y,
                                                                         ix->d_tid, words, gbm, arena, cap, cursor, segbase,
-                                                                        segcnt, work, ovf_list);
+                                                                        segcnt, work, ovf_list, nullptr);
             timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
             count_launch(ctx);
             GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
@@ -824,6 +943,71 @@ int run_gather(gat_ctx* ctx, const gat_index* ix, int nq, int mode, const int64_
 }
 
 
+/* Plain execution of id-set queries: one query per launch sequence of four kernels (items,
+ * hash scan, bitmap scan for a query beyond the hash set, emit), chained as dependent launches.
+ * Every buffer is sized for any single query before the first launch (items by the index's
+ * candidate-range bound, the result arena by the set's trajectory count), so nothing waits on
+ * the host between queries; one synchronisation at the end reads the total and the status. */
+int run_plain_ids(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int64_t* d_off, int32_t* d_tid,
+                  int64_t capacity, int64_t* needed) {
+    cudaStream_t s = ctx->stream;
+    int st = GAT_OK;
+    /* items of one query: every candidate range (a leaf, a block, or a row of cells) yields its
+     * points in chunks of kChunk - 3 or more points, plus one partial chunk */
+    const int64_t ranges = ix->kind == GAT_INDEX_FSG ? (int64_t)ix->fsg.ny + 2 : std::max<int64_t>(ix->leaves, 1);
+    const int64_t item_cap = 2 * ranges + ix->npoints / (kChunk - 4) + 2 * kSub + 16;
+    const int64_t acap = (int64_t)ix->db->n + 1; /* distinct ids of one query */
+    int64_t* ioff = (int64_t*)scratch(ctx, S_RANGE_IOFF, (kSub + 1) * sizeof(int64_t), &st);
+    int2* items = (int2*)scratch(ctx, S_RANGE_ITEMS, (size_t)(item_cap + 1) * sizeof(int2), &st);
+    int64_t* segbase = (int64_t*)scratch(ctx, S_RANGE_SEGBASE, 2 * sizeof(int64_t), &st);
+    int64_t* segcnt = (int64_t*)scratch(ctx, S_RANGE_SEGCNT, 2 * sizeof(int64_t), &st);
+    /* cursor: [0] arena, [1] per-query work, [2] query counter, [3] overflowed (cleared per
+     * query), [4] truncation word, [5] work of the whole call */
+    unsigned long long* cursor = (unsigned long long*)scratch(ctx, S_RANGE_CURSOR, 64, &st);
+    int* ovf_list = (int*)scratch(ctx, S_RANGE_OVF, 2 * sizeof(int), &st);
+    uint32_t* arena = (uint32_t*)scratch(ctx, S_RANGE_ARENA, (size_t)acap * 4, &st);
+    if (!ioff || !items || !segbase || !segcnt || !cursor || !ovf_list || !arena) return st;
+    const int words = (ix->db->n + 1 + 31) / 32;
+    const size_t smem_bm = (size_t)words * 4;
+    const bool bm_in_smem = smem_bm <= 200 * 1024;
+    uint32_t* gbm = nullptr;
+    if (!bm_in_smem && !(gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, smem_bm, &st))) return st;
+    const size_t smem_hs = (size_t)(kHashSize + kHashMax) * sizeof(int);
+    allow_smem(k_range_hash, smem_hs);
+    if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 64, s), "range");
+    int32_t* trunc = reinterpret_cast<int32_t*>(cursor + 4);
+    unsigned long long* work = ctx->timing ? cursor + 5 : nullptr;
+    auto items_kernel = ix->kind == GAT_INDEX_GRID ? k_plain_items<GAT_INDEX_GRID>
+                        : ix->kind == GAT_INDEX_STIG ? k_plain_items<GAT_INDEX_STIG>
+                                                     : k_plain_items<GAT_INDEX_FSG>;
+    for (int qi = 0; qi < nq; qi++) {
+        cudaError_t e = launch_dep(ctx, items_kernel, dim3(1), dim3(kSub), 0, s, ix->grid, ix->stig, ix->fsg, d_q, qi,
+                                   ioff, items, item_cap, cursor, ctx->d_flag);
+        timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
+        if (e == cudaSuccess)
+            e = launch_dep(ctx, k_range_hash, dim3(1), dim3(kThreads), smem_hs, s, d_q + qi, 1, ioff, items, ix->d_x,
+                           ix->d_y, ix->d_tid, arena, acap, cursor, segbase, segcnt, ovf_list, work, (const int*)nullptr);
+        if (e == cudaSuccess)
+            e = launch_dep(ctx, k_range_ids, dim3(1), dim3(kThreads), bm_in_smem ? smem_bm : 0, s, d_q + qi, 0, ioff,
+                           items, ix->d_x, ix->d_y, ix->d_tid, words, gbm, arena, acap, cursor, segbase, segcnt, work,
+                           ovf_list, cursor + 3);
+        timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
+        if (e == cudaSuccess)
+            e = launch_dep(ctx, k_plain_emit, dim3(1), dim3(256), 0, s, qi, segbase, segcnt, arena, d_off, d_tid,
+                           capacity, trunc);
+        count_launch(ctx, 4);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "range plain launch");
+    }
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, d_off + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 1, cursor + 4, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+    if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
+    *needed = ctx->h_pinned[0];
+    if (ctx->timing) timed_add_work(ctx, GAT_KERNEL_RANGE_SCAN, (double)ctx->h_pinned[2]);
+    if ((int32_t)ctx->h_pinned[1] != 0) return fail(ctx, GAT_ERR_TRUNCATED, "range: output capacity too small");
+    return GAT_OK;
+}
+
 /* Device-side entry shared by the host and device APIs. Offsets, tids and pidx go to device
  * buffers with the given capacity; needed receives the total. */
 int range_dev(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int mode, int exec, int64_t* d_off,
@@ -844,7 +1028,8 @@ int range_dev(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         if ((st = run_gather(ctx, ix, nq, mode, d_off, d_tid, d_pidx)) != GAT_OK) return st;
         return gat_ctx_sync(ctx);
     }
-    /* plain: one query per pipeline run */
+    if (mode == GAT_RESULT_IDS) return run_plain_ids(ctx, ix, d_q, nq, d_off, d_tid, capacity, needed);
+    /* plain point lists: one query per pipeline run */
     int64_t done = 0;
     int64_t* off1 = (int64_t*)scratch(ctx, S_RANGE_OFF, 2 * sizeof(int64_t), &st);
     if (!off1) return st;

@@ -15,7 +15,13 @@
  * Estimates: range requests reserve 1 KB plus 16 bytes per expected result entry (a running
  * mean of the index's observed result sizes); top-k requests reserve 32 bytes per trajectory
  * of the set (lower bounds, candidate order, distances) plus 64 KB. After a batch, a lane
- * whose scratch arena exceeds its share of the budget (budget / lanes) frees it. */
+ * whose scratch arena exceeds its share of the budget (budget / lanes) frees it.
+ *
+ * Head-of-line blocking: a top-k batch runs for milliseconds, a range batch for well under one.
+ * With two or more lanes, top-k batches may hold all lanes but one, so a range request never
+ * waits behind top-k work for a lane; and a top-k batch stops growing once its queries hold
+ * kTopkBatchPoints points (its DP work grows with them), so one batch of long queries cannot
+ * hold a lane for long. */
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -32,6 +38,7 @@ using namespace gat;
 namespace {
 
 enum { REQ_RANGE = 0, REQ_TOPK = 1 };
+constexpr int64_t kTopkBatchPoints = 8192; /* query points per top-k batch (at least one request) */
 
 struct Request {
     int64_t id = 0;
@@ -72,6 +79,7 @@ struct gat_server {
     std::vector<Batch*> lane_batch;
     int64_t next_id = 0;
     int64_t reserved = 0;
+    int topk_running = 0; /* lanes running a top-k batch */
     bool stopping = false, lanes_stop = false;
     double hits_mean[3] = {4096, 4096, 4096};
     int64_t stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -114,7 +122,9 @@ struct gat_server {
     Batch* form_batch() {
         std::deque<Request*>* best = nullptr;
         int64_t best_t = INT64_MAX;
-        if (!q_topk.empty()) {
+        /* top-k batches leave one lane to range requests */
+        const bool topk_lane = lane_batch.size() < 2 || topk_running < (int)lane_batch.size() - 1;
+        if (!q_topk.empty() && topk_lane) {
             best = &q_topk;
             best_t = q_topk.front()->t[0];
         }
@@ -131,11 +141,16 @@ struct gat_server {
         b->kind = head->kind;
         b->index_kind = head->index_kind;
         b->result_kind = head->result_kind;
+        int64_t points = 0;
         for (auto it = best->begin(); it != best->end() && (int)b->reqs.size() < limit;) {
             Request* r = *it;
             if (r->kind == REQ_TOPK && r->eps != head->eps) {
                 ++it;
                 continue;
+            }
+            if (r->kind == REQ_TOPK) {
+                if (!b->reqs.empty() && points + (int64_t)r->lon.size() > kTopkBatchPoints) break;
+                points += (int64_t)r->lon.size();
             }
             if (reserved + b->reserve + r->reserve > cfg.budget_bytes) {
                 if (r->reserve > cfg.budget_bytes) { /* can never fit */
@@ -176,6 +191,7 @@ struct gat_server {
             stats[6] = std::max<int64_t>(stats[6], (int64_t)b->reqs.size());
             stats[2]++;
             stats[b->kind == REQ_TOPK ? 4 : 3]++;
+            if (b->kind == REQ_TOPK) topk_running++;
             lane_batch[lane] = b;
             cv_lane.notify_all();
         }
@@ -258,6 +274,7 @@ struct gat_server {
             if (gat_ctx_scratch_bytes(w) > cfg.budget_bytes / (int64_t)lanes.size()) gat_ctx_trim(w);
             std::lock_guard<std::mutex> lk(mu);
             reserved -= b->reserve;
+            if (b->kind == REQ_TOPK) topk_running--;
             lane_batch[i] = nullptr;
             delete b;
             cv_done.notify_all();

@@ -120,3 +120,35 @@ def test_id_sets_beyond_shared_memory_set(gpu_ctx, c1, kind):
     off, ids = o.range(qq, 0)
     assert np.array_equal(r.offsets, off) and np.array_equal(r.tids, ids)
     assert off[41] - off[40] > 4096  # the whole-box query really overflows the set
+
+
+@pytest.mark.parametrize("kind", ["grid", "stig", "fsg"])
+def test_plain_and_ordered_batches_with_overflow(gpu_ctx, c1, kind):
+    """Plain execution (one launch sequence per query, no host wait in between) and batches of
+    at least 256 queries (scanned in the locality order of their first candidate) on every
+    index, with whole-box queries that overflow the shared-memory set in both forms."""
+    t, q, db = c1
+    ix = {"grid": lambda: G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512), "stig": lambda: G.STIG(gpu_ctx, db, 512),
+          "fsg": lambda: G.FSG(gpu_ctx, db, D.BOX, 0.01)}[kind]()
+    o = {"grid": lambda: po.OracleGrid(t, D.BOX, 0.01, 2, 512), "stig": lambda: po.OracleSTIG(t, 512),
+         "fsg": lambda: po.OracleFSG(t, D.BOX, 0.01)}[kind]()
+    big = np.array([[121.0, 30.7, 122.0, 31.7], [121.2, 30.9, 122.0, 31.7]], np.float32)
+    batch = np.concatenate([q[:700], big[:1], q[700:], big[1:]])
+    r = ix.range_query(batch)
+    off, ids = o.range(batch, 0)
+    assert np.array_equal(r.offsets, off) and np.array_equal(r.tids, ids)
+    plain = np.concatenate([q[::23], big[:1], q[5:40]])
+    r = ix.range_query(plain, execution="plain")
+    off, ids = o.range(plain, 0)
+    assert np.array_equal(r.offsets, off) and np.array_equal(r.tids, ids)
+
+
+def test_plain_truncation_reports_needed(gpu_ctx, c1):
+    t, q, db = c1
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512)
+    full = g.range_query(q[:60], execution="plain")
+    with pytest.raises(G.GatError) as e:
+        g.range_query(q[:60], execution="plain", capacity=max(0, len(full.tids) - 1))
+    assert e.value.status == 4
+    again = g.range_query(q[:60], execution="plain")
+    assert np.array_equal(again.offsets, full.offsets) and np.array_equal(again.tids, full.tids)
