@@ -1266,7 +1266,7 @@ def host_cpu() -> tuple[int, str]:
 
 def suite_config(world: int, n: int) -> dict:
     """The configuration both arms print (the reference arm times the same workload on the host)."""
-    return {"workload": f"C3 batched range queries over the GT-quadtree, STIG and FSG: {n} random walks U[50,350] "
+    return {"workload": f"C3 batched range queries over the GT-quadtree, STIG, FSG and MortonGrid: {n} random walks U[50,350] "
                         "points, 100k rectangles with log-U[0.001,0.05] deg sides, cell 0.001 deg, leaf cap 512, STIG "
                         "block 10240, trajectory-id sets; value = GT-quadtree batched queries/s. Beside it: the plain "
                         "form (one query per launch sequence), C4 batched EDR (4096 pairs, both sides log-U[16,4096], "
@@ -1325,7 +1325,8 @@ def run_suite(args, world, rank, local, td):
     t0 = time.time()
     idx = {"grid": G.Grid(ctx, db, G.BOX, SUITE["cell"], SUITE["vparam"], SUITE["leaf_cap"]),
            "fsg": G.FSG(ctx, db, G.BOX, SUITE["cell"])}
-    log("grid + fsg built", round(time.time() - t0, 1))
+    idx["morton"] = G.MortonGrid(idx["grid"])
+    log("grid + fsg + morton built", round(time.time() - t0, 1))
     t0 = time.time()
     idx["stig"] = G.STIG(ctx, db, SUITE["stig_block"])
     log("stig built", round(time.time() - t0, 1))
@@ -1343,7 +1344,7 @@ def run_suite(args, world, rank, local, td):
     # ---- timed: batched range steps on each index (the GT-quadtree's are the line's value)
     res = {}
     clk = None
-    for name in ("grid", "fsg", "stig"):
+    for name in ("grid", "fsg", "stig", "morton"):
         ix = idx[name]
         for _ in range(args.warmup):
             H.time(lambda: call(ix))
@@ -1389,6 +1390,7 @@ def run_suite(args, world, rank, local, td):
     pq = min(nq, SUITE["parity_queries"])
     psel = np.arange(0, nq, nq // pq)[:pq]
     fsg_r = idx["fsg"].range_query(q[psel])
+    morton_r = idx["morton"].range_query(q[psel])
     # ---- config 4: batched EDR pairs and their plain form
     edr = measure_edr_pairs(ctx, H, args, td, rank, local, dev)
     # ---- config 5: served mix on the same resident set
@@ -1437,6 +1439,7 @@ def run_suite(args, world, rank, local, td):
         po_off, po_ids = og.range(q[sel][np.arange(0, ps, max(1, ps // pq))[:pq]])
         checks = {"grid_batched": bool(np.array_equal(g_off, o_off) and np.array_equal(g_ids, o_ids)),
                   "fsg_batched": bool(np.array_equal(fsg_r.offsets, f_off) and np.array_equal(fsg_r.tids, f_ids)),
+                  "morton_batched": bool(np.array_equal(morton_r.offsets, o_off) and np.array_equal(morton_r.tids, o_ids)),
                   "grid_plain": bool(np.array_equal(p_off, po_off) and np.array_equal(p_ids, po_ids)),
                   "edr_batched": edr.pop("_parity_ok")}
         line["parity"] = {"checked": {"range_queries": int(pq), "edr_pairs": int(edr["pairs"])},

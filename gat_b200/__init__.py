@@ -5,5 +5,6 @@ include/gat_b200.h); this package is its Python mirror. Importing it loads the l
 fails loudly when it has not been built (`python -m gat_b200.build`).
 """
 from . import _lib  # noqa: F401  (loads libgat_b200.so or raises)
-from .api import FSG, STIG, Context, GatError, Grid, RangeResult, Server, SystemTest, TrajectorySet, edr_pairs  # noqa: F401
+from .api import (FSG, STIG, Context, GatError, Grid, MortonGrid, RangeResult, Server, SystemTest,  # noqa: F401
+                  TrajectorySet, edr_pairs)
 from .data import BOX, Trajectories  # noqa: F401

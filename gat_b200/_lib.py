@@ -29,7 +29,7 @@ class MBB(C.Structure):
 
 
 GAT_OK, GAT_ERR_ARG, GAT_ERR_OOM, GAT_ERR_CUDA, GAT_ERR_TRUNCATED, GAT_ERR_TIMEOUT, GAT_ERR_STATE = range(7)
-GAT_INDEX_GRID, GAT_INDEX_STIG, GAT_INDEX_FSG = 0, 1, 2
+GAT_INDEX_GRID, GAT_INDEX_STIG, GAT_INDEX_FSG, GAT_INDEX_MORTON = 0, 1, 2, 3
 GAT_RESULT_IDS, GAT_RESULT_POINTS = 0, 1
 GAT_EXEC_PLAIN, GAT_EXEC_BATCHED = 0, 1
 GAT_LEN_UNIFORM, GAT_LEN_LOGNORMAL, GAT_LEN_LOGUNIFORM = 0, 1, 2
@@ -67,6 +67,8 @@ SIGNATURES = [
     ("gat_grid_build", c_int, [c_p, c_p, MBB, c_f, c_int, c_int, C.POINTER(c_p)]),
     ("gat_stig_build", c_int, [c_p, c_p, c_int, C.POINTER(c_p)]),
     ("gat_fsg_build", c_int, [c_p, c_p, MBB, c_f, C.POINTER(c_p)]),
+    ("gat_morton_grid_build", c_int, [c_p, c_p, C.POINTER(c_p)]),
+    ("gat_morton_grid_leaves", c_int, [c_p, c_p, P_i32, P_i32, c_i64, P_i64]),
     ("gat_index_destroy", None, [c_p]),
     ("gat_index_info", c_int, [c_p, P_i64]),
     ("gat_index_points", c_int, [c_p, c_p, c_i64, P_f32, P_f32, P_i32, P_i32]),

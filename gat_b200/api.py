@@ -284,6 +284,30 @@ class FSG(Index):
         self.h = h
 
 
+class MortonGrid(Index):
+    """MortonGrid (MortonGrid.h:27): the quadtree of `grid` as a leaf bitmap over implicit node ids
+    with computed node boxes; the same range results as the Grid, over the Grid's points (keep the
+    Grid alive while this is used)."""
+
+    kind = L.GAT_INDEX_MORTON
+
+    def __init__(self, grid: Grid):
+        super().__init__(grid.ctx, grid.db)
+        h = C.c_void_p()
+        grid.ctx.check(lib.gat_morton_grid_build(grid.ctx.h, grid.h, C.byref(h)), "gat_morton_grid_build")
+        self.h = h
+        self.grid = grid
+
+    def leaves(self):
+        """(level, id) of every leaf, in bitmap order."""
+        n = C.c_int64(0)
+        lib.gat_morton_grid_leaves(self.ctx.h, self.h, None, None, 0, C.byref(n))
+        lv, ids = np.zeros(n.value, np.int32), np.zeros(n.value, np.int32)
+        self.ctx.check(lib.gat_morton_grid_leaves(self.ctx.h, self.h, _p(lv, L.P_i32), _p(ids, L.P_i32), n.value, C.byref(n)),
+                       "gat_morton_grid_leaves")
+        return lv, ids
+
+
 def edr_pairs(ctx: Context, q_len, q_xy, c_len, c_xy, eps: float) -> np.ndarray:
     """EDR of pair i = (q_xy[q_off[i]:...], c_xy[c_off[i]:...]) with offsets from the lengths."""
     ql, cl = _c(q_len, np.int32), _c(c_len, np.int32)
@@ -392,8 +416,9 @@ class Server:
 class SystemTest:
     """The reference's harness entry points (SystemTest.h:13-35) over this library."""
 
-    def __init__(self, tradb: Trajectories, g: Grid | None, stig: STIG | None, fsg: FSG | None, eps: float = 0.005):
-        self.tradb, self.g, self.stig, self.fsg, self.eps = tradb, g, stig, fsg, eps
+    def __init__(self, tradb: Trajectories, g: Grid | None, stig: STIG | None, fsg: FSG | None, eps: float = 0.005,
+                 mgrid: MortonGrid | None = None):
+        self.tradb, self.g, self.stig, self.fsg, self.eps, self.mgrid = tradb, g, stig, fsg, eps, mgrid
 
     @staticmethod
     def _repeat(mbb, n):
@@ -409,14 +434,16 @@ class SystemTest:
         return self.fsg.range_query(self._repeat(rangeQueryMBB, rangeQueryNum))
 
     def rangeQueryTestWithoutMorton(self, rangeQueryMBB, rangeQueryNum: int) -> RangeResult:
-        """SystemTest.h:29. The reference's row-major walk over the Grid's points
-        (Grid.cpp:544-662) returns the Grid's id sets; this runs the GT-quadtree path."""
+        """SystemTest.h:29. The reference's pretend-row-major walk (Grid.cpp:544-662) never
+        advances its segment offsets (Grid.cpp:818-827), so its results are not the Grid's and
+        there is nothing of its own to reproduce; this runs the GT-quadtree path."""
         return self.rangeQueryTest(rangeQueryMBB, rangeQueryNum)
 
     def MortonGridRangeQueryTest(self, rangeQueryMBB, rangeQueryNum: int) -> RangeResult:
-        """SystemTest.h:33. MortonGrid (MortonGrid.cpp:238-400) is the Grid with a leaf bitmap
-        over implicit node ids and the same leaf rule; its id sets are the Grid's."""
-        return self.rangeQueryTest(rangeQueryMBB, rangeQueryNum)
+        """SystemTest.h:33: the MortonGrid's implicit-tree walk (MortonGrid.cpp:268-393); its id
+        sets are the Grid's. Without a MortonGrid the Grid answers."""
+        ix = self.mgrid if self.mgrid is not None else self.g
+        return ix.range_query(self._repeat(rangeQueryMBB, rangeQueryNum))
 
     def similarityQueryTest(self, t, similarityScale: int, similarityKValue: int):
         """t: a Trajectories holding one query, or an int trajectory number (README.md:30)."""

@@ -454,7 +454,7 @@ int gat_index_info(const gat_index* ix, int64_t info[8]) {
     info[1] = ix->npoints;
     info[2] = ix->leaves;
     info[3] = ix->nodes;
-    if (ix->kind == GAT_INDEX_GRID) info[4] = info[5] = ix->grid.axis;
+    if (ix->kind == GAT_INDEX_GRID || ix->kind == GAT_INDEX_MORTON) info[4] = info[5] = ix->grid.axis;
     if (ix->kind == GAT_INDEX_FSG) {
         info[4] = ix->fsg.nx;
         info[5] = ix->fsg.ny;
@@ -466,6 +466,7 @@ int gat_index_info(const gat_index* ix, int64_t info[8]) {
 int gat_index_points(gat_ctx* ctx, const gat_index* ix, int64_t n, float* x, float* y, int32_t* tid,
                      int32_t* pidx) {
     if (!ctx || !ix || n != ix->npoints) return fail(ctx, GAT_ERR_ARG, "gat_index_points: size mismatch");
+    if (ix->kind == GAT_INDEX_MORTON) return gat_index_points(ctx, ix->base, n, x, y, tid, pidx); /* the Grid's order */
     {
         /* a device-placed index whose host copies were never asked for: read the device arrays */
         std::lock_guard<std::mutex> lk(const_cast<gat_index*>(ix)->host_mu);

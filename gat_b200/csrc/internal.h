@@ -60,6 +60,17 @@ struct FsgDev {
     const int32_t* cend;
 };
 
+/* MortonGrid (MortonGrid.h:22-40): the Grid's quadtree as an implicit tree. Node (level, id)
+ * covers the Morton cells [id * 4^(L - level), (id + 1) * 4^(L - level)); it is a leaf when bit
+ * (4^level - 1) / 3 + id of `leaf` is set (findIdxInBitmap, MortonGrid.cpp:8-13); its points are
+ * [cbeg[first cell], cbeg[last cell + 1]) of the Grid's point order. */
+struct MortonDev {
+    float rxmin, rymax, cell;
+    int total_level;
+    const uint32_t* leaf;
+    const int32_t* cbeg;
+};
+
 /* One EDR problem: query side (a) and candidate side (b), offsets into two point arrays. */
 struct EdrPair {
     int64_t a_off;
@@ -148,6 +159,8 @@ struct gat_index {
     gat::GridDev grid{};
     gat::StigDev stig{};
     gat::FsgDev fsg{};
+    gat::MortonDev morton{};
+    const gat_index* base = nullptr; /* MortonGrid: the Grid whose point arrays it reads */
     /* Grid FVTable (CSR over tids 0..n) */
     int64_t* d_fv_off = nullptr;
     int32_t* d_fv_cell = nullptr;

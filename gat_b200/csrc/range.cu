@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <climits>
 
+#include "cells.cuh"
 #include "internal.h"
 #include "launch.cuh"
 
@@ -147,6 +148,52 @@ __device__ void fsg_walk(const FsgDev& f, const Box& q, Emit emit, int first = 0
     }
 }
 
+/* MortonGrid implicit nodes: the leaf bit of (level, id) (findIdxInBitmap, MortonGrid.cpp:8-13),
+ * the node's box from its first and last Morton cells (generateMBBfromNode,
+ * MortonGrid.cpp:261-265) and its point range. */
+__device__ __forceinline__ bool morton_leaf(const MortonDev& m, int level, uint32_t id) {
+    const uint64_t idx = (((uint64_t)1 << (2 * level)) - 1) / 3 + id;
+    return (__ldg(m.leaf + (idx >> 5)) >> (idx & 31)) & 1u;
+}
+__device__ __forceinline__ Box morton_box(const MortonDev& m, int level, uint32_t id) {
+    const uint32_t span = 1u << (2 * (m.total_level - level));
+    const float4 a = morton_cell_box(m.rxmin, m.rymax, m.cell, (int)(id * span));
+    const float4 b = morton_cell_box(m.rxmin, m.rymax, m.cell, (int)(id * span + span - 1));
+    return Box{a.x, b.y, b.z, a.w};
+}
+template <class Emit>
+__device__ __forceinline__ void morton_emit(const MortonDev& m, int level, uint32_t id, Emit emit) {
+    const uint32_t span = 1u << (2 * (m.total_level - level));
+    emit(__ldg(m.cbeg + id * span), __ldg(m.cbeg + id * span + span));
+}
+
+/* MortonGrid::findMatchNodeInQuadTree (MortonGrid.cpp:356-393): leaves are taken without a
+ * test, children in the order UL, UR, DL, DR when BoxIntersect(query, child box) is non-zero.
+ * Stack entries pack (id << 4) | level (level <= 13). */
+template <class Emit>
+__device__ bool morton_walk(const MortonDev& m, const Box& q, Emit emit, int level0, uint32_t id0) {
+    uint32_t stack[kStack];
+    int sp = 0;
+    stack[sp++] = (id0 << 4) | (uint32_t)level0;
+    while (sp > 0) {
+        const uint32_t e = stack[--sp];
+        const int level = (int)(e & 15u);
+        const uint32_t id = e >> 4;
+        if (morton_leaf(m, level, id)) {
+            morton_emit(m, level, id, emit);
+            continue;
+        }
+        for (int c = 3; c >= 0; c--) {
+            const uint32_t cid = (id << 2) + (uint32_t)c;
+            if (box_intersect(q, morton_box(m, level + 1, cid))) {
+                if (sp >= kStack) return false;
+                stack[sp++] = (cid << 4) | (uint32_t)(level + 1);
+            }
+        }
+    }
+    return true;
+}
+
 /* kSub threads per query: thread `sub` takes the path given by its digits (base 4 over
  * kGridDepth quadtree levels, base 2 over kStigDepth STIG levels), with the traversal's own
  * intersection tests, and walks the subtree it reaches; a leaf met on the way belongs to the
@@ -158,8 +205,8 @@ constexpr int kGridDepth = 3, kStigDepth = 6, kSub = 64;
  * to items[0..] when items is non-NULL; returns how many there are. Sets GAT_ERR_ARG in flag when
  * a walk's stack overflows. */
 template <int KIND>
-__device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& f, const Box& q, int sub, int2* items,
-                              int32_t* flag) {
+__device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& f, const MortonDev& m, const Box& q,
+                              int sub, int2* items, int32_t* flag) {
     int64_t cnt = 0;
     /* Ranges that continue the previous one (neighbouring leaves / cells are contiguous in the
      * index's point order) are joined, and everything is cut into chunks of at most kChunk
@@ -226,19 +273,36 @@ __device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& 
         if (walk) ok = stig_walk(s, q, emit, nd);
     }
     if (KIND == GAT_INDEX_FSG) fsg_walk(f, q, emit, sub, kSub);
+    if (KIND == GAT_INDEX_MORTON) {
+        int level = 0; /* the Grid's digit split over the implicit nodes */
+        uint32_t id = 0;
+        bool walk = true;
+        for (int lev = 0; lev < kGridDepth && walk; lev++) {
+            if (morton_leaf(m, level, id)) {
+                if ((sub & ((1 << (2 * (kGridDepth - lev))) - 1)) == 0) morton_emit(m, level, id, emit);
+                walk = false;
+                break;
+            }
+            const uint32_t cid = (id << 2) + (uint32_t)((sub >> (2 * (kGridDepth - 1 - lev))) & 3);
+            if (!box_intersect(q, morton_box(m, level + 1, cid))) walk = false;
+            level++;
+            id = cid;
+        }
+        if (walk) ok = morton_walk(m, q, emit, level, id);
+    }
     flush();
     if (!ok) set_flag(flag, GAT_ERR_ARG);
     return cnt;
 }
 
 template <int KIND>
-__global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, int nq, const int64_t* ioff,
+__global__ void k_items(GridDev g, StigDev s, FsgDev f, MortonDev m, const gat_mbb* queries, int nq, const int64_t* ioff,
                         int64_t* icnt, int2* items, int32_t* flag) {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (int64_t)nq * kSub) return;
     const int qi = (int)(tid / kSub), sub = (int)(tid % kSub);
     const Box q = load_box(queries, qi);
-    const int64_t cnt = walk_items<KIND>(g, s, f, q, sub, ioff ? items + ioff[tid] : nullptr, flag);
+    const int64_t cnt = walk_items<KIND>(g, s, f, m, q, sub, ioff ? items + ioff[tid] : nullptr, flag);
     if (!ioff) icnt[tid] = cnt;
 }
 
@@ -248,14 +312,14 @@ __global__ void k_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, 
  * single query; a query beyond it (impossible with the bound the host computes) raises
  * GAT_ERR_ARG and scans nothing. */
 template <int KIND>
-__global__ void __launch_bounds__(kSub) k_plain_items(GridDev g, StigDev s, FsgDev f, const gat_mbb* queries, int qi,
+__global__ void __launch_bounds__(kSub) k_plain_items(GridDev g, StigDev s, FsgDev f, MortonDev m, const gat_mbb* queries, int qi,
                                                       int64_t* ioff, int2* items, int64_t item_cap,
                                                       unsigned long long* ctr, int32_t* flag) {
     dep_wait();
     __shared__ int64_t pre[kSub + 1];
     const Box q = load_box(queries, qi);
     const int sub = threadIdx.x;
-    pre[sub] = walk_items<KIND>(g, s, f, q, sub, nullptr, flag);
+    pre[sub] = walk_items<KIND>(g, s, f, m, q, sub, nullptr, flag);
     if (sub < 4) ctr[sub] = 0ull;
     __syncthreads();
     if (sub == 0) {
@@ -275,7 +339,7 @@ __global__ void __launch_bounds__(kSub) k_plain_items(GridDev g, StigDev s, FsgD
         if (sub == 0) set_flag(flag, GAT_ERR_ARG);
         return;
     }
-    walk_items<KIND>(g, s, f, q, sub, items + pre[sub], flag);
+    walk_items<KIND>(g, s, f, m, q, sub, items + pre[sub], flag);
 }
 
 /* Plain execution, step 4 of 4: the query's sorted ids (arena[segbase[0]..], segcnt[0] of them)
@@ -808,13 +872,16 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
     auto launch_items = [&](const int64_t* ioff, int64_t* cnt, int2* items) {
         switch (ix->kind) {
             case GAT_INDEX_GRID:
-                k_items<GAT_INDEX_GRID><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, d_q, nq, ioff, cnt, items, ctx->d_flag);
+                k_items<GAT_INDEX_GRID><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ioff, cnt, items, ctx->d_flag);
                 break;
             case GAT_INDEX_STIG:
-                k_items<GAT_INDEX_STIG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, d_q, nq, ioff, cnt, items, ctx->d_flag);
+                k_items<GAT_INDEX_STIG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ioff, cnt, items, ctx->d_flag);
+                break;
+            case GAT_INDEX_MORTON:
+                k_items<GAT_INDEX_MORTON><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ioff, cnt, items, ctx->d_flag);
                 break;
             default:
-                k_items<GAT_INDEX_FSG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, d_q, nq, ioff, cnt, items, ctx->d_flag);
+                k_items<GAT_INDEX_FSG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ioff, cnt, items, ctx->d_flag);
         }
         count_launch(ctx);
     };
@@ -978,12 +1045,13 @@ int run_plain_ids(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq,
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 64, s), "range");
     int32_t* trunc = reinterpret_cast<int32_t*>(cursor + 4);
     unsigned long long* work = ctx->timing ? cursor + 5 : nullptr;
-    auto items_kernel = ix->kind == GAT_INDEX_GRID ? k_plain_items<GAT_INDEX_GRID>
-                        : ix->kind == GAT_INDEX_STIG ? k_plain_items<GAT_INDEX_STIG>
-                                                     : k_plain_items<GAT_INDEX_FSG>;
+    auto items_kernel = ix->kind == GAT_INDEX_GRID     ? k_plain_items<GAT_INDEX_GRID>
+                        : ix->kind == GAT_INDEX_STIG   ? k_plain_items<GAT_INDEX_STIG>
+                        : ix->kind == GAT_INDEX_MORTON ? k_plain_items<GAT_INDEX_MORTON>
+                                                       : k_plain_items<GAT_INDEX_FSG>;
     for (int qi = 0; qi < nq; qi++) {
-        cudaError_t e = launch_dep(ctx, items_kernel, dim3(1), dim3(kSub), 0, s, ix->grid, ix->stig, ix->fsg, d_q, qi,
-                                   ioff, items, item_cap, cursor, ctx->d_flag);
+        cudaError_t e = launch_dep(ctx, items_kernel, dim3(1), dim3(kSub), 0, s, ix->grid, ix->stig, ix->fsg, ix->morton,
+                                   d_q, qi, ioff, items, item_cap, cursor, ctx->d_flag);
         timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
         if (e == cudaSuccess)
             e = launch_dep(ctx, k_range_hash, dim3(1), dim3(kThreads), smem_hs, s, d_q + qi, 1, ioff, items, ix->d_x,

@@ -117,6 +117,8 @@ int gat_index_save(gat_ctx* ctx, const gat_index* index, const char* path) {
     if (!ctx || !index || !path) return fail(ctx, GAT_ERR_ARG, "gat_index_save: bad arguments");
     if (int rq = require_device(ctx, "gat_index_save")) return rq;
     if (!same_owner(index->ctx, ctx)) return fail(ctx, GAT_ERR_STATE, "gat_index_save: index from another context");
+    if (index->kind == GAT_INDEX_MORTON)
+        return fail(ctx, GAT_ERR_ARG, "gat_index_save: a MortonGrid is not saved; save its Grid and rebuild it");
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
     gat_index* ix = const_cast<gat_index*>(index);

@@ -56,7 +56,7 @@ typedef struct {
     float xmin, ymin, xmax, ymax;
 } gat_mbb;
 
-enum { GAT_INDEX_GRID = 0, GAT_INDEX_STIG = 1, GAT_INDEX_FSG = 2 };
+enum { GAT_INDEX_GRID = 0, GAT_INDEX_STIG = 1, GAT_INDEX_FSG = 2, GAT_INDEX_MORTON = 3 };
 /* GAT_RESULT_IDS: per query, the sorted set of trajectory ids with at least one point in the
  * box (the reference's vector<bool> result row, QueryResult.h:4).
  * GAT_RESULT_POINTS: per query, the sorted (trajectory id, point index) pairs in the box. */
@@ -144,6 +144,18 @@ int gat_grid_build(gat_ctx* ctx, const gat_db* db, gat_mbb range, float cell_siz
 int gat_stig_build(gat_ctx* ctx, const gat_db* db, int block_size, gat_index** out);
 /* FSG::FSG(range, cell_size) + addDatasetToGrid (FSG.cpp:7-143) */
 int gat_fsg_build(gat_ctx* ctx, const gat_db* db, gat_mbb range, float cell_size, gat_index** out);
+/* MortonGrid (MortonGrid.h:27, MortonGrid::buildQuadTree MortonGrid.cpp:238-259): the same
+ * quadtree as `grid`, kept as an implicit tree (a leaf bitmap over node ids (level, id) plus the
+ * first point of every Morton cell) and walked by computing each node's box from its corner
+ * cells (MortonGrid::generateMBBfromNode, MortonGrid.cpp:261-265) instead of reading stored node
+ * boxes. It answers gat_range_query (MortonGrid::rangeQueryBatch, MortonGrid.cpp:268-312) with
+ * the Grid's results and reads the Grid's point arrays: destroy it before the Grid. Not part of
+ * index snapshots (rebuild it from a loaded Grid). Grids of more than 4^13 cells give GAT_ERR_ARG. */
+int gat_morton_grid_build(gat_ctx* ctx, const gat_index* grid, gat_index** out);
+/* The MortonGrid's leaves as (level, id) pairs in bitmap order; *count receives their number
+ * (GAT_ERR_TRUNCATED when capacity is smaller). */
+int gat_morton_grid_leaves(gat_ctx* ctx, const gat_index* morton, int32_t* level, int32_t* id, int64_t capacity,
+                           int64_t* count);
 void gat_index_destroy(gat_index* index);
 /* info[0] = kind, [1] = points, [2] = leaves / blocks / cells, [3] = nodes, [4] = axis or
  * cells along x, [5] = cells along y, [6] = device bytes */

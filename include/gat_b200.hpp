@@ -192,6 +192,24 @@ public:
     float cell_size;
 };
 
+/* MortonGrid.h:46 MortonGrid(range, cell_size, VITURAL_CELL_PARAM) + addDatasetToGrid: the Grid's
+ * cells and point order with the quadtree kept as a leaf bitmap over implicit node ids
+ * (gat_morton_grid_build over a Grid it owns). */
+class MortonGrid : public Index {
+public:
+    MortonGrid(Context& c, const MBB& mbb, float val_cell_size, int VITURAL_CELL_PARAM = 2, int leafCap = 512)
+        : Index(c, GAT_INDEX_MORTON), grid(c, mbb, val_cell_size, VITURAL_CELL_PARAM, leafCap) {}
+    ~MortonGrid() override {
+        if (h) gat_index_destroy(h); /* before its Grid */
+        h = nullptr;
+    }
+    int addDatasetToGrid(const Trajectory* db, int traNum) {
+        int rc = grid.addDatasetToGrid(db, traNum);
+        return rc != GAT_OK ? rc : gat_morton_grid_build(ctx.h, grid.h, &h);
+    }
+    Grid grid;
+};
+
 /* PreProcess::readTraFromFormatedFile (PreProcess.cpp:224-315): the formatted trajectory file
  * into tradb[1..n] (tradb[0] empty, as the reference's global table) and the file's box. */
 inline int readTrajectoryFile(const char* path, std::vector<Trajectory>& tradb, MBB* range = nullptr) {
@@ -271,13 +289,14 @@ inline int range_query(const Index& ix, const MBB* q, int nq, int kind, int exec
 class SystemTest {
 public:
     SystemTest() = default;
-    SystemTest(const Trajectory* tradb_, Grid* g_, STIG* stig_, FSG* fsg_)
-        : tradb(tradb_), g(g_), stig(stig_), fsg(fsg_) {}
+    SystemTest(const Trajectory* tradb_, Grid* g_, STIG* stig_, FSG* fsg_, MortonGrid* mgrid_ = nullptr)
+        : tradb(tradb_), g(g_), stig(stig_), fsg(fsg_), mgrid(mgrid_) {}
 
     const Trajectory* tradb = nullptr;
     Grid* g = nullptr;
     STIG* stig = nullptr;
     FSG* fsg = nullptr;
+    MortonGrid* mgrid = nullptr;
     MBB rangeQueryMBB;
     int rangeQueryNum = 0;
     int similarityScale = 0;
@@ -292,14 +311,18 @@ public:
     int rangeQueryTest(MBB mbb, int num) { return repeat_range(g, "", mbb, num); }
     int STIGrangeQueryTest(MBB mbb, int num) { return repeat_range(stig, " STIG", mbb, num); }
     int FSGrangeQueryTest(MBB mbb, int num) { return repeat_range(fsg, " FSG", mbb, num); }
-    /* SystemTest.h:29 and :33. The reference's two ablations of the GT-quadtree change only how
-     * its points and tree are laid out: rangeQueryBatchGPUWithoutMorton (Grid.cpp:544-662) walks
-     * the Morton-ordered points through per-block segment lists as if they were row-major, and
-     * MortonGrid (MortonGrid.cpp:238-400) replaces the node pointers with a leaf bitmap over
-     * implicit node ids, under the same leaf rule. Both return the Grid's trajectory-id sets, so
-     * here both run the GT-quadtree path. */
+    /* SystemTest.h:29. The reference's rangeQueryBatchGPUWithoutMorton (Grid.cpp:544-662) walks
+     * the Grid's Morton-ordered points through per-block segment lists that pretend to be
+     * row-major; every segment starts at offset 0 of its block (the offset it pushes is never
+     * advanced, Grid.cpp:818-827), so it rescans each block's first points and its results are
+     * not the Grid's. There is no correct answer of its own to reproduce; this runs the
+     * GT-quadtree path. */
     int rangeQueryTestWithoutMorton(MBB mbb, int num) { return repeat_range(g, " (without Morton)", mbb, num); }
-    int MortonGridRangeQueryTest(MBB mbb, int num) { return repeat_range(g, " Morton Grid", mbb, num); }
+    /* SystemTest.h:33 (SystemTest.cpp:386-425): the MortonGrid's implicit-tree walk; its id sets
+     * are the Grid's. Without a MortonGrid the Grid answers. */
+    int MortonGridRangeQueryTest(MBB mbb, int num) {
+        return repeat_range(mgrid ? static_cast<Index*>(mgrid) : static_cast<Index*>(g), " Morton Grid", mbb, num);
+    }
 
     /* SystemTest.h:30: similarityScale copies of t against the grid's set */
     int similarityQueryTest(const Trajectory& t, int scale, int k) {

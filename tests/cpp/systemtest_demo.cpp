@@ -68,7 +68,11 @@ int main(int argc, char** argv) {
         rc = rc ? rc : fsg.addDatasetToGrid(tradb.data(), n);
         printf("build %d\n", rc);
         if (rc) return 3;
-        gat::SystemTest st(tradb.data(), &g, &stig, &fsg);
+        /* the MortonGrid needs a device (GAT_ERR_STATE on a host-only context) */
+        gat::MortonGrid mgrid(ctx, range, 0.01f, 2, 512);
+        const int mrc = mgrid.addDatasetToGrid(tradb.data(), n);
+        printf("mortonbuild %d\n", mrc);
+        gat::SystemTest st(tradb.data(), &g, &stig, &fsg, mrc == GAT_OK ? &mgrid : nullptr);
         st.verbose = false;
         st.epsilon = 5e-4;
         const gat::MBB q(121.40f, 31.00f, 121.45f, 31.06f);

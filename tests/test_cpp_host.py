@@ -1,5 +1,5 @@
 """The C++ host layer (include/gat_b200.hpp): a GAT-style program using gat::SystemTest, Grid,
-STIG and FSG over the C ABI, compiled with g++ and checked against the oracle."""
+STIG, FSG and MortonGrid over the C ABI, compiled with g++ and checked against the oracle."""
 import os
 import subprocess
 
@@ -28,7 +28,7 @@ def run(exe, device, n=2000, path=None):
     out = {}
     for line in r.stdout.splitlines():
         f = line.split()
-        if len(f) >= 2 and f[0] in ("build", "rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest",
+        if len(f) >= 2 and f[0] in ("build", "mortonbuild", "rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest",
                                     "rangeQueryTestWithoutMorton", "MortonGridRangeQueryTest", "rangeQueryBatch",
                                     "similarityQueryTest", "file_roundtrip", "tuning"):
             out[f[0]] = int(f[1])
@@ -44,6 +44,7 @@ def test_host_only(demo, tmp_path):
     rc, out, log = run(demo, -1, path=str(tmp_path / "tradb.txt"))
     assert rc == 0, log
     assert out["build"] == 0 and out["file_roundtrip"] == 1 and out["tuning"] == 3
+    assert out["mortonbuild"] == L.GAT_ERR_STATE
     for k in ("rangeQueryTest", "STIGrangeQueryTest", "FSGrangeQueryTest", "rangeQueryTestWithoutMorton",
               "MortonGridRangeQueryTest", "rangeQueryBatch", "similarityQueryTest"):
         assert out[k] == L.GAT_ERR_STATE, (k, log)
@@ -55,6 +56,7 @@ def test_systemtest_matches_oracle(demo):
 
     rc, out, log = run(demo, 0)
     assert rc == 0, log
+    assert out["mortonbuild"] == 0  # MortonGridRangeQueryTest below runs the MortonGrid
     t = D.walks(D.lengths(2000, 0, 0, 0, 20, 200, 0), 0)
     q = np.array([[121.40, 31.00, 121.45, 31.06]], np.float32)
     off, ids = po.OracleGrid(t, D.BOX, 0.01, 2, 512).range(q, 0)

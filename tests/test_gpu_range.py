@@ -152,3 +152,43 @@ def test_plain_truncation_reports_needed(gpu_ctx, c1):
     assert e.value.status == 4
     again = g.range_query(q[:60], execution="plain")
     assert np.array_equal(again.offsets, full.offsets) and np.array_equal(again.tids, full.tids)
+
+
+@pytest.mark.parametrize("cell,cap", [(0.01, 512), (0.02, 1), (0.02, 10_000_000), (0.005, 64)])
+def test_morton_grid_leaves_and_results(gpu_ctx, c1, cell, cap):
+    """MortonGrid (MortonGrid.cpp:238-393): its leaf bitmap holds exactly the Grid's leaves as
+    (level, id) (the oracle's quadtree, Grid.cpp:58-94), and its implicit-tree walk with computed
+    node boxes returns the oracle's id sets and point lists, batched and plain."""
+    t, q, db = c1
+    g = G.Grid(gpu_ctx, db, D.BOX, cell, 2, cap)
+    m = G.MortonGrid(g)
+    o = po.OracleGrid(t, D.BOX, cell, 2, cap)
+    nd = o.nodes()
+    want = sorted(zip(nd["level"][nd["leaf"] == 1].tolist(), nd["id"][nd["leaf"] == 1].tolist()))
+    lv, ids = m.leaves()
+    assert sorted(zip(lv.tolist(), ids.tolist())) == want
+    assert m.info()["kind"] == 3 and m.info()["points"] == g.info()["points"]
+    off, tids = o.range(q, 0)
+    r = m.range_query(q)
+    assert np.array_equal(r.offsets, off) and np.array_equal(r.tids, tids)
+    qq = q[::11]
+    off, tids = o.range(qq, 0)
+    r = m.range_query(qq, execution="plain")
+    assert np.array_equal(r.offsets, off) and np.array_equal(r.tids, tids)
+    off, tid, pidx = o.range(qq, 1)
+    r = m.range_query(qq, "points")
+    assert csr_equal(r.offsets, r.tids, off, tid) and np.array_equal(r.pidx, pidx)
+    m.close()
+    g.close()
+
+
+def test_morton_grid_rejects_other_kinds(gpu_ctx, c1):
+    t, q, db = c1
+    f = G.FSG(gpu_ctx, db, D.BOX, 0.01)
+    with pytest.raises(G.GatError) as e:
+        G.MortonGrid(f)
+    assert e.value.status == 1
+    g = G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512)
+    m = G.MortonGrid(g)
+    with pytest.raises(G.GatError):
+        m.save("/tmp/gat_morton_snapshot.bin")
