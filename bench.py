@@ -1371,6 +1371,19 @@ def run_suite(args, world, rank, local, td):
     plain_ids = d_tid[:int(plain_off[-1])].cpu().numpy()
     ptot = max_over_ranks(td, sum(pms), dev)
     plain_qps = ps * world * len(pms) / (ptot / 1e3)
+    # ---- config 1 in both forms (10k walks, 1k squares of 0.01 deg): the plain form's own workload
+    t1, q1 = D.config1(seed=0, n=C1["n"], nq=C1["nq"])
+    db1 = G.TrajectorySet(ctx, t1)
+    g1 = G.Grid(ctx, db1, G.BOX, C1["cell"], 2, C1["leaf_cap"])
+    d_q1 = torch.from_numpy(q1).to(dev)
+    H.time(lambda: call(g1, d_q1, len(q1), L.GAT_EXEC_PLAIN))
+    c1_pms = [H.time(lambda: call(g1, d_q1, len(q1), L.GAT_EXEC_PLAIN)) for _ in range(max(1, min(args.steps, 5)))]
+    c1_off = d_off[:len(q1) + 1].cpu().numpy()
+    c1_ids = d_tid[:int(c1_off[-1])].cpu().numpy()
+    H.time(lambda: call(g1, d_q1, len(q1)))
+    c1_bms = [H.time(lambda: call(g1, d_q1, len(q1))) for _ in range(max(1, min(args.steps, 5)))]
+    c1_plain = len(q1) * world * len(c1_pms) / (max_over_ranks(td, sum(c1_pms), dev) / 1e3)
+    c1_batched = len(q1) * world * len(c1_bms) / (max_over_ranks(td, sum(c1_bms), dev) / 1e3)
     # ---- end to end through the host-buffer call (pinned host rectangles in, id sets out)
     h_q = torch.from_numpy(q).pin_memory()
     h_off = torch.empty(nq + 1, dtype=torch.int64).pin_memory()
@@ -1417,6 +1430,9 @@ def run_suite(args, world, rank, local, td):
                       "form": "gat_range_query_dev with GAT_EXEC_PLAIN: one query per launch sequence",
                       "sample": f"every {nq // ps}th of the 100k rectangles"},
             "batched_over_plain": round(value / plain_qps, 1),
+            "c1": {"workload": "10k walks U[20,200], 1k squares of 0.01 deg, cell 0.01, leaf cap 512, GT-quadtree",
+                   "plain_queries_per_s": round(c1_plain, 1), "batched_queries_per_s": round(c1_batched, 1),
+                   "batched_over_plain": round(c1_batched / c1_plain, 1)},
         },
         "edr": edr,
         "served": {"requests_per_load": args.c5_requests, "saturation": c5["saturation"], "loads": c5["loads"],
@@ -1437,12 +1453,14 @@ def run_suite(args, world, rank, local, td):
         f_off, f_ids = of.range(q[psel])
         p_off, p_ids = sample_rows(plain_off, plain_ids, np.arange(0, ps, max(1, ps // pq))[:pq])
         po_off, po_ids = og.range(q[sel][np.arange(0, ps, max(1, ps // pq))[:pq]])
+        c1o_off, c1o_ids = po.OracleGrid(t1, G.BOX, C1["cell"], 2, C1["leaf_cap"]).range(q1)
         checks = {"grid_batched": bool(np.array_equal(g_off, o_off) and np.array_equal(g_ids, o_ids)),
+                  "c1_plain": bool(np.array_equal(c1_off, c1o_off) and np.array_equal(c1_ids, c1o_ids)),
                   "fsg_batched": bool(np.array_equal(fsg_r.offsets, f_off) and np.array_equal(fsg_r.tids, f_ids)),
                   "morton_batched": bool(np.array_equal(morton_r.offsets, o_off) and np.array_equal(morton_r.tids, o_ids)),
                   "grid_plain": bool(np.array_equal(p_off, po_off) and np.array_equal(p_ids, po_ids)),
                   "edr_batched": edr.pop("_parity_ok")}
-        line["parity"] = {"checked": {"range_queries": int(pq), "edr_pairs": int(edr["pairs"])},
+        line["parity"] = {"checked": {"range_queries": int(pq), "c1_plain_queries": int(len(q1)), "edr_pairs": int(edr["pairs"])},
                           "against": "oracle restatement (pinned to the reference's compiled CPU code by the CPU tests)",
                           "stig": "checked against the oracle by tests/test_gpu_configs.py (its oracle build takes minutes)",
                           "cases": checks, "equal": all(checks.values())}

@@ -95,6 +95,20 @@ int check_device_flag(gat_ctx* ctx, const char* what) {
     return fail(ctx, flag, std::string(what) + ": device reported status " + std::to_string(flag));
 }
 
+int ctx_use_priority_stream(gat_ctx* ctx) {
+    if (!ctx || ctx->device < 0) return GAT_OK;
+    int least = 0, greatest = 0;
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "priority stream");
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    ctx->stream = s;
+    return GAT_OK;
+}
+
 bool same_owner(const gat_ctx* owner, const gat_ctx* user) {
     const gat_ctx* a = owner->root ? owner->root : owner;
     const gat_ctx* b = user->root ? user->root : user;

@@ -622,7 +622,8 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     cudaStream_t s = ctx->stream;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr_tiles<R, COL, Src>, kTileWarps * 32, 0);
-    const int grid = ctx->sm_count * (per_sm > 0 ? per_sm : 1);
+    /* a serving lane leaves sm_reserve SMs free of this persistent grid for other streams */
+    const int grid = std::max(1, ctx->sm_count - ctx->sm_reserve) * (per_sm > 0 ? per_sm : 1);
     /* carry rows run along the step side; tiles are cut along the lane side */
     const int max_lane = COL ? max_cols : max_rows, max_step = COL ? max_rows : max_cols;
     const int stride = max_step + 2;

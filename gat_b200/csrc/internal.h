@@ -111,6 +111,7 @@ struct gat_ctx {
     int index_build = 0;                 /* 0 = device when present, 1 = host, 2 = device */
     int dep_launch = 1;                  /* programmatic dependent launch on the query path */
     int test_stall_pair = 0;             /* GAT_TUNE_TEST_STALL_CARRY (tests of the bounded wait) */
+    int sm_reserve = 0;                  /* SMs the persistent EDR kernel leaves to other streams (serving lanes) */
     cudaMemPool_t build_pool = nullptr;  /* index-build temporaries, kept for reuse until gat_ctx_trim */
     std::map<uint64_t, int> edr_tune; /* worker contexts use their root's table */
     std::mutex tune_mu;
@@ -203,6 +204,8 @@ void timed_end(gat_ctx* ctx, int cls, double work);
 /* device-side work counter for classes whose work is only known on the device (EDR cells) */
 void timed_add_work(gat_ctx* ctx, int cls, double work);
 
+/* replaces the context's (still unused) stream by one of the device's greatest priority */
+int ctx_use_priority_stream(gat_ctx* ctx);
 /* GAT_ERR_STATE for a host-only context (device -1) */
 int require_device(gat_ctx* ctx, const char* what);
 /* Opts a kernel into `bytes` of dynamic shared memory when that (plus the kernel's few KB of

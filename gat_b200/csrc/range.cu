@@ -199,14 +199,17 @@ __device__ bool morton_walk(const MortonDev& m, const Box& q, Emit emit, int lev
  * intersection tests, and walks the subtree it reaches; a leaf met on the way belongs to the
  * thread whose remaining digits are all zero. FSG rows are dealt round robin. Concatenated in
  * thread order the items are the sequential traversal's, cut at subtree boundaries. */
-constexpr int kGridDepth = 3, kStigDepth = 6, kSub = 64;
+constexpr int kGridDepth = 3, kSub = 64;
+/* plain execution walks one query with 1024 threads: the split goes two levels deeper */
+constexpr int kPlainDepth = 5, kPlainSub = 1024;
 
 /* The candidate ranges of sub-thread `sub` of a query, joined and cut into items. Writes them
  * to items[0..] when items is non-NULL; returns how many there are. Sets GAT_ERR_ARG in flag when
  * a walk's stack overflows. */
-template <int KIND>
+template <int KIND, int GD = kGridDepth>
 __device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& f, const MortonDev& m, const Box& q,
                               int sub, int2* items, int32_t* flag) {
+    constexpr int SD = 2 * GD, NSUB = 1 << (2 * GD); /* STIG levels and threads of the split */
     int64_t cnt = 0;
     /* Ranges that continue the previous one (neighbouring leaves / cells are contiguous in the
      * index's point order) are joined, and everything is cut into chunks of at most kChunk
@@ -236,14 +239,14 @@ __device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& 
     if (KIND == GAT_INDEX_GRID) {
         int nd = 0; /* the root is taken without a test (Grid.cpp:428-446) */
         bool walk = true;
-        for (int lev = 0; lev < kGridDepth && walk; lev++) {
+        for (int lev = 0; lev < GD && walk; lev++) {
             const int ch = g.node_child[nd];
             if (ch < 0) {
-                if ((sub & ((1 << (2 * (kGridDepth - lev))) - 1)) == 0) emit(g.node_pbeg[nd], g.node_pend[nd]);
+                if ((sub & ((1 << (2 * (GD - lev))) - 1)) == 0) emit(g.node_pbeg[nd], g.node_pend[nd]);
                 walk = false;
                 break;
             }
-            const int c = ch + ((sub >> (2 * (kGridDepth - 1 - lev))) & 3);
+            const int c = ch + ((sub >> (2 * (GD - 1 - lev))) & 3);
             const float4 m = g.node_mbb[c];
             if (!box_intersect(q, Box{m.x, m.y, m.z, m.w})) walk = false;
             nd = c;
@@ -253,9 +256,9 @@ __device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& 
     if (KIND == GAT_INDEX_STIG) {
         int nd = 0;
         bool walk = true;
-        for (int lev = 0; lev < kStigDepth && walk; lev++) {
+        for (int lev = 0; lev < SD && walk; lev++) {
             if (s.kind[nd]) {
-                if ((sub & ((1 << (kStigDepth - lev)) - 1)) == 0) {
+                if ((sub & ((1 << (SD - lev)) - 1)) == 0) {
                     const float4 m = s.mbb[nd];
                     if (box_intersect(Box{m.x, m.y, m.z, m.w}, q)) emit(s.lo[nd], s.hi[nd] + 1);
                 }
@@ -265,25 +268,25 @@ __device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& 
             const float lo = s.dim[nd] == 0 ? q.xmin : q.ymin;
             const float hi = s.dim[nd] == 0 ? q.xmax : q.ymax;
             const float med = s.median[nd];
-            const bool right = (sub >> (kStigDepth - 1 - lev)) & 1;
+            const bool right = (sub >> (SD - 1 - lev)) & 1;
             const bool go = right ? (!(hi < med) && !(lo > 180.0f)) : (!(hi < 0.0f) && !(lo > med));
             if (!go) walk = false;
             nd = right ? s.right[nd] : s.left[nd];
         }
         if (walk) ok = stig_walk(s, q, emit, nd);
     }
-    if (KIND == GAT_INDEX_FSG) fsg_walk(f, q, emit, sub, kSub);
+    if (KIND == GAT_INDEX_FSG) fsg_walk(f, q, emit, sub, NSUB);
     if (KIND == GAT_INDEX_MORTON) {
         int level = 0; /* the Grid's digit split over the implicit nodes */
         uint32_t id = 0;
         bool walk = true;
-        for (int lev = 0; lev < kGridDepth && walk; lev++) {
+        for (int lev = 0; lev < GD && walk; lev++) {
             if (morton_leaf(m, level, id)) {
-                if ((sub & ((1 << (2 * (kGridDepth - lev))) - 1)) == 0) morton_emit(m, level, id, emit);
+                if ((sub & ((1 << (2 * (GD - lev))) - 1)) == 0) morton_emit(m, level, id, emit);
                 walk = false;
                 break;
             }
-            const uint32_t cid = (id << 2) + (uint32_t)((sub >> (2 * (kGridDepth - 1 - lev))) & 3);
+            const uint32_t cid = (id << 2) + (uint32_t)((sub >> (2 * (GD - 1 - lev))) & 3);
             if (!box_intersect(q, morton_box(m, level + 1, cid))) walk = false;
             level++;
             id = cid;
@@ -306,61 +309,168 @@ __global__ void k_items(GridDev g, StigDev s, FsgDev f, MortonDev m, const gat_m
     if (!ioff) icnt[tid] = cnt;
 }
 
-/* Plain execution, step 1 of 4 for query qi (one CTA of kSub threads): counts every
- * sub-thread's items, lays out the query's item offsets ioff[0..kSub] (the layout of a batch of
- * one), writes the items and clears the scan's counters. item_cap bounds the items of any
- * single query; a query beyond it (impossible with the bound the host computes) raises
- * GAT_ERR_ARG and scans nothing. */
+/* Plain execution (one query per launch sequence of three kernels, nothing waiting on the host
+ * in between), step 1: one CTA of kPlainSub threads walks query qi, each thread the subtree its
+ * digits select (two levels deeper than the batched split, so every thread's walk is short),
+ * counts its items, and after a block scan writes them at their offsets. ioff[0] receives the
+ * query's item count. item_cap bounds the items of any single query; a query beyond it
+ * (impossible with the bound the host computes) raises GAT_ERR_ARG and scans nothing. */
 template <int KIND>
-__global__ void __launch_bounds__(kSub) k_plain_items(GridDev g, StigDev s, FsgDev f, MortonDev m, const gat_mbb* queries, int qi,
-                                                      int64_t* ioff, int2* items, int64_t item_cap,
-                                                      unsigned long long* ctr, int32_t* flag) {
+__global__ void __launch_bounds__(kPlainSub) k_plain_items(GridDev g, StigDev s, FsgDev f, MortonDev m,
+                                                           const gat_mbb* queries, int qi, int64_t* ioff, int2* items,
+                                                           int64_t item_cap, int32_t* flag) {
     dep_wait();
-    __shared__ int64_t pre[kSub + 1];
+    __shared__ int64_t wsum[kPlainSub / 32 + 1];
     const Box q = load_box(queries, qi);
-    const int sub = threadIdx.x;
-    pre[sub] = walk_items<KIND>(g, s, f, m, q, sub, nullptr, flag);
-    if (sub < 4) ctr[sub] = 0ull;
+    const int sub = threadIdx.x, lane = sub & 31, warp = sub >> 5;
+    const int64_t c = walk_items<KIND, kPlainDepth>(g, s, f, m, q, sub, nullptr, flag);
+    int64_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
     __syncthreads();
     if (sub == 0) {
         int64_t run = 0;
-        for (int i = 0; i < kSub; i++) {
-            const int64_t c = pre[i];
-            pre[i] = run;
-            run += c;
+        for (int w = 0; w < kPlainSub / 32; w++) {
+            const int64_t t = wsum[w];
+            wsum[w] = run;
+            run += t;
         }
-        pre[kSub] = run;
+        wsum[kPlainSub / 32] = run;
     }
     __syncthreads();
-    const bool fits = pre[kSub] <= item_cap;
-    ioff[sub] = fits ? pre[sub] : 0;
-    if (sub == 0) ioff[kSub] = fits ? pre[kSub] : 0;
-    if (!fits) {
-        if (sub == 0) set_flag(flag, GAT_ERR_ARG);
-        return;
+    const int64_t total = wsum[kPlainSub / 32];
+    const bool fits = total <= item_cap;
+    if (sub == 0) {
+        ioff[0] = fits ? total : 0;
+        if (!fits) set_flag(flag, GAT_ERR_ARG);
     }
-    walk_items<KIND>(g, s, f, m, q, sub, items + pre[sub], flag);
+    if (fits) walk_items<KIND, kPlainDepth>(g, s, f, m, q, sub, items + wsum[warp] + x - c, flag);
 }
 
-/* Plain execution, step 4 of 4: the query's sorted ids (arena[segbase[0]..], segcnt[0] of them)
- * go to out_tid[off[qi]..] and off[qi + 1] = off[qi] + count. When they do not fit `capacity`,
- * nothing is written and trunc[0] is set; the offsets keep counting. */
-__global__ void k_plain_emit(int qi, const int64_t* __restrict__ segbase, const int64_t* __restrict__ segcnt,
-                             const uint32_t* __restrict__ arena, int64_t* off, int32_t* out_tid, int64_t capacity,
-                             int32_t* trunc) {
+/* Plain execution, step 2: warps of the whole grid take the query's items (ioff[0] of them) and
+ * mark the trajectory id of every run of hits (MBB::pInBox, MBB.cpp:21-26) in a bitmap over the
+ * set's ids, with 128-bit loads of x / y / tid. work (optional) accumulates algorithmic bytes. */
+__global__ void __launch_bounds__(kThreads) k_plain_scan(const gat_mbb* queries, int qi, const int64_t* __restrict__ ioff,
+                                                         const int2* __restrict__ items, const float* __restrict__ X,
+                                                         const float* __restrict__ Y, const int32_t* __restrict__ tid,
+                                                         uint32_t* bitmap, unsigned long long* work) {
     dep_wait();
-    const int64_t o = qi == 0 ? 0 : off[qi];
-    const int64_t n = segcnt[0];
-    if (threadIdx.x == 0) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t nitems = ioff[0];
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const Box q = load_box(queries, qi);
+    unsigned long long cand = 0, hits = 0;
+    auto mark = [&](int t) { atomicOr(bitmap + (t >> 5), 1u << (t & 31)); };
+    for (int64_t it = gw; it < nitems; it += nw) {
+        const int2 r = items[it];
+        if (lane == 0) cand += (unsigned long long)(r.y - r.x);
+        const int head_end = min(r.y, (r.x + 3) & ~3);
+        const int vb = head_end, ve = head_end + ((r.y - head_end) & ~3);
+        for (int i = r.x + lane; i < head_end; i += 32)
+            if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
+                mark(__ldg(tid + i));
+                hits++;
+            }
+        for (int i = ve + lane; i < r.y; i += 32)
+            if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
+                mark(__ldg(tid + i));
+                hits++;
+            }
+        const float4* X4 = reinterpret_cast<const float4*>(X + vb);
+        const float4* Y4 = reinterpret_cast<const float4*>(Y + vb);
+        const int4* T4 = reinterpret_cast<const int4*>(tid + vb);
+        const int nv = (ve - vb) >> 2;
+        int carry = -1;
+        for (int k0 = 0; k0 < nv; k0 += 32) {
+            const int k = k0 + lane;
+            int t0 = -1, t1 = -1, t2 = -1, t3 = -1;
+            if (k < nv) {
+                const float4 x = __ldg(X4 + k), y = __ldg(Y4 + k);
+                const bool h0 = in_box(q, x.x, y.x), h1 = in_box(q, x.y, y.y);
+                const bool h2 = in_box(q, x.z, y.z), h3 = in_box(q, x.w, y.w);
+                if (h0 | h1 | h2 | h3) {
+                    const int4 tt = __ldg(T4 + k);
+                    t0 = h0 ? tt.x : -1;
+                    t1 = h1 ? tt.y : -1;
+                    t2 = h2 ? tt.z : -1;
+                    t3 = h3 ? tt.w : -1;
+                    hits += (unsigned long long)(h0 + h1 + h2 + h3);
+                }
+            }
+            /* one mark per run of hits of one trajectory */
+            int prev = __shfl_up_sync(FULL, t3, 1);
+            if (lane == 0) prev = carry;
+            carry = __shfl_sync(FULL, t3, 31);
+            if (t0 >= 0 && t0 != prev) mark(t0);
+            if (t1 >= 0 && t1 != t0) mark(t1);
+            if (t2 >= 0 && t2 != t1) mark(t2);
+            if (t3 >= 0 && t3 != t2) mark(t3);
+        }
+    }
+    if (work) {
+        unsigned long long w = 8ull * cand + 4ull * hits;
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(FULL, w, o);
+        if (lane == 0 && w) atomicAdd(work, w);
+    }
+}
+
+/* Plain execution, step 3 (one CTA of kPlainSub threads): the bitmap's ids in ascending order
+ * go to out_tid[off[qi]..] and off[qi + 1] = off[qi] + count; the words are cleared for the next
+ * query. When the ids do not fit `capacity`, nothing is written and trunc[0] is set; the offsets
+ * keep counting. */
+__global__ void __launch_bounds__(kPlainSub) k_plain_emit(int qi, uint32_t* bitmap, int words, int64_t* off,
+                                                          int32_t* out_tid, int64_t capacity, int32_t* trunc) {
+    dep_wait();
+    __shared__ int wsum[kPlainSub / 32 + 1];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int per = (words + kPlainSub - 1) / kPlainSub;
+    const int w0 = min(words, t * per), w1 = min(words, w0 + per);
+    int c = 0;
+    for (int w = w0; w < w1; w++) c += __popc(bitmap[w]);
+    int x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (t == 0) {
+        int run = 0;
+        for (int w = 0; w < kPlainSub / 32; w++) {
+            const int v = wsum[w];
+            wsum[w] = run;
+            run += v;
+        }
+        wsum[kPlainSub / 32] = run;
+    }
+    __syncthreads();
+    const int64_t base = qi == 0 ? 0 : off[qi];
+    const int64_t total = wsum[kPlainSub / 32];
+    __syncthreads(); /* every thread has read off[qi] before it is rewritten below (qi == 0) */
+    if (t == 0) {
         if (qi == 0) off[0] = 0;
-        off[qi + 1] = o + n;
+        off[qi + 1] = base + total;
+        if (base + total > capacity) *trunc = 1;
     }
-    if (o + n > capacity) {
-        if (threadIdx.x == 0) *trunc = 1;
-        return;
+    const bool write = base + total <= capacity;
+    int64_t o = base + wsum[warp] + x - c;
+    for (int w = w0; w < w1; w++) {
+        uint32_t v = bitmap[w];
+        if (!v) continue;
+        bitmap[w] = 0u;
+        if (!write) continue;
+        while (v) {
+            const int b = __ffs(v) - 1;
+            v &= v - 1;
+            out_tid[o++] = w * 32 + b;
+        }
     }
-    const uint32_t* src = arena + segbase[0];
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) out_tid[o + i] = (int32_t)src[i];
 }
 
 /* ---------------------------------------------------------------- block helpers */
@@ -1010,11 +1120,10 @@ int run_gather(gat_ctx* ctx, const gat_index* ix, int nq, int mode, const int64_
 }
 
 
-/* Plain execution of id-set queries: one query per launch sequence of four kernels (items,
- * hash scan, bitmap scan for a query beyond the hash set, emit), chained as dependent launches.
- * Every buffer is sized for any single query before the first launch (items by the index's
- * candidate-range bound, the result arena by the set's trajectory count), so nothing waits on
- * the host between queries; one synchronisation at the end reads the total and the status. */
+/* Plain execution of id-set queries: per query three dependent launches (items, scan, emit),
+ * every buffer sized for any single query before the first launch (items by the index's
+ * candidate-range bound, the id bitmap by the set's trajectory count), so nothing waits on the
+ * host between queries; one synchronisation at the end reads the total and the status. */
 int run_plain_ids(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int64_t* d_off, int32_t* d_tid,
                   int64_t capacity, int64_t* needed) {
     cudaStream_t s = ctx->stream;
@@ -1022,53 +1131,40 @@ int run_plain_ids(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq,
     /* items of one query: every candidate range (a leaf, a block, or a row of cells) yields its
      * points in chunks of kChunk - 3 or more points, plus one partial chunk */
     const int64_t ranges = ix->kind == GAT_INDEX_FSG ? (int64_t)ix->fsg.ny + 2 : std::max<int64_t>(ix->leaves, 1);
-    const int64_t item_cap = 2 * ranges + ix->npoints / (kChunk - 4) + 2 * kSub + 16;
-    const int64_t acap = (int64_t)ix->db->n + 1; /* distinct ids of one query */
-    int64_t* ioff = (int64_t*)scratch(ctx, S_RANGE_IOFF, (kSub + 1) * sizeof(int64_t), &st);
-    int2* items = (int2*)scratch(ctx, S_RANGE_ITEMS, (size_t)(item_cap + 1) * sizeof(int2), &st);
-    int64_t* segbase = (int64_t*)scratch(ctx, S_RANGE_SEGBASE, 2 * sizeof(int64_t), &st);
-    int64_t* segcnt = (int64_t*)scratch(ctx, S_RANGE_SEGCNT, 2 * sizeof(int64_t), &st);
-    /* cursor: [0] arena, [1] per-query work, [2] query counter, [3] overflowed (cleared per
-     * query), [4] truncation word, [5] work of the whole call */
-    unsigned long long* cursor = (unsigned long long*)scratch(ctx, S_RANGE_CURSOR, 64, &st);
-    int* ovf_list = (int*)scratch(ctx, S_RANGE_OVF, 2 * sizeof(int), &st);
-    uint32_t* arena = (uint32_t*)scratch(ctx, S_RANGE_ARENA, (size_t)acap * 4, &st);
-    if (!ioff || !items || !segbase || !segcnt || !cursor || !ovf_list || !arena) return st;
+    const int64_t item_cap = 2 * ranges + ix->npoints / (kChunk - 4) + 2 * kPlainSub + 16;
     const int words = (ix->db->n + 1 + 31) / 32;
-    const size_t smem_bm = (size_t)words * 4;
-    const bool bm_in_smem = smem_bm <= 200 * 1024;
-    uint32_t* gbm = nullptr;
-    if (!bm_in_smem && !(gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, smem_bm, &st))) return st;
-    const size_t smem_hs = (size_t)(kHashSize + kHashMax) * sizeof(int);
-    allow_smem(k_range_hash, smem_hs);
-    if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
+    int64_t* ioff = (int64_t*)scratch(ctx, S_RANGE_IOFF, 2 * sizeof(int64_t), &st);
+    int2* items = (int2*)scratch(ctx, S_RANGE_ITEMS, (size_t)(item_cap + 1) * sizeof(int2), &st);
+    uint32_t* bitmap = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, (size_t)words * 4, &st);
+    /* cursor: [0] truncation word, [1] work of the whole call */
+    unsigned long long* cursor = (unsigned long long*)scratch(ctx, S_RANGE_CURSOR, 64, &st);
+    if (!ioff || !items || !bitmap || !cursor) return st;
+    GAT_CUDA_TRY(ctx, cudaMemsetAsync(bitmap, 0, (size_t)words * 4, s), "range");
     GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 64, s), "range");
-    int32_t* trunc = reinterpret_cast<int32_t*>(cursor + 4);
-    unsigned long long* work = ctx->timing ? cursor + 5 : nullptr;
+    int32_t* trunc = reinterpret_cast<int32_t*>(cursor);
+    unsigned long long* work = ctx->timing ? cursor + 1 : nullptr;
     auto items_kernel = ix->kind == GAT_INDEX_GRID     ? k_plain_items<GAT_INDEX_GRID>
                         : ix->kind == GAT_INDEX_STIG   ? k_plain_items<GAT_INDEX_STIG>
                         : ix->kind == GAT_INDEX_MORTON ? k_plain_items<GAT_INDEX_MORTON>
                                                        : k_plain_items<GAT_INDEX_FSG>;
+    const int scan_grid = ctx->sm_count;
     for (int qi = 0; qi < nq; qi++) {
-        cudaError_t e = launch_dep(ctx, items_kernel, dim3(1), dim3(kSub), 0, s, ix->grid, ix->stig, ix->fsg, ix->morton,
-                                   d_q, qi, ioff, items, item_cap, cursor, ctx->d_flag);
+        cudaError_t e = launch_dep(ctx, items_kernel, dim3(1), dim3(kPlainSub), 0, s, ix->grid, ix->stig, ix->fsg,
+                                   ix->morton, d_q, qi, ioff, items, item_cap, ctx->d_flag);
         timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
         if (e == cudaSuccess)
-            e = launch_dep(ctx, k_range_hash, dim3(1), dim3(kThreads), smem_hs, s, d_q + qi, 1, ioff, items, ix->d_x,
-                           ix->d_y, ix->d_tid, arena, acap, cursor, segbase, segcnt, ovf_list, work, (const int*)nullptr);
-        if (e == cudaSuccess)
-            e = launch_dep(ctx, k_range_ids, dim3(1), dim3(kThreads), bm_in_smem ? smem_bm : 0, s, d_q + qi, 0, ioff,
-                           items, ix->d_x, ix->d_y, ix->d_tid, words, gbm, arena, acap, cursor, segbase, segcnt, work,
-                           ovf_list, cursor + 3);
+            e = launch_dep(ctx, k_plain_scan, dim3(scan_grid), dim3(kThreads), 0, s, d_q, qi, (const int64_t*)ioff,
+                           (const int2*)items, (const float*)ix->d_x, (const float*)ix->d_y, (const int32_t*)ix->d_tid,
+                           bitmap, work);
         timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
         if (e == cudaSuccess)
-            e = launch_dep(ctx, k_plain_emit, dim3(1), dim3(256), 0, s, qi, segbase, segcnt, arena, d_off, d_tid,
-                           capacity, trunc);
-        count_launch(ctx, 4);
+            e = launch_dep(ctx, k_plain_emit, dim3(1), dim3(kPlainSub), 0, s, qi, bitmap, words, d_off, d_tid, capacity,
+                           trunc);
+        count_launch(ctx, 3);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "range plain launch");
     }
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, d_off + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 1, cursor + 4, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 1, cursor, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
     if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
     *needed = ctx->h_pinned[0];
     if (ctx->timing) timed_add_work(ctx, GAT_KERNEL_RANGE_SCAN, (double)ctx->h_pinned[2]);

@@ -18,10 +18,12 @@
  * whose scratch arena exceeds its share of the budget (budget / lanes) frees it.
  *
  * Head-of-line blocking: a top-k batch runs for milliseconds, a range batch for well under one.
- * With two or more lanes, top-k batches may hold all lanes but one, so a range request never
- * waits behind top-k work for a lane; and a top-k batch stops growing once its queries hold
- * kTopkBatchPoints points (its DP work grows with them), so one batch of long queries cannot
- * hold a lane for long. */
+ * With two or more lanes, lane 0 runs range batches only, on a stream of the device's greatest
+ * priority, so a range request never waits behind top-k work for a lane; the other lanes leave
+ * an eighth of the SMs free of their persistent EDR grids, so the range kernels also find SMs
+ * while top-k work runs (a persistent grid holds its SMs until it ends); and a top-k batch stops
+ * growing once its queries hold kTopkBatchPoints points (its DP work grows with them), so one
+ * batch of long queries cannot hold a lane for long. */
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -79,7 +81,16 @@ struct gat_server {
     std::vector<Batch*> lane_batch;
     int64_t next_id = 0;
     int64_t reserved = 0;
-    int topk_running = 0; /* lanes running a top-k batch */
+    /* a free lane for a batch of this kind, or -1: with two or more lanes, lane 0 takes range
+     * batches only (and is preferred for them) */
+    int lane_for(int kind) const {
+        const int L = (int)lane_batch.size();
+        if (L < 2) return lane_batch[0] ? -1 : 0;
+        if (kind == REQ_RANGE && !lane_batch[0]) return 0;
+        for (int i = 1; i < L; i++)
+            if (!lane_batch[i]) return i;
+        return -1;
+    }
     bool stopping = false, lanes_stop = false;
     double hits_mean[3] = {4096, 4096, 4096};
     int64_t stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -122,9 +133,7 @@ struct gat_server {
     Batch* form_batch() {
         std::deque<Request*>* best = nullptr;
         int64_t best_t = INT64_MAX;
-        /* top-k batches leave one lane to range requests */
-        const bool topk_lane = lane_batch.size() < 2 || topk_running < (int)lane_batch.size() - 1;
-        if (!q_topk.empty() && topk_lane) {
+        if (!q_topk.empty() && lane_for(REQ_TOPK) >= 0) {
             best = &q_topk;
             best_t = q_topk.front()->t[0];
         }
@@ -183,7 +192,7 @@ struct gat_server {
                 if (!idle()) cv_sched.wait(lk);
                 continue;
             }
-            const int lane = free_lane();
+            const int lane = lane_for(b->kind);
             const int64_t t = now();
             for (Request* r : b->reqs) r->t[1] = t;
             reserved += b->reserve;
@@ -191,7 +200,6 @@ struct gat_server {
             stats[6] = std::max<int64_t>(stats[6], (int64_t)b->reqs.size());
             stats[2]++;
             stats[b->kind == REQ_TOPK ? 4 : 3]++;
-            if (b->kind == REQ_TOPK) topk_running++;
             lane_batch[lane] = b;
             cv_lane.notify_all();
         }
@@ -274,7 +282,6 @@ struct gat_server {
             if (gat_ctx_scratch_bytes(w) > cfg.budget_bytes / (int64_t)lanes.size()) gat_ctx_trim(w);
             std::lock_guard<std::mutex> lk(mu);
             reserved -= b->reserve;
-            if (b->kind == REQ_TOPK) topk_running--;
             lane_batch[i] = nullptr;
             delete b;
             cv_done.notify_all();
@@ -316,7 +323,19 @@ int gat_server_create(gat_ctx* ctx, const gat_index* grid, const gat_index* stig
             delete s;
             return fail(ctx, rc, "gat_server_create: worker context");
         }
+        /* lane 0 takes range batches on a high-priority stream; the others leave SMs to it */
+        if (c.lanes >= 2) {
+            if (i == 0)
+                rc = ctx_use_priority_stream(w);
+            else
+                w->sm_reserve = std::max(1, w->sm_count / 8);
+        }
         s->lanes.push_back(w);
+        if (rc != GAT_OK) {
+            for (gat_ctx* x : s->lanes) gat_ctx_destroy(x);
+            delete s;
+            return fail(ctx, rc, "gat_server_create: lane stream");
+        }
     }
     s->lane_batch.assign((size_t)c.lanes, nullptr);
     for (int i = 0; i < c.lanes; i++) s->workers.emplace_back([s, i] { s->run_lane(i); });

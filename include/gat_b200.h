@@ -262,9 +262,10 @@ int gat_topk_merge_dev(gat_ctx* ctx, int nq, int k, int nparts, const int32_t* d
  * worker contexts is free, from the queue whose head request is oldest (range requests grouped
  * by index and result kind, top-k requests by eps), and admits it only while the estimated
  * device bytes of all admitted batches stay within budget_bytes. Batches of different lanes
- * overlap on the device. With two or more lanes, top-k batches leave one lane to range requests
- * (which then never wait behind top-k work), and a top-k batch stops growing at 8192 query
- * points. Results equal those of the same request run alone. */
+ * overlap on the device. With two or more lanes, lane 0 runs range batches only, on a stream of
+ * the greatest priority, and the other lanes' persistent EDR grids leave an eighth of the SMs
+ * free, so range requests never wait behind top-k work; a top-k batch stops growing at 8192
+ * query points. Results equal those of the same request run alone. */
 typedef struct gat_server gat_server;
 typedef struct {
     int lanes;            /* worker contexts (streams) running batches concurrently; default 4 */
