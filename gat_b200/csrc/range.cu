@@ -630,26 +630,39 @@ __global__ void k_order_scatter(int nq, const int* __restrict__ bucket, unsigned
 }
 
 /* ---------------------------------------------------------------- id sets, hash form */
-/* Queries are taken from a counter by persistent CTAs. Each warp scans one candidate point
- * range at a time (128 points per step as float4 x / y / tid), tests MBB::pInBox, and inserts
- * the trajectory id of every hit that starts a run (the previous point is not a hit of the
- * same trajectory: a trajectory's points in one cell are contiguous in every index order)
- * into an open-addressing set in shared memory. The set is then compacted (which also clears
- * it), sorted (bitonic) and written to the arena. A query whose distinct ids exceed kHashMax
- * goes on the overflow list for the bitmap kernel; the result is the same set either way. */
+/* Queries are taken from a counter by persistent CTAs (the next query's index is fetched while
+ * the current one finishes). The CTA's warps take the query's candidate items from a
+ * shared-memory counter, scan each with 128-bit loads of x / y / tid (MBB::pInBox) and insert
+ * the trajectory id of every hit that starts a run (the previous point is not a hit of the same
+ * trajectory: a trajectory's points in one cell are contiguous in every index order) into an
+ * open-addressing set in shared memory; a successful insert also appends the id to a list, so
+ * the query's m distinct ids are known without scanning the set. The list is sorted (each warp
+ * sorts runs of 32 ids in registers, then every id's rank is its position in its run plus its
+ * lower bound in every other run; long lists use a block-wide bitonic sort) and written to the
+ * arena at the rank; the set is cleared by probing each listed id again. A query whose distinct
+ * ids exceed kHashMax goes on the overflow list for the bitmap kernel; the result is the same set
+ * either way. */
 constexpr int kHashBits = 13;
 constexpr int kHashSize = 1 << kHashBits; /* 32 KB of ids */
 constexpr int kHashMax = 4096;            /* distinct ids per query (load factor <= 1/2) */
+constexpr int kRankSortMax = 512;         /* lists up to this length are sorted by run ranks */
 
-__device__ __forceinline__ void hs_insert(int* tab, int t, int* count, int* ovf) {
-    unsigned h = ((unsigned)t * 2654435761u) >> (32 - kHashBits);
+__device__ __forceinline__ unsigned hs_slot(int t) { return ((unsigned)t * 2654435761u) >> (32 - kHashBits); }
+
+/* inserts t; a new id is appended to list (count: ids inserted; ovf: the list or a probe ran out) */
+__device__ __forceinline__ void hs_insert(int* tab, int* list, int t, int* count, int* ovf) {
+    unsigned h = hs_slot(t);
     for (int p = 0; p < 64; p++) {
         int v = tab[h];
         if (v == t) return;
         if (v == -1) {
             v = atomicCAS(&tab[h], -1, t);
             if (v == -1) {
-                if (atomicAdd(count, 1) >= kHashMax) *ovf = 1;
+                const int pos = atomicAdd(count, 1);
+                if (pos < kHashMax)
+                    list[pos] = t;
+                else
+                    *ovf = 1;
                 return;
             }
             if (v == t) return;
@@ -657,6 +670,43 @@ __device__ __forceinline__ void hs_insert(int* tab, int t, int* count, int* ovf)
         h = (h + 1) & (kHashSize - 1);
     }
     *ovf = 1;
+}
+
+/* empties the slot holding t (t is in the set) */
+__device__ __forceinline__ void hs_erase(int* tab, int t) {
+    unsigned h = hs_slot(t);
+    for (int p = 0; p < kHashSize; p++) {
+        if (tab[h] == t) {
+            tab[h] = -1;
+            return;
+        }
+        h = (h + 1) & (kHashSize - 1);
+    }
+}
+
+/* ascending sort of the 32 values of a warp (one per lane), bitonic network over shuffles */
+__device__ __forceinline__ int warp_sort32(int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool up = (lane & k) == 0;
+            const bool lower = (lane & j) == 0;
+            v = (lower == up) ? min(v, o) : max(v, o);
+        }
+    return v;
+}
+
+/* number of the 32 ascending values run[0..32) below x: a binary search over the first 31
+ * (it leaves lo = how many of them are below x), then the last */
+__device__ __forceinline__ int lower_bound32(const int* run, int x) {
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1)
+        if (run[lo + step - 1] < x) lo += step;
+    return lo + (run[31] < x ? 1 : 0);
 }
 
 __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queries, int nq, const int64_t* ioff,
@@ -668,31 +718,38 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
     dep_wait();
     extern __shared__ int hs_smem[];
     int* tab = hs_smem;              /* kHashSize */
-    int* buf = hs_smem + kHashSize;  /* kHashMax sorted ids */
-    __shared__ int sh[kThreads / 32 + 1];
-    __shared__ int cnt_sh, ovf_sh, q_sh;
+    int* buf = hs_smem + kHashSize;  /* kHashMax ids in insertion order */
+    __shared__ int cnt_sh, ovf_sh, q_sh, next_sh, item_sh;
     __shared__ unsigned long long base_sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     for (int i = threadIdx.x; i < kHashSize; i += blockDim.x) tab[i] = -1;
-    unsigned long long my_work = 0; /* algorithmic bytes of this thread, added once at exit */
     /* ctr: [0] arena cursor, [1] work bytes, [2] query counter, [3] overflow count */
+    auto fetch = [&]() {
+        const int j = (int)atomicAdd(&ctr[2], 1ull);
+        return j >= nq ? nq : (order ? order[j] : j);
+    };
+    if (threadIdx.x == 0) {
+        next_sh = fetch();
+        cnt_sh = 0;
+        ovf_sh = 0;
+        item_sh = 0;
+    }
+    unsigned long long my_work = 0; /* algorithmic bytes of this thread, added once at exit */
     for (;;) {
-        if (threadIdx.x == 0) {
-            const int j = (int)atomicAdd(&ctr[2], 1ull);
-            q_sh = j >= nq ? nq : (order ? order[j] : j);
-            cnt_sh = 0;
-            ovf_sh = 0;
-        }
-        __syncthreads();
-        const int qi = q_sh;
+        __syncthreads(); /* the set and list are clear, the next query is known */
+        const int qi = next_sh;
         if (qi >= nq) break;
         const Box q = load_box(queries, qi);
         const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
         unsigned long long cand = 0, hits = 0;
-        for (int64_t it = i0 + warp; it < i1; it += kThreads / 32) {
-            /* stop early once the set has overflowed (warp-uniform read) */
-            if (__shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
+        for (;;) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(&item_sh, 1);
+            k = __shfl_sync(FULL, k, 0);
+            const int64_t it = i0 + k;
+            /* stop once every item is taken or the set has overflowed (warp-uniform reads) */
+            if (it >= i1 || __shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
             const int2 r = items[it];
             if (lane == 0) cand += (unsigned long long)(r.y - r.x);
             const int head_end = min(r.y, (r.x + 3) & ~3);
@@ -700,12 +757,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
             /* unaligned head and tail points: plain inserts */
             for (int i = r.x + lane; i < head_end; i += 32)
                 if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
-                    hs_insert(tab, __ldg(tid + i), &cnt_sh, &ovf_sh);
+                    hs_insert(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
                     hits++;
                 }
             for (int i = ve + lane; i < r.y; i += 32)
                 if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
-                    hs_insert(tab, __ldg(tid + i), &cnt_sh, &ovf_sh);
+                    hs_insert(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
                     hits++;
                 }
             const float4* X4 = reinterpret_cast<const float4*>(X + vb);
@@ -720,18 +777,18 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
                 ny = __ldg(Y4 + lane);
             }
             for (int k0 = 0; k0 < nv; k0 += 32) {
-                const int k = k0 + lane;
+                const int kk = k0 + lane;
                 const float4 x = nx, y = ny;
-                if (k + 32 < nv) {
-                    nx = __ldg(X4 + k + 32);
-                    ny = __ldg(Y4 + k + 32);
+                if (kk + 32 < nv) {
+                    nx = __ldg(X4 + kk + 32);
+                    ny = __ldg(Y4 + kk + 32);
                 }
                 int t0 = -1, t1 = -1, t2 = -1, t3 = -1;
-                if (k < nv) {
+                if (kk < nv) {
                     const bool h0 = in_box(q, x.x, y.x), h1 = in_box(q, x.y, y.y);
                     const bool h2 = in_box(q, x.z, y.z), h3 = in_box(q, x.w, y.w);
                     if (h0 | h1 | h2 | h3) {
-                        const int4 tt = __ldg(T4 + k);
+                        const int4 tt = __ldg(T4 + kk);
                         t0 = h0 ? tt.x : -1;
                         t1 = h1 ? tt.y : -1;
                         t2 = h2 ? tt.z : -1;
@@ -742,69 +799,81 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
                 int prev = __shfl_up_sync(FULL, t3, 1);
                 if (lane == 0) prev = carry;
                 carry = __shfl_sync(FULL, t3, 31);
-                if (t0 >= 0 && t0 != prev) hs_insert(tab, t0, &cnt_sh, &ovf_sh);
-                if (t1 >= 0 && t1 != t0) hs_insert(tab, t1, &cnt_sh, &ovf_sh);
-                if (t2 >= 0 && t2 != t1) hs_insert(tab, t2, &cnt_sh, &ovf_sh);
-                if (t3 >= 0 && t3 != t2) hs_insert(tab, t3, &cnt_sh, &ovf_sh);
+                if (t0 >= 0 && t0 != prev) hs_insert(tab, buf, t0, &cnt_sh, &ovf_sh);
+                if (t1 >= 0 && t1 != t0) hs_insert(tab, buf, t1, &cnt_sh, &ovf_sh);
+                if (t2 >= 0 && t2 != t1) hs_insert(tab, buf, t2, &cnt_sh, &ovf_sh);
+                if (t3 >= 0 && t3 != t2) hs_insert(tab, buf, t3, &cnt_sh, &ovf_sh);
             }
         }
         my_work += 8ull * cand + 4ull * hits;
-        __syncthreads();
+        __syncthreads(); /* every insert is done */
+        const int m = cnt_sh;
         const bool overflow = ovf_sh != 0;
-        /* compact the set into buf (clearing it on the way) */
-        /* slots threadIdx.x + kThreads * w (consecutive threads, consecutive banks) */
-        constexpr int per = kHashSize / kThreads;
-        int c = 0;
-        for (int w = 0; w < per; w++) c += tab[threadIdx.x + kThreads * w] >= 0;
-        int m;
-        int pre = block_scan_excl(c, &m, sh);
-        for (int w = 0; w < per; w++) {
-            const int v = tab[threadIdx.x + kThreads * w];
-            if (v >= 0) {
-                if (!overflow && pre < kHashMax) buf[pre] = v;
-                pre++;
-                tab[threadIdx.x + kThreads * w] = -1;
-            }
-        }
-        if (overflow) {
-            if (threadIdx.x == 0) {
+        if (threadIdx.x == 0) {
+            if (overflow) {
                 const int o = (int)atomicAdd(&ctr[3], 1ull);
                 ovf_list[o] = qi;
                 segcnt[qi] = 0;
                 segbase[qi] = 0;
+            } else {
+                base_sh = atomicAdd(&ctr[0], (unsigned long long)m);
+                segcnt[qi] = m;
+                segbase[qi] = (int64_t)base_sh;
+            }
+            next_sh = fetch();
+        }
+        __syncthreads(); /* the arena base and the next query are known */
+        const int64_t base = (int64_t)base_sh;
+        const bool write = !overflow && base + m <= cap;
+        if (overflow) {
+            for (int i = threadIdx.x; i < kHashSize; i += blockDim.x) tab[i] = -1;
+        } else if (m <= kRankSortMax) {
+            /* runs of 32 sorted in registers (padded with INT_MAX), written back in place */
+            const int runs = (m + 31) >> 5;
+            for (int c = warp; c < runs; c += kThreads / 32) {
+                const int i = 32 * c + lane;
+                const int v = warp_sort32(i < m ? buf[i] : INT_MAX);
+                __syncwarp();
+                buf[i] = v;
             }
             __syncthreads();
-            continue;
-        }
-        /* bitonic sort of the m ids (padded to a power of two) */
-        int P = 1;
-        while (P < m) P <<= 1;
-        for (int i = m + threadIdx.x; i < P; i += blockDim.x) buf[i] = INT_MAX;
-        __syncthreads();
-        for (int kk = 2; kk <= P; kk <<= 1)
-            for (int jj = kk >> 1; jj > 0; jj >>= 1) {
-                for (int i = threadIdx.x; i < P; i += blockDim.x) {
-                    const int ixj = i ^ jj;
-                    if (ixj > i) {
-                        const int a = buf[i], b = buf[ixj];
-                        if ((a > b) == ((i & kk) == 0)) {
-                            buf[i] = b;
-                            buf[ixj] = a;
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                const int x = buf[i], own = i >> 5;
+                int rank = i & 31;
+                for (int c = 0; c < runs; c++)
+                    if (c != own) rank += lower_bound32(buf + 32 * c, x);
+                if (write) arena[base + rank] = (uint32_t)x;
+                hs_erase(tab, x);
+            }
+        } else {
+            /* long lists: clear the set, then a block-wide bitonic sort padded to a power of two */
+            for (int i = threadIdx.x; i < m; i += blockDim.x) hs_erase(tab, buf[i]);
+            int P = 1;
+            while (P < m) P <<= 1;
+            for (int i = m + threadIdx.x; i < P; i += blockDim.x) buf[i] = INT_MAX;
+            __syncthreads();
+            for (int kk = 2; kk <= P; kk <<= 1)
+                for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+                    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                        const int ixj = i ^ jj;
+                        if (ixj > i) {
+                            const int a = buf[i], b = buf[ixj];
+                            if ((a > b) == ((i & kk) == 0)) {
+                                buf[i] = b;
+                                buf[ixj] = a;
+                            }
                         }
                     }
+                    __syncthreads();
                 }
-                __syncthreads();
-            }
-        if (threadIdx.x == 0) {
-            base_sh = atomicAdd(&ctr[0], (unsigned long long)m);
-            segcnt[qi] = m;
-            segbase[qi] = (int64_t)base_sh;
+            if (write)
+                for (int i = threadIdx.x; i < m; i += blockDim.x) arena[base + i] = (uint32_t)buf[i];
         }
-        __syncthreads();
-        const int64_t base = (int64_t)base_sh;
-        if (base + m <= cap)
-            for (int i = threadIdx.x; i < m; i += blockDim.x) arena[base + i] = (uint32_t)buf[i];
-        __syncthreads();
+        if (threadIdx.x == 0) {
+            cnt_sh = 0;
+            ovf_sh = 0;
+            item_sh = 0;
+        }
     }
     if (work) {
         for (int o = 16; o > 0; o >>= 1) my_work += __shfl_down_sync(FULL, my_work, o);
