@@ -206,9 +206,9 @@ constexpr int kPlainDepth = 5, kPlainSub = 1024;
 /* The candidate ranges of sub-thread `sub` of a query, joined and cut into items. Writes them
  * to items[0..] when items is non-NULL; returns how many there are. Sets GAT_ERR_ARG in flag when
  * a walk's stack overflows. */
-template <int KIND, int GD = kGridDepth>
-__device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& f, const MortonDev& m, const Box& q,
-                              int sub, int2* items, int32_t* flag) {
+template <int KIND, int GD, class Sink>
+__device__ int64_t walk_ranges(const GridDev& g, const StigDev& s, const FsgDev& f, const MortonDev& m, const Box& q,
+                               int sub, Sink sink, int32_t* flag) {
     constexpr int SD = 2 * GD, NSUB = 1 << (2 * GD); /* STIG levels and threads of the split */
     int64_t cnt = 0;
     /* Ranges that continue the previous one (neighbouring leaves / cells are contiguous in the
@@ -220,7 +220,7 @@ __device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& 
         while (cur_b < cur_e) {
             int e = cur_e;
             if (e - cur_b > kChunk) e = (cur_b + kChunk) & ~3;
-            if (items) items[cnt] = make_int2(cur_b, e);
+            sink(cnt, make_int2(cur_b, e));
             cnt++;
             cur_b = e;
         }
@@ -298,12 +298,25 @@ __device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& 
     return cnt;
 }
 
+/* walk_ranges writing the items to items[0..] (nothing when items is NULL) */
+template <int KIND, int GD = kGridDepth>
+__device__ int64_t walk_items(const GridDev& g, const StigDev& s, const FsgDev& f, const MortonDev& m, const Box& q,
+                              int sub, int2* items, int32_t* flag) {
+    return walk_ranges<KIND, GD>(
+        g, s, f, m, q, sub,
+        [items](int64_t c, int2 v) {
+            if (items) items[c] = v;
+        },
+        flag);
+}
+
+/* items of queries 0..nq-1, or of the nq queries listed in qlist (offsets by list position) */
 template <int KIND>
-__global__ void k_items(GridDev g, StigDev s, FsgDev f, MortonDev m, const gat_mbb* queries, int nq, const int64_t* ioff,
-                        int64_t* icnt, int2* items, int32_t* flag) {
+__global__ void k_items(GridDev g, StigDev s, FsgDev f, MortonDev m, const gat_mbb* queries, int nq, const int* qlist,
+                        const int64_t* ioff, int64_t* icnt, int2* items, int32_t* flag) {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (int64_t)nq * kSub) return;
-    const int qi = (int)(tid / kSub), sub = (int)(tid % kSub);
+    const int qi = qlist ? qlist[tid / kSub] : (int)(tid / kSub), sub = (int)(tid % kSub);
     const Box q = load_box(queries, qi);
     const int64_t cnt = walk_items<KIND>(g, s, f, m, q, sub, ioff ? items + ioff[tid] : nullptr, flag);
     if (!ioff) icnt[tid] = cnt;
@@ -542,7 +555,7 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
                                                         const int32_t* tid, int words, uint32_t* gbitmap,
                                                         uint32_t* arena, int64_t cap, unsigned long long* cursor,
                                                         int64_t* segbase, int64_t* segcnt, unsigned long long* work,
-                                                        const int* qlist, const unsigned long long* nq_dev) {
+                                                        const int* qlist, int ioff_by_pos) {
     dep_wait();
     extern __shared__ uint32_t smem_bm[];
     __shared__ int sh[kThreads / 32 + 1];
@@ -550,14 +563,14 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
     uint32_t* bm = gbitmap ? gbitmap + (size_t)blockIdx.x * words : smem_bm;
     int per = (words + kThreads - 1) / kThreads;
     unsigned long long my_work = 0; /* added once at exit */
-    if (nq_dev) nq = (int)*nq_dev; /* plain execution: the overflowed queries counted by the hash scan */
     for (int j = blockIdx.x; j < nq; j += gridDim.x) {
         const int qi = qlist ? qlist[j] : j;
         for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
         __syncthreads();
         Box q = load_box(queries, qi);
         unsigned long long cand = 0, hits = 0;
-        for (int64_t it = ioff[(int64_t)qi * kSub]; it < ioff[(int64_t)(qi + 1) * kSub]; it++) {
+        const int64_t ib = (int64_t)(ioff_by_pos ? j : qi) * kSub;
+        for (int64_t it = ioff[ib]; it < ioff[ib + kSub]; it++) {
             int2 r = items[it];
             cand += (unsigned long long)(r.y - r.x);
             scan_range(X, Y, r.x, r.y, q, [&](int i) {
@@ -601,23 +614,72 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
 }
 
 /* ---------------------------------------------------------------- locality order */
-/* A batch's queries are scanned in the order of the index position of their first candidate
- * point, bucketed: queries that start near each other in the index's point order (Morton-cell
- * order for the Grid, row-major cells for FSG, KD-leaf order for STIG) read overlapping point
- * ranges, and the CTAs working at one time then share those ranges in L2 instead of each
- * fetching them from HBM. The order only changes which CTA scans a query and when; every
- * query's result lands in its own slot, so results are the same. Queries without candidates
- * go last. */
+/* A batch's queries are scanned in the order of the index position of (about) their first
+ * candidate point, bucketed: queries that start near each other in the index's point order
+ * (Morton-cell order for the Grid, row-major cells for FSG, KD-leaf order for STIG) read
+ * overlapping point ranges, and the CTAs working at one time then share those ranges in L2
+ * instead of each fetching them from HBM. The order only changes which CTA scans a query and
+ * when; every query's result lands in its own slot, so results are the same. */
 constexpr int kOrderBuckets = 1 << 16;
 constexpr int kOrderMin = 256; /* smaller batches keep the given order */
 
-__global__ void k_order_keys(int nq, const int64_t* __restrict__ ioff, const int2* __restrict__ items, int64_t npoints,
+/* The key of a query: the index position of the leaf (block, cell) reached by descending from
+ * the root into the first child the query intersects, the first candidate of the traversal or
+ * close to it; a key only orders queries, so an approximation costs nothing but locality. */
+template <int KIND>
+__device__ int64_t order_key(const GridDev& g, const StigDev& s, const FsgDev& f, const MortonDev& m, const Box& q) {
+    if (KIND == GAT_INDEX_GRID) {
+        int nd = 0;
+        for (int guard = 0; guard < 64; guard++) {
+            const int ch = g.node_child[nd];
+            if (ch < 0) break;
+            int next = -1;
+            for (int c = 0; c < 4 && next < 0; c++) {
+                const float4 b = g.node_mbb[ch + c];
+                if (box_intersect(q, Box{b.x, b.y, b.z, b.w})) next = ch + c;
+            }
+            if (next < 0) break;
+            nd = next;
+        }
+        return g.node_pbeg[nd];
+    }
+    if (KIND == GAT_INDEX_MORTON) {
+        int level = 0;
+        uint32_t id = 0;
+        while (level < m.total_level && !morton_leaf(m, level, id)) {
+            int next = -1;
+            for (int c = 0; c < 4 && next < 0; c++)
+                if (box_intersect(q, morton_box(m, level + 1, (id << 2) + c))) next = c;
+            if (next < 0) break;
+            id = (id << 2) + (uint32_t)next;
+            level++;
+        }
+        return __ldg(m.cbeg + id * (1u << (2 * (m.total_level - level))));
+    }
+    if (KIND == GAT_INDEX_STIG) {
+        int nd = 0;
+        for (int guard = 0; guard < 64 && !s.kind[nd]; guard++) {
+            const float lo = s.dim[nd] == 0 ? q.xmin : q.ymin;
+            nd = !(lo > s.median[nd]) ? s.left[nd] : s.right[nd];
+        }
+        return s.kind[nd] ? s.lo[nd] : 0;
+    }
+    /* FSG: the first cell of the candidate rectangle's first row, clamped to the grid */
+    const int g1 = (int)__fdiv_rn(__fsub_rn(q.xmin, f.rxmin), f.cell);
+    const int g3 = (int)__fdiv_rn(__fsub_rn(f.rymax, q.ymax), f.cell);
+    long long c = (long long)max(g1, 0) + (long long)max(g3, 0) * f.nx;
+    if (c > f.cellnum - 1) c = f.cellnum - 1;
+    return c < 0 ? 0 : f.cbeg[c];
+}
+
+template <int KIND>
+__global__ void k_order_keys(GridDev g, StigDev s, FsgDev f, MortonDev m, const gat_mbb* queries, int nq, int64_t npoints,
                              unsigned long long* __restrict__ hist, int* __restrict__ bucket) {
+    dep_wait();
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= nq) return;
-    const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
-    int b = kOrderBuckets - 1;
-    if (i0 < i1) b = (int)min((long long)kOrderBuckets - 2, (long long)items[i0].x * (kOrderBuckets - 1) / (npoints + 1));
+    const int64_t key = order_key<KIND>(g, s, f, m, load_box(queries, qi));
+    const int b = (int)min((long long)kOrderBuckets - 1, (long long)key * (kOrderBuckets - 1) / (npoints + 1));
     bucket[qi] = b;
     atomicAdd(&hist[b], 1ull);
 }
@@ -646,6 +708,9 @@ constexpr int kHashBits = 13;
 constexpr int kHashSize = 1 << kHashBits; /* 32 KB of ids */
 constexpr int kHashMax = 4096;            /* distinct ids per query (load factor <= 1/2) */
 constexpr int kRankSortMax = 512;         /* lists up to this length are sorted by run ranks */
+constexpr int kQueryItems = 768;          /* candidate items of one query held in shared memory */
+constexpr int kFusedDepth = 4;            /* the walk's split: 4^4 = kThreads subtrees */
+static_assert(1 << (2 * kFusedDepth) == kThreads, "one subtree per thread of the scan CTA");
 
 __device__ __forceinline__ unsigned hs_slot(int t) { return ((unsigned)t * 2654435761u) >> (32 - kHashBits); }
 
@@ -709,17 +774,20 @@ __device__ __forceinline__ int lower_bound32(const int* run, int x) {
     return lo + (run[31] < x ? 1 : 0);
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queries, int nq, const int64_t* ioff,
-                                                         const int2* items, const float* __restrict__ X,
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, 4) k_range_hash(GridDev g, StigDev st, FsgDev f, MortonDev mo,
+                                                         const gat_mbb* queries, int nq, const float* __restrict__ X,
                                                          const float* __restrict__ Y, const int32_t* __restrict__ tid,
                                                          uint32_t* arena, int64_t cap, unsigned long long* ctr,
                                                          int64_t* segbase, int64_t* segcnt, int* ovf_list,
-                                                         unsigned long long* work, const int* __restrict__ order) {
+                                                         unsigned long long* work, const int* __restrict__ order,
+                                                         int32_t* flag) {
     dep_wait();
     extern __shared__ int hs_smem[];
-    int* tab = hs_smem;              /* kHashSize */
-    int* buf = hs_smem + kHashSize;  /* kHashMax ids in insertion order */
-    __shared__ int cnt_sh, ovf_sh, q_sh, next_sh, item_sh;
+    int* tab = hs_smem;                                             /* kHashSize */
+    int* buf = hs_smem + kHashSize;                                 /* kHashMax ids in insertion order */
+    int2* qitems = reinterpret_cast<int2*>(hs_smem + kHashSize + kHashMax); /* kQueryItems candidate items */
+    __shared__ int cnt_sh, ovf_sh, q_sh, next_sh, item_sh, nit_sh;
     __shared__ unsigned long long base_sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
@@ -734,6 +802,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
         cnt_sh = 0;
         ovf_sh = 0;
         item_sh = 0;
+        nit_sh = 0;
     }
     unsigned long long my_work = 0; /* algorithmic bytes of this thread, added once at exit */
     for (;;) {
@@ -741,16 +810,37 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
         const int qi = next_sh;
         if (qi >= nq) break;
         const Box q = load_box(queries, qi);
-        const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
+        /* candidate stage: the CTA's threads walk the index, each the subtree its digits select,
+         * and append the query's items to shared memory (their order does not change a set) */
+        walk_ranges<KIND, kFusedDepth>(
+            g, st, f, mo, q, threadIdx.x,
+            [&](int64_t, int2 v) {
+                const int p = atomicAdd(&nit_sh, 1);
+                if (p < kQueryItems) qitems[p] = v;
+            },
+            flag);
+        __syncthreads();
+        const int nit = nit_sh;
+        if (nit > kQueryItems) {
+            /* too many items for shared memory: the bitmap pass takes the query */
+            __syncthreads(); /* every thread has read nit_sh */
+            if (threadIdx.x == 0) {
+                ovf_list[(int)atomicAdd(&ctr[3], 1ull)] = qi;
+                segcnt[qi] = 0;
+                segbase[qi] = 0;
+                next_sh = fetch();
+                nit_sh = 0;
+            }
+            continue;
+        }
         unsigned long long cand = 0, hits = 0;
         for (;;) {
             int k = 0;
             if (lane == 0) k = atomicAdd(&item_sh, 1);
             k = __shfl_sync(FULL, k, 0);
-            const int64_t it = i0 + k;
             /* stop once every item is taken or the set has overflowed (warp-uniform reads) */
-            if (it >= i1 || __shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
-            const int2 r = items[it];
+            if (k >= nit || __shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
+            const int2 r = qitems[k];
             if (lane == 0) cand += (unsigned long long)(r.y - r.x);
             const int head_end = min(r.y, (r.x + 3) & ~3);
             const int vb = head_end, ve = head_end + ((r.y - head_end) & ~3);
@@ -873,6 +963,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
             cnt_sh = 0;
             ovf_sh = 0;
             item_sh = 0;
+            nit_sh = 0;
         }
     }
     if (work) {
@@ -1037,84 +1128,133 @@ int key_bits_of(const gat_index* ix) {
     return b;
 }
 
+/* Candidate items of queries 0..nq-1, or of the nq queries listed in device array qlist (their
+ * offsets then by list position): a count pass, a scan of the counts, a pass writing the items.
+ * Leaves ioff (kSub offsets per query, nq * kSub + 1 entries) and items in scratch. */
+int build_items(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, const int* qlist, int64_t** ioff_out,
+                int2** items_out) {
+    cudaStream_t s = ctx->stream;
+    int st = GAT_OK;
+    const int64_t nsub = (int64_t)nq * kSub;
+    int64_t* icnt = (int64_t*)scratch(ctx, S_RANGE_ICNT, (nsub + 1) * sizeof(int64_t), &st);
+    int64_t* ioff = icnt ? (int64_t*)scratch(ctx, S_RANGE_IOFF, (nsub + 1) * sizeof(int64_t), &st) : nullptr;
+    if (!ioff) return st;
+    const int tb = 128, gb = (int)((nsub + tb - 1) / tb);
+    auto launch = [&](const int64_t* off, int64_t* cnt, int2* items) {
+        switch (ix->kind) {
+            case GAT_INDEX_GRID:
+                k_items<GAT_INDEX_GRID><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, qlist, off, cnt,
+                                                          items, ctx->d_flag);
+                break;
+            case GAT_INDEX_STIG:
+                k_items<GAT_INDEX_STIG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, qlist, off, cnt,
+                                                          items, ctx->d_flag);
+                break;
+            case GAT_INDEX_MORTON:
+                k_items<GAT_INDEX_MORTON><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, qlist, off,
+                                                            cnt, items, ctx->d_flag);
+                break;
+            default:
+                k_items<GAT_INDEX_FSG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, qlist, off, cnt,
+                                                         items, ctx->d_flag);
+        }
+        count_launch(ctx);
+    };
+    launch(nullptr, icnt, nullptr);
+    if ((st = scan_i64(ctx, icnt, ioff, nsub)) != GAT_OK) return st;
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, ioff + nsub, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
+    const int64_t nitems = ctx->h_pinned[0];
+    int2* items = (int2*)scratch(ctx, S_RANGE_ITEMS, (nitems + 1) * sizeof(int2), &st);
+    if (!items) return st;
+    launch(ioff, nullptr, items);
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "range candidates launch");
+    *ioff_out = ioff;
+    *items_out = items;
+    return GAT_OK;
+}
+
+/* Locality order of a batch (k_order_keys): the query indices bucketed by their order key. */
+int locality_order(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int** order_out) {
+    cudaStream_t s = ctx->stream;
+    int st = GAT_OK;
+    /* [order nq | bucket nq | hist kOrderBuckets + 1 (u64, 8-byte aligned; the scan writes the
+     * total into the last entry)] */
+    const size_t qwords = ((size_t)2 * nq + 1) & ~(size_t)1;
+    int* ob = (int*)scratch(ctx, S_RANGE_ORDER, qwords * sizeof(int) + (size_t)(kOrderBuckets + 1) * 8, &st);
+    if (!ob) return st;
+    int* bucket = ob + nq;
+    auto* hist = reinterpret_cast<unsigned long long*>(ob + qwords);
+    (void)launch_dep(ctx, k_zero_words, dim3(64), dim3(256), 0, s, reinterpret_cast<int*>(hist), 2 * kOrderBuckets);
+    const int grid = (nq + 255) / 256;
+    switch (ix->kind) {
+        case GAT_INDEX_GRID:
+            k_order_keys<GAT_INDEX_GRID><<<grid, 256, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ix->npoints,
+                                                                hist, bucket);
+            break;
+        case GAT_INDEX_STIG:
+            k_order_keys<GAT_INDEX_STIG><<<grid, 256, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ix->npoints,
+                                                                hist, bucket);
+            break;
+        case GAT_INDEX_MORTON:
+            k_order_keys<GAT_INDEX_MORTON><<<grid, 256, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq,
+                                                                  ix->npoints, hist, bucket);
+            break;
+        default:
+            k_order_keys<GAT_INDEX_FSG><<<grid, 256, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ix->npoints,
+                                                               hist, bucket);
+    }
+    if ((st = scan_i64(ctx, reinterpret_cast<int64_t*>(hist), reinterpret_cast<int64_t*>(hist), kOrderBuckets)) != GAT_OK)
+        return st;
+    k_order_scatter<<<grid, 256, 0, s>>>(nq, bucket, hist, ob);
+    count_launch(ctx, 3);
+    GAT_CUDA_TRY(ctx, cudaGetLastError(), "range order");
+    *order_out = ob;
+    return GAT_OK;
+}
+
 /* Runs the pipeline for queries d_q[0..nq) and leaves per-query (segbase, segcnt) in scratch.
- * Returns the total result count in *total. */
+ * Returns the total result count in *total.
+ * Id sets: one launch of the hash kernel, which walks each query's candidates itself; queries
+ * whose items exceed shared memory or whose ids exceed the hash set then get their items built
+ * and go through the bitmap kernel. Point lists: items first, then the point-list kernel. */
 int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int mode, int64_t* d_off_out,
               int64_t* total) {
     cudaStream_t s = ctx->stream;
     int st = GAT_OK;
-    /* one count per (query, subtree thread); the item offsets of query q start at q * kSub */
-    const int64_t nsub = (int64_t)nq * kSub;
-    int64_t* icnt = (int64_t*)scratch(ctx, S_RANGE_ICNT, (nsub + 1) * sizeof(int64_t), &st);
-    if (!icnt) return st;
-    int tb = 128, gb = (int)((nsub + tb - 1) / tb);
-    auto launch_items = [&](const int64_t* ioff, int64_t* cnt, int2* items) {
-        switch (ix->kind) {
-            case GAT_INDEX_GRID:
-                k_items<GAT_INDEX_GRID><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ioff, cnt, items, ctx->d_flag);
-                break;
-            case GAT_INDEX_STIG:
-                k_items<GAT_INDEX_STIG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ioff, cnt, items, ctx->d_flag);
-                break;
-            case GAT_INDEX_MORTON:
-                k_items<GAT_INDEX_MORTON><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ioff, cnt, items, ctx->d_flag);
-                break;
-            default:
-                k_items<GAT_INDEX_FSG><<<gb, tb, 0, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ioff, cnt, items, ctx->d_flag);
-        }
-        count_launch(ctx);
-    };
-    launch_items(nullptr, icnt, nullptr);
-    int64_t* ioff = (int64_t*)scratch(ctx, S_RANGE_IOFF, (nsub + 1) * sizeof(int64_t), &st);
-    if (!ioff) return st;
-    if ((st = scan_i64(ctx, icnt, ioff, nsub)) != GAT_OK) return st;
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, ioff + nsub, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
-    GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
-    int64_t nitems = ctx->h_pinned[0];
-    int2* items = (int2*)scratch(ctx, S_RANGE_ITEMS, (nitems + 1) * sizeof(int2), &st);
-    if (!items) return st;
-    launch_items(ioff, nullptr, items);
-    if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
-    int* order = nullptr;
-    if (mode == GAT_RESULT_IDS && nq >= kOrderMin) {
-        /* [order nq | bucket nq | hist kOrderBuckets + 1 (u64, 8-byte aligned; the scan writes the
-         * total into the last entry)] */
-        const size_t qwords = ((size_t)2 * nq + 1) & ~(size_t)1;
-        int* ob = (int*)scratch(ctx, S_RANGE_ORDER, qwords * sizeof(int) + (size_t)(kOrderBuckets + 1) * 8, &st);
-        if (!ob) return st;
-        order = ob;
-        int* bucket = ob + nq;
-        auto* hist = reinterpret_cast<unsigned long long*>(ob + qwords);
-        (void)launch_dep(ctx, k_zero_words, dim3(64), dim3(256), 0, s, reinterpret_cast<int*>(hist), 2 * kOrderBuckets);
-        const int ob_grid = (nq + 255) / 256;
-        k_order_keys<<<ob_grid, 256, 0, s>>>(nq, ioff, items, ix->npoints, hist, bucket);
-        if ((st = scan_i64(ctx, reinterpret_cast<int64_t*>(hist), reinterpret_cast<int64_t*>(hist), kOrderBuckets)) != GAT_OK)
-            return st;
-        k_order_scatter<<<ob_grid, 256, 0, s>>>(nq, bucket, hist, order);
-        count_launch(ctx, 3);
-        GAT_CUDA_TRY(ctx, cudaGetLastError(), "range order");
-    }
-
     int64_t* segbase = (int64_t*)scratch(ctx, S_RANGE_SEGBASE, (nq + 1) * sizeof(int64_t), &st);
     int64_t* segcnt = (int64_t*)scratch(ctx, S_RANGE_SEGCNT, (nq + 1) * sizeof(int64_t), &st);
     unsigned long long* cursor = (unsigned long long*)scratch(ctx, S_RANGE_CURSOR, 64, &st);
-    if (!segbase || !segcnt || !cursor) return st;
     int* ovf_list = (int*)scratch(ctx, S_RANGE_OVF, (size_t)(nq + 1) * sizeof(int), &st);
-    if (!ovf_list) return st;
+    if (!segbase || !segcnt || !cursor || !ovf_list) return st;
     const int words = (ix->db->n + 1 + 31) / 32;
     const size_t smem_bm = (size_t)words * 4;
     const bool bm_in_smem = smem_bm <= 200 * 1024;
-    const size_t smem_hs = (size_t)(kHashSize + kHashMax) * sizeof(int);
-    int grid_pts = 0, grid_hs = 0;
-    if (mode == GAT_RESULT_IDS) {
-        allow_smem(k_range_hash, smem_hs);
+    const bool ids = mode == GAT_RESULT_IDS;
+    int64_t* ioff = nullptr;
+    int2* items = nullptr;
+    int* order = nullptr;
+    int grid = 1;
+    size_t smem = 0;
+    void (*hash_kernel)(GridDev, StigDev, FsgDev, MortonDev, const gat_mbb*, int, const float*, const float*,
+                        const int32_t*, uint32_t*, int64_t, unsigned long long*, int64_t*, int64_t*, int*,
+                        unsigned long long*, const int*, int32_t*) = nullptr;
+    if (ids) {
+        if (nq >= kOrderMin && (st = locality_order(ctx, ix, d_q, nq, &order)) != GAT_OK) return st;
+        hash_kernel = ix->kind == GAT_INDEX_GRID     ? k_range_hash<GAT_INDEX_GRID>
+                      : ix->kind == GAT_INDEX_STIG   ? k_range_hash<GAT_INDEX_STIG>
+                      : ix->kind == GAT_INDEX_MORTON ? k_range_hash<GAT_INDEX_MORTON>
+                                                     : k_range_hash<GAT_INDEX_FSG>;
+        smem = (size_t)(kHashSize + kHashMax) * sizeof(int) + (size_t)kQueryItems * sizeof(int2);
+        allow_smem(hash_kernel, smem);
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_hash, kThreads, smem_hs);
-        grid_hs = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hash_kernel, kThreads, smem);
+        grid = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
     } else {
+        if ((st = build_items(ctx, ix, d_q, nq, nullptr, &ioff, &items)) != GAT_OK) return st;
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_points, kThreads, 0);
-        grid_pts = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
+        grid = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
     }
     const int key_bits = key_bits_of(ix);
     /* result arena: start from a size guess and grow once if the cursor overshoots */
@@ -1127,33 +1267,35 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 4 * sizeof(unsigned long long), s), "range");
         unsigned long long* work = ctx->timing ? cursor + 1 : nullptr;
         timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
-        if (mode == GAT_RESULT_IDS)
-            k_range_hash<<<grid_hs, kThreads, smem_hs, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap,
-                                                           cursor, segbase, segcnt, ovf_list, work, order);
+        if (ids)
+            hash_kernel<<<grid, kThreads, smem, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ix->d_x, ix->d_y,
+                                                     ix->d_tid, arena, cap, cursor, segbase, segcnt, ovf_list, work, order,
+                                                     ctx->d_flag);
         else
-            k_range_points<<<grid_pts, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits,
-                                                         arena, cap, cursor, segbase, segcnt);
+            k_range_points<<<grid, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits, arena,
+                                                     cap, cursor, segbase, segcnt);
         timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
         count_launch(ctx);
         GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
         GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
         GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
-        const int64_t n_ovf = mode == GAT_RESULT_IDS ? ctx->h_pinned[3] : 0;
+        const int64_t n_ovf = ids ? ctx->h_pinned[3] : 0;
         if (n_ovf > 0) {
-            /* queries with more distinct ids than the shared-memory set holds: bitmap form */
+            /* queries beyond the shared-memory items or id set: their items, then the bitmap form */
+            if ((st = build_items(ctx, ix, d_q, (int)n_ovf, ovf_list, &ioff, &items)) != GAT_OK) return st;
             int per_sm = 0;
             if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_ids, kThreads, bm_in_smem ? smem_bm : 0);
-            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_ovf, (int64_t)std::max(1, per_sm) * ctx->sm_count));
+            const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>(n_ovf, (int64_t)std::max(1, per_sm) * ctx->sm_count));
             uint32_t* gbm = nullptr;
             if (!bm_in_smem) {
-                gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, (size_t)grid * words * 4, &st);
+                gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, (size_t)g2 * words * 4, &st);
                 if (!gbm) return st;
             }
             timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
-            k_range_ids<<<grid, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, (int)n_ovf, ioff, items, ix->d_x, ix->d_y,
-                                                                        ix->d_tid, words, gbm, arena, cap, cursor, segbase,
-                                                                        segcnt, work, ovf_list, nullptr);
+            k_range_ids<<<g2, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, (int)n_ovf, ioff, items, ix->d_x, ix->d_y,
+                                                                      ix->d_tid, words, gbm, arena, cap, cursor, segbase,
+                                                                      segcnt, work, ovf_list, 1);
             timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
             count_launch(ctx);
             GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
@@ -1168,6 +1310,7 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         if (attempt == 1) return fail(ctx, GAT_ERR_OOM, "range: result arena overflow");
         cap = used;
     }
+    if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
     if ((st = scan_i64(ctx, segcnt, d_off_out, nq)) != GAT_OK) return st;
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, d_off_out + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
     GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
