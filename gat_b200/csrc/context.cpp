@@ -35,18 +35,32 @@ void* scratch(gat_ctx* ctx, int slot, size_t bytes, int* status) {
             return nullptr;
         }
     }
+    /* Slots live in the context's stream-ordered pool: growing one frees and allocates in the
+     * stream's order, with no device-wide synchronisation (cudaFree would wait for the kernels of
+     * every stream, so one context's growth would stall the others: the serving lanes) */
+    cudaMemPool_t pool = ctx->device >= 0 ? build_pool(ctx) : nullptr;
+    auto release = [&](void* q) {
+        if (pool) {
+            cudaFreeAsync(q, ctx->stream);
+        } else {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(q);
+        }
+    };
+    auto take = [&](void** q, size_t b) {
+        return pool ? cudaMallocFromPoolAsync(q, b, pool, ctx->stream) : cudaMalloc(q, b);
+    };
     if (ctx->slot_ptr[slot]) {
-        cudaStreamSynchronize(ctx->stream);
-        cudaFree(ctx->slot_ptr[slot]);
+        release(ctx->slot_ptr[slot]);
         ctx->slot_ptr[slot] = nullptr;
         ctx->slot_bytes[slot] = 0;
     }
     size_t grow = bytes + bytes / 4;
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, grow);
+    cudaError_t e = take(&p, grow);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        e = cudaMalloc(&p, bytes);
+        e = take(&p, bytes);
         grow = bytes;
     }
     if (e != cudaSuccess) {
@@ -57,6 +71,21 @@ void* scratch(gat_ctx* ctx, int slot, size_t bytes, int* status) {
     ctx->slot_bytes[slot] = grow;
     ctx->slot_fresh[slot] = 1;
     return p;
+}
+
+/* returns every scratch slot (to the context's pool when it has one) and waits for the stream */
+void free_slots(gat_ctx* ctx) {
+    for (size_t i = 0; i < ctx->slot_ptr.size(); i++) {
+        if (ctx->slot_ptr[i]) {
+            if (ctx->build_pool)
+                cudaFreeAsync(ctx->slot_ptr[i], ctx->stream);
+            else
+                cudaFree(ctx->slot_ptr[i]);
+        }
+        ctx->slot_ptr[i] = nullptr;
+        ctx->slot_bytes[i] = 0;
+    }
+    cudaStreamSynchronize(ctx->stream);
 }
 
 void* scratch_zeroed(gat_ctx* ctx, int slot, size_t bytes, int* status) {
@@ -229,11 +258,7 @@ int gat_ctx_trim(gat_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     release_owned(ctx);
-    for (size_t i = 0; i < ctx->slot_ptr.size(); i++) {
-        if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
-        ctx->slot_ptr[i] = nullptr;
-        ctx->slot_bytes[i] = 0;
-    }
+    free_slots(ctx);
     if (ctx->build_pool) cudaMemPoolTrimTo(ctx->build_pool, 0);
     return GAT_OK;
 }
@@ -249,8 +274,7 @@ void gat_ctx_destroy(gat_ctx* ctx) {
     release_owned(ctx);
     drain_events(ctx);
     for (cudaEvent_t e : ctx->ev_free) cudaEventDestroy(e);
-    for (void* p : ctx->slot_ptr)
-        if (p) cudaFree(p);
+    free_slots(ctx);
     if (ctx->build_pool) cudaMemPoolDestroy(ctx->build_pool);
     if (ctx->d_flag) cudaFree(ctx->d_flag);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
@@ -370,12 +394,14 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
 int64_t gat_ctx_scratch_bytes(const gat_ctx* ctx) {
     if (!ctx) return 0;
     int64_t s = 0;
-    for (size_t b : ctx->slot_bytes) s += (int64_t)b;
     if (ctx->build_pool) {
+        /* the pool holds the scratch slots and the kept index-build temporaries */
         uint64_t held = 0;
         if (cudaMemPoolGetAttribute(ctx->build_pool, cudaMemPoolAttrReservedMemCurrent, &held) == cudaSuccess)
-            s += (int64_t)held;
+            s = (int64_t)held;
+        return s;
     }
+    for (size_t b : ctx->slot_bytes) s += (int64_t)b;
     return s;
 }
 

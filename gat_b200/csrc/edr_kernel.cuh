@@ -236,7 +236,6 @@ struct TileCtl {
     int32_t* flag;
     int spin_limit;  /* polls before a carry wait gives up (kSpinLimit) */
     int stall_pair;  /* tests of the bounded wait: this pair's first pipelined tile writes no carries (-1: none) */
-    int one;         /* 1, passed at run time (see add_sign) */
 };
 
 /* The carry word is the only datum exchanged, so neither access needs to order other memory
@@ -341,50 +340,39 @@ __global__ void k_sched_write(Src src, int cap, int* __restrict__ ctr, const int
     }
 }
 
-/* Match word of one cell: negative exactly when |x1 - x2| < u and |y1 - y2| < u (float
- * differences, no contraction). fl(|d| - u) is negative exactly when |d| < u: the difference of
- * two floats rounds to zero only when they are equal and keeps its sign otherwise (gradual
- * underflow is exact), while |d| NaN or infinite gives a NaN without sign or +inf. The two sign
- * bits are combined with one AND. Everything but the AND runs on the FMA pipe. */
-__device__ __forceinline__ int below(float d, float u) { return __float_as_int(__fsub_rn(fabsf(d), u)); }
-__device__ __forceinline__ int match_word(float ax, float ay, float2 b, float u) {
-    return below(__fsub_rn(ax, b.x), u) & below(__fsub_rn(ay, b.y), u);
-}
-
-/* v + (w < 0 ? -1 : 0) as one integer multiply-add (the high word of w * one), and v + 1 as
- * v * one + one: `one` is 1 held in a register the compiler cannot see through (a kernel
- * parameter), so both stay multiply-adds on the FMA pipe instead of joining the compares, mins
- * and selects on the ALU pipe, which bounds this kernel. */
-__device__ __forceinline__ int add_sign(int w, int one, int v) {
-    int r;
-    asm("mad.hi.s32 %0, %1, %2, %3;" : "=r"(r) : "r"(w), "r"(one), "r"(v));
-    return r;
-}
-__device__ __forceinline__ int plus_one(int v, int one) {
-    int r;
-    asm("mad.lo.s32 %0, %1, %2, %2;" : "=r"(r) : "r"(v), "r"(one));
-    return r;
+/* Match mask of one cell: -1 when |x1 - x2| < u and |y1 - y2| < u (float differences, no
+ * contraction), else 0. */
+__device__ __forceinline__ int match_mask(float ax, float ay, float2 b, float u) {
+    const float dx = __fsub_rn(ax, b.x), dy = __fsub_rn(ay, b.y);
+    int m;
+    asm("{\n\t.reg .pred p;\n\t.reg .f32 t0, t1;\n\t"
+        "abs.f32 t0, %1;\n\tabs.f32 t1, %2;\n\t"
+        "setp.lt.f32 p, t0, %3;\n\t"
+        "set.lt.and.s32.f32 %0, t1, %3, p;\n\t}"
+        : "=r"(m)
+        : "f"(dx), "f"(dy), "f"(u));
+    return m;
 }
 
 /* One wavefront step of a lane's R rows at column c (DP column index). Values are held shifted
  * by their column: E[r][c] = D[r][c] - c. The reference's three operands at (r, c) become, in
  * column c's shift, m = E[r-1][c-1] + (match ? -1 : 0), l = E[r][c-1] and u = E[r-1][c] + 1;
- * a common shift keeps every comparison, so the reference's choice (u when m == l, else the
- * least of the three) is taken on shifted values unchanged: one three-way min and one select
- * per cell. State per row i: Lp[i] = E[r0+i+1][c-1]; diag0 = E[r0][c-1]; up0 = E[r0][c] (the
- * value above the lane's first row). */
+ * a common shift keeps every comparison, so the choice min(u, mml), mml = min(m, l) or +inf
+ * when m == l, is taken on shifted values unchanged. State per row i: Lp[i] = E[r0+i+1][c-1];
+ * diag0 = E[r0][c-1]; up0 = E[r0][c] (the value above the lane's first row). */
 template <int R>
 __device__ __forceinline__ int wf_step(const float (&ax)[R], const float (&ay)[R], int (&Lp)[R], int& diag0, float2 b,
-                                       int up0, float u, int one) {
-    int m[R];
+                                       int up0, float u) {
+    int mml[R];
 #pragma unroll
-    for (int i = 0; i < R; i++) m[i] = add_sign(match_word(ax[i], ay[i], b, u), one, i == 0 ? diag0 : Lp[i - 1]);
+    for (int i = 0; i < R; i++) {
+        const int m = (i == 0 ? diag0 : Lp[i - 1]) + match_mask(ax[i], ay[i], b, u);
+        mml[i] = (m == Lp[i]) ? kBig : min(m, Lp[i]);
+    }
     int up = up0;
 #pragma unroll
     for (int i = 0; i < R; i++) {
-        const int uu = plus_one(up, one), l = Lp[i];
-        const int least = __vimin3_s32(uu, m[i], l);
-        up = (m[i] == l) ? uu : least;
+        up = __viaddmin_s32(up, 1, mml[i]);
         Lp[i] = up;
     }
     diag0 = up0;
@@ -394,23 +382,23 @@ __device__ __forceinline__ int wf_step(const float (&ax)[R], const float (&ay)[R
 /* Column-tile form of the same recurrence: a lane owns R consecutive DP columns and a step
  * advances one DP row r. Values are held shifted by their row: F[r][c] = D[r][c] - r, so in
  * row r's shift u = F[r-1][c] needs no add, m = F[r-1][c-1] + (match ? -1 : 0) and
- * l = F[r][c-1] + 1, whose chain runs along the lane's columns; the cell is u when m == l, else
- * the least of the three. State per column j: F[j] = F[r-1][c_j] on entry, F[r][c_j] on exit;
- * diag0 = F[r-1][c_0 - 1]; left = F[r][c_0 - 1] (the value to the left of the lane's first
- * column). Same interface as wf_step. */
+ * l = F[r][c-1] + 1, whose chain runs along the lane's columns: with mm1 = m - 1 and
+ * prev = F[r][c-1], m == l exactly when mm1 == prev, min(m, l) = min(mm1, prev) + 1, and the
+ * cell is u when they are equal, else min(u, min(m, l)). State per column j: F[j] =
+ * F[r-1][c_j] on entry, F[r][c_j] on exit; diag0 = F[r-1][c_0 - 1]; left = F[r][c_0 - 1] (the
+ * value to the left of the lane's first column). Same interface as wf_step. */
 template <int R>
 __device__ __forceinline__ int cf_step(const float (&bx)[R], const float (&by)[R], int (&F)[R], int& diag0, float2 a,
-                                       int left, float u, int one) {
-    int m[R];
-    m[0] = add_sign(match_word(bx[0], by[0], a, u), one, diag0);
-#pragma unroll
-    for (int j = 1; j < R; j++) m[j] = add_sign(match_word(bx[j], by[j], a, u), one, F[j - 1]);
+                                       int left, float u) {
     int prev = left;
+    int diag = diag0;
 #pragma unroll
     for (int j = 0; j < R; j++) {
-        const int up = F[j], l = plus_one(prev, one);
-        const int least = __vimin3_s32(up, m[j], l);
-        const int d = (m[j] == l) ? up : least;
+        const int up = F[j];
+        const int mm1 = diag + match_mask(bx[j], by[j], a, u) - 1;
+        const int mn = min(mm1, prev);
+        const int d = (mm1 == prev) ? up : __viaddmin_s32(mn, 1, up);
+        diag = up;
         F[j] = d;
         prev = d;
     }
@@ -435,7 +423,7 @@ template <int R, bool COL = false>
 __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const float2* __restrict__ cols, int len1,
                                          int len2, int t, const carry_t* cin, carry_t* cout, carry_t tag_in,
                                          carry_t tag_out, float u, float2* sb, int* sc, int& result,
-                                         int spin_limit, int one) {
+                                         int spin_limit) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const bool lane0 = lane == 0;
@@ -516,8 +504,7 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
             for (int k = 0; k < 32; k++) {
                 const int from_above = __shfl_up_sync(FULL, bottom, 1);
                 const int up0 = lane0 ? sc[k] : from_above;
-                bottom = COL ? cf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u, one)
-                             : wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u, one);
+                bottom = COL ? cf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u) : wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u);
                 if (writer) st_carry(cout + (s0 + k - 30), tag_hi | (carry_t)(unsigned short)bottom);
             }
         } else {
@@ -527,8 +514,8 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
                 const int j = s0 + k - lane;
                 if (j >= 0 && j < len2) {
                     const int up0 = lane0 ? sc[k] : from_above;
-                    bottom = COL ? cf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u, one)
-                                 : wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u, one);
+                    bottom = COL ? cf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u)
+                                 : wf_step<R>(ax, ay, Lp, diag0, pb[k], up0, u);
                     if (writer) st_carry(cout + (j + 1), tag_hi | (carry_t)(unsigned short)bottom);
                 }
             }
@@ -597,14 +584,14 @@ __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(S
             for (int tt = 0; tt < T && ok; tt++)
                 ok = edr_tile<R, COL>(lpts, spts, nlane, nstep, tt, tt > 0 ? ((tt - 1) & 1 ? wc1 : wc0) : nullptr,
                                       tt + 1 < T ? ((tt & 1) ? wc1 : wc0) : nullptr, ep | ((tt - 1) & 0xff),
-                                      ep | (tt & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit, ctl.one);
+                                      ep | (tt & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit);
             finished = true;
         } else {
             carry_t* pc = ctl.pair_carry + (size_t)it.z * 2 * ctl.stride;
             const bool stalled = p == ctl.stall_pair && t == 0;
             ok = edr_tile<R, COL>(lpts, spts, nlane, nstep, t, t > 0 ? pc + ((t - 1) & 1) * ctl.stride : nullptr,
                                   t + 1 < T && !stalled ? pc + (t & 1) * ctl.stride : nullptr, ep | ((t - 1) & 0xff),
-                                  ep | (t & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit, ctl.one);
+                                  ep | (t & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit);
             finished = t == T - 1;
         }
         if (!ok) {
@@ -663,7 +650,7 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     /* the stall knob (tests of the bounded wait) also shortens the wait to ~2^12 polls */
     const int stall = ctx->test_stall_pair - 1;
     TileCtl ctl{items, ctr + 2, pcarry, wcarry, stride, reinterpret_cast<const unsigned long long*>(ctr + kCtrEpoch),
-                ctx->d_flag, stall >= 0 ? (1 << 12) : kSpinLimit, stall, 1};
+                ctx->d_flag, stall >= 0 ? (1 << 12) : kSpinLimit, stall};
     timed_begin(ctx, GAT_KERNEL_EDR);
     if (ev0) cudaEventRecord(ev0, s);
     (void)launch_dep(ctx, k_edr_tiles<R, COL, Src>, dim3(grid), dim3(kTileWarps * 32), 0, s, src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);

@@ -369,25 +369,6 @@ __global__ void k_fv_cells(int64_t R, const unsigned long long* __restrict__ run
 }
 
 /* ---------------------------------------------------------------- host side */
-/* The context's pool for index-build temporaries: stream-ordered, and it keeps freed memory
- * (release threshold unbounded), so repeated builds do not map and unmap gigabytes each time;
- * gat_ctx_trim returns it. Null when the device has no memory pools. */
-cudaMemPool_t build_pool(gat_ctx* ctx) {
-    if (ctx->build_pool) return ctx->build_pool;
-    int ok = 0;
-    if (cudaDeviceGetAttribute(&ok, cudaDevAttrMemoryPoolsSupported, ctx->device) != cudaSuccess || !ok) return nullptr;
-    cudaMemPoolProps props{};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = ctx->device;
-    cudaMemPool_t pool = nullptr;
-    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
-    uint64_t keep = ~0ull;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    ctx->build_pool = pool;
-    return pool;
-}
-
 /* device temporaries of one build, taken from the context's pool in stream order and returned
  * to it (after the work queued on the stream) when the build ends */
 struct Temps {
@@ -753,6 +734,26 @@ int build_vectors(gat_index* ix, const Placement& pl, int vparam, Temps& tmp) {
 }
 
 }  // namespace
+
+/* The context's pool for scratch slots and index-build temporaries: stream-ordered, and it keeps freed memory
+ * (release threshold unbounded), so repeated builds do not map and unmap gigabytes each time;
+ * gat_ctx_trim returns it. Null when the device has no memory pools. */
+cudaMemPool_t build_pool(gat_ctx* ctx) {
+    if (ctx->build_pool) return ctx->build_pool;
+    int ok = 0;
+    if (cudaDeviceGetAttribute(&ok, cudaDevAttrMemoryPoolsSupported, ctx->device) != cudaSuccess || !ok) return nullptr;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    ctx->build_pool = pool;
+    return pool;
+}
+
 
 int device_build_grid(gat_index* ix, const DevicePlaceArgs& a, int total_level, int leaf_cap) {
     gat_ctx* ctx = ix->ctx;

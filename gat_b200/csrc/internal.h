@@ -112,7 +112,7 @@ struct gat_ctx {
     int dep_launch = 1;                  /* programmatic dependent launch on the query path */
     int test_stall_pair = 0;             /* GAT_TUNE_TEST_STALL_CARRY (tests of the bounded wait) */
     int sm_reserve = 0;                  /* SMs the persistent EDR kernel leaves to other streams (serving lanes) */
-    cudaMemPool_t build_pool = nullptr;  /* index-build temporaries, kept for reuse until gat_ctx_trim */
+    cudaMemPool_t build_pool = nullptr;  /* scratch slots and index-build temporaries, kept until gat_ctx_trim */
     std::map<uint64_t, int> edr_tune; /* worker contexts use their root's table */
     std::mutex tune_mu;
     /* objects that hold device memory of this context's scratch or workers (cached CUDA graphs);
@@ -204,6 +204,11 @@ void timed_end(gat_ctx* ctx, int cls, double work);
 /* device-side work counter for classes whose work is only known on the device (EDR cells) */
 void timed_add_work(gat_ctx* ctx, int cls, double work);
 
+/* the context's stream-ordered memory pool (scratch slots, index-build temporaries; it keeps
+ * freed memory until gat_ctx_trim); null when the device has no memory pools (index_gpu.cu) */
+cudaMemPool_t build_pool(gat_ctx* ctx);
+/* returns every scratch slot and waits for the context's stream */
+void free_slots(gat_ctx* ctx);
 /* replaces the context's (still unused) stream by one of the device's greatest priority */
 int ctx_use_priority_stream(gat_ctx* ctx);
 /* GAT_ERR_STATE for a host-only context (device -1) */

@@ -708,9 +708,6 @@ constexpr int kHashBits = 13;
 constexpr int kHashSize = 1 << kHashBits; /* 32 KB of ids */
 constexpr int kHashMax = 4096;            /* distinct ids per query (load factor <= 1/2) */
 constexpr int kRankSortMax = 512;         /* lists up to this length are sorted by run ranks */
-constexpr int kQueryItems = 768;          /* candidate items of one query held in shared memory */
-constexpr int kFusedDepth = 4;            /* the walk's split: 4^4 = kThreads subtrees */
-static_assert(1 << (2 * kFusedDepth) == kThreads, "one subtree per thread of the scan CTA");
 
 __device__ __forceinline__ unsigned hs_slot(int t) { return ((unsigned)t * 2654435761u) >> (32 - kHashBits); }
 
@@ -774,20 +771,17 @@ __device__ __forceinline__ int lower_bound32(const int* run, int x) {
     return lo + (run[31] < x ? 1 : 0);
 }
 
-template <int KIND>
-__global__ void __launch_bounds__(kThreads, 4) k_range_hash(GridDev g, StigDev st, FsgDev f, MortonDev mo,
-                                                         const gat_mbb* queries, int nq, const float* __restrict__ X,
+__global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queries, int nq, const int64_t* ioff,
+                                                         const int2* items, const float* __restrict__ X,
                                                          const float* __restrict__ Y, const int32_t* __restrict__ tid,
                                                          uint32_t* arena, int64_t cap, unsigned long long* ctr,
                                                          int64_t* segbase, int64_t* segcnt, int* ovf_list,
-                                                         unsigned long long* work, const int* __restrict__ order,
-                                                         int32_t* flag) {
+                                                         unsigned long long* work, const int* __restrict__ order) {
     dep_wait();
     extern __shared__ int hs_smem[];
-    int* tab = hs_smem;                                             /* kHashSize */
-    int* buf = hs_smem + kHashSize;                                 /* kHashMax ids in insertion order */
-    int2* qitems = reinterpret_cast<int2*>(hs_smem + kHashSize + kHashMax); /* kQueryItems candidate items */
-    __shared__ int cnt_sh, ovf_sh, q_sh, next_sh, item_sh, nit_sh;
+    int* tab = hs_smem;             /* kHashSize */
+    int* buf = hs_smem + kHashSize; /* kHashMax ids in insertion order */
+    __shared__ int cnt_sh, ovf_sh, q_sh, next_sh, item_sh;
     __shared__ unsigned long long base_sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
@@ -802,7 +796,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(GridDev g, StigDev s
         cnt_sh = 0;
         ovf_sh = 0;
         item_sh = 0;
-        nit_sh = 0;
     }
     unsigned long long my_work = 0; /* algorithmic bytes of this thread, added once at exit */
     for (;;) {
@@ -810,37 +803,16 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(GridDev g, StigDev s
         const int qi = next_sh;
         if (qi >= nq) break;
         const Box q = load_box(queries, qi);
-        /* candidate stage: the CTA's threads walk the index, each the subtree its digits select,
-         * and append the query's items to shared memory (their order does not change a set) */
-        walk_ranges<KIND, kFusedDepth>(
-            g, st, f, mo, q, threadIdx.x,
-            [&](int64_t, int2 v) {
-                const int p = atomicAdd(&nit_sh, 1);
-                if (p < kQueryItems) qitems[p] = v;
-            },
-            flag);
-        __syncthreads();
-        const int nit = nit_sh;
-        if (nit > kQueryItems) {
-            /* too many items for shared memory: the bitmap pass takes the query */
-            __syncthreads(); /* every thread has read nit_sh */
-            if (threadIdx.x == 0) {
-                ovf_list[(int)atomicAdd(&ctr[3], 1ull)] = qi;
-                segcnt[qi] = 0;
-                segbase[qi] = 0;
-                next_sh = fetch();
-                nit_sh = 0;
-            }
-            continue;
-        }
+        const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
         unsigned long long cand = 0, hits = 0;
         for (;;) {
             int k = 0;
             if (lane == 0) k = atomicAdd(&item_sh, 1);
             k = __shfl_sync(FULL, k, 0);
+            const int64_t it = i0 + k;
             /* stop once every item is taken or the set has overflowed (warp-uniform reads) */
-            if (k >= nit || __shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
-            const int2 r = qitems[k];
+            if (it >= i1 || __shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
+            const int2 r = items[it];
             if (lane == 0) cand += (unsigned long long)(r.y - r.x);
             const int head_end = min(r.y, (r.x + 3) & ~3);
             const int vb = head_end, ve = head_end + ((r.y - head_end) & ~3);
@@ -963,7 +935,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(GridDev g, StigDev s
             cnt_sh = 0;
             ovf_sh = 0;
             item_sh = 0;
-            nit_sh = 0;
         }
     }
     if (work) {
@@ -1215,9 +1186,9 @@ int locality_order(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq
 
 /* Runs the pipeline for queries d_q[0..nq) and leaves per-query (segbase, segcnt) in scratch.
  * Returns the total result count in *total.
- * Id sets: one launch of the hash kernel, which walks each query's candidates itself; queries
- * whose items exceed shared memory or whose ids exceed the hash set then get their items built
- * and go through the bitmap kernel. Point lists: items first, then the point-list kernel. */
+ * Candidate items first (k_items); id sets then take one launch of the hash kernel in the
+ * batch's locality order, and queries whose ids exceed its set go through the bitmap kernel;
+ * point lists take the point-list kernel. */
 int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int mode, int64_t* d_off_out,
               int64_t* total) {
     cudaStream_t s = ctx->stream;
@@ -1236,22 +1207,16 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
     int* order = nullptr;
     int grid = 1;
     size_t smem = 0;
-    void (*hash_kernel)(GridDev, StigDev, FsgDev, MortonDev, const gat_mbb*, int, const float*, const float*,
-                        const int32_t*, uint32_t*, int64_t, unsigned long long*, int64_t*, int64_t*, int*,
-                        unsigned long long*, const int*, int32_t*) = nullptr;
+    if ((st = build_items(ctx, ix, d_q, nq, nullptr, &ioff, &items)) != GAT_OK) return st;
+    if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
     if (ids) {
         if (nq >= kOrderMin && (st = locality_order(ctx, ix, d_q, nq, &order)) != GAT_OK) return st;
-        hash_kernel = ix->kind == GAT_INDEX_GRID     ? k_range_hash<GAT_INDEX_GRID>
-                      : ix->kind == GAT_INDEX_STIG   ? k_range_hash<GAT_INDEX_STIG>
-                      : ix->kind == GAT_INDEX_MORTON ? k_range_hash<GAT_INDEX_MORTON>
-                                                     : k_range_hash<GAT_INDEX_FSG>;
-        smem = (size_t)(kHashSize + kHashMax) * sizeof(int) + (size_t)kQueryItems * sizeof(int2);
-        allow_smem(hash_kernel, smem);
+        smem = (size_t)(kHashSize + kHashMax) * sizeof(int);
+        allow_smem(k_range_hash, smem);
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hash_kernel, kThreads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_hash, kThreads, smem);
         grid = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
     } else {
-        if ((st = build_items(ctx, ix, d_q, nq, nullptr, &ioff, &items)) != GAT_OK) return st;
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_points, kThreads, 0);
         grid = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
@@ -1268,9 +1233,8 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         unsigned long long* work = ctx->timing ? cursor + 1 : nullptr;
         timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
         if (ids)
-            hash_kernel<<<grid, kThreads, smem, s>>>(ix->grid, ix->stig, ix->fsg, ix->morton, d_q, nq, ix->d_x, ix->d_y,
-                                                     ix->d_tid, arena, cap, cursor, segbase, segcnt, ovf_list, work, order,
-                                                     ctx->d_flag);
+            k_range_hash<<<grid, kThreads, smem, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap, cursor,
+                                                      segbase, segcnt, ovf_list, work, order);
         else
             k_range_points<<<grid, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits, arena,
                                                      cap, cursor, segbase, segcnt);
@@ -1281,8 +1245,7 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
         const int64_t n_ovf = ids ? ctx->h_pinned[3] : 0;
         if (n_ovf > 0) {
-            /* queries beyond the shared-memory items or id set: their items, then the bitmap form */
-            if ((st = build_items(ctx, ix, d_q, (int)n_ovf, ovf_list, &ioff, &items)) != GAT_OK) return st;
+            /* queries with more distinct ids than the shared-memory set holds: bitmap form */
             int per_sm = 0;
             if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_ids, kThreads, bm_in_smem ? smem_bm : 0);
@@ -1295,7 +1258,7 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
             timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
             k_range_ids<<<g2, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, (int)n_ovf, ioff, items, ix->d_x, ix->d_y,
                                                                       ix->d_tid, words, gbm, arena, cap, cursor, segbase,
-                                                                      segcnt, work, ovf_list, 1);
+                                                                      segcnt, work, ovf_list, 0);
             timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
             count_launch(ctx);
             GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
@@ -1310,7 +1273,6 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         if (attempt == 1) return fail(ctx, GAT_ERR_OOM, "range: result arena overflow");
         cap = used;
     }
-    if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
     if ((st = scan_i64(ctx, segcnt, d_off_out, nq)) != GAT_OK) return st;
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, d_off_out + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
     GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
