@@ -246,6 +246,8 @@ enum Slot {
     S_RANGE_OVF,
     S_RANGE_CSR,
     S_RANGE_ORDER,
+    S_RANGE_TPOS,
+    S_RANGE_TASK,
     S_EDR_PAIRS,
     S_EDR_CARRY,
     S_EDR_COUNTERS,
