@@ -258,18 +258,8 @@ __device__ __forceinline__ int duration_class(long long d) {
     return min(2 * e + half, kClasses - 1);
 }
 
-/* Tile form of a pair: column tiles (lanes own columns of the longer side, steps walk the
- * shorter) when they take fewer lane-steps than row tiles, unless `form` forces one (1 row, 2
- * column). A pair much longer than wide then keeps its lanes busy either way. */
-template <int R>
-__device__ __forceinline__ bool column_form(int len1, int len2, int form) {
-    if (form != 0) return form == 2;
-    const long long tr = (len1 + 32 * R - 1) / (32 * R), tc = (len2 + 32 * R - 1) / (32 * R);
-    return tc * (len1 + 31) < tr * (len2 + 31);
-}
-
-template <int R, class Src>
-__global__ void k_sched_count(Src src, int cap, int coop_cap, int form, int* __restrict__ ctr, int2* __restrict__ meta) {
+template <int R, bool COL, class Src>
+__global__ void k_sched_count(Src src, int cap, int coop_cap, int* __restrict__ ctr, int2* __restrict__ meta) {
     dep_wait();
     __shared__ int hist[kClasses];
     for (int i = threadIdx.x; i < kClasses; i += blockDim.x) hist[i] = 0;
@@ -281,8 +271,7 @@ __global__ void k_sched_count(Src src, int cap, int coop_cap, int form, int* __r
         int32_t* o;
         src.get(p, a, la, b, lb, o);
         const int len1 = min(la, lb), len2 = max(la, lb);
-        const bool col = column_form<R>(len1, len2, form);
-        const int nlane = col ? len2 : len1, nstep = col ? len1 : len2;
+        const int nlane = COL ? len2 : len1, nstep = COL ? len1 : len2;
         const int T = nlane <= 0 ? 1 : (nlane + 32 * R - 1) / (32 * R);
         int slot = -1, items = 1;
         if (T >= 2) {
@@ -295,7 +284,7 @@ __global__ void k_sched_count(Src src, int cap, int coop_cap, int form, int* __r
         const long long dur = slot >= 0 ? (long long)nstep + 32LL * (T - 1) : (long long)T * (nstep + 31);
         const int c = duration_class(dur);
         atomicAdd(&hist[c], items);
-        meta[p] = make_int2(slot, (c << 16) | (col ? 1 << 15 : 0) | items);
+        meta[p] = make_int2(slot, (c << 16) | items);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kClasses; i += blockDim.x)
@@ -328,13 +317,12 @@ __global__ void k_sched_write(Src src, int cap, int* __restrict__ ctr, const int
         for (int i = threadIdx.x; i < kClasses; i += blockDim.x) lcnt[i] = 0;
         __syncthreads();
         const int p = base + threadIdx.x;
-        int c = 0, nit = 0, loc = 0, slot = -1, colbit = 0;
+        int c = 0, nit = 0, loc = 0, slot = -1;
         if (p < n) {
             const int2 m = meta[p];
             slot = m.x;
             c = m.y >> 16;
-            colbit = (m.y >> 15) & 1;
-            nit = m.y & 0x7fff;
+            nit = m.y & 0xffff;
             loc = atomicAdd(&lcnt[c], nit);
         }
         __syncthreads();
@@ -343,11 +331,10 @@ __global__ void k_sched_write(Src src, int cap, int* __restrict__ ctr, const int
         __syncthreads();
         if (p < n) {
             const int pos = off[c] + lbase[c] + loc;
-            /* .w: the pair's tile count, bit 16 set for column tiles */
             if (slot < 0)
-                items[pos] = make_int4(p, -1, -1, 1 | colbit << 16);
+                items[pos] = make_int4(p, -1, -1, 1);
             else
-                for (int t = 0; t < nit; t++) items[pos + t] = make_int4(p, t, slot, nit | colbit << 16);
+                for (int t = 0; t < nit; t++) items[pos + t] = make_int4(p, t, slot, nit);
         }
         __syncthreads();
     }
@@ -544,7 +531,7 @@ __device__ __forceinline__ bool edr_tile(const float2* __restrict__ rows, const 
     return true;
 }
 
-template <int R, class Src>
+template <int R, bool COL, class Src>
 __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(Src src, float u, TileCtl ctl, unsigned* __restrict__ work,
                                                            unsigned long long* __restrict__ cells) {
     dep_wait();
@@ -585,31 +572,26 @@ __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(S
             if (lane == 0) *outp = len1 + len2;
             continue;
         }
-        /* the pair's tile form (chosen by the schedule); lane side and step side: rows /
-         * columns for row tiles, columns / rows for column tiles */
-        const bool col = (it.w >> 16) & 1;
-        const float2* lpts = col ? cols : rows;
-        const float2* spts = col ? rows : cols;
-        const int nlane = col ? len2 : len1, nstep = col ? len1 : len2;
+        /* lane side and step side: rows / columns for row tiles, columns / rows for column tiles */
+        const float2* lpts = COL ? cols : rows;
+        const float2* spts = COL ? rows : cols;
+        const int nlane = COL ? len2 : len1, nstep = COL ? len1 : len2;
         constexpr int kTile = 32 * R;
         const int T = (nlane + kTile - 1) / kTile;
         int result = 0;
-        auto tile = [&](int tt, const carry_t* cin, carry_t* cout) {
-            return col ? edr_tile<R, true>(lpts, spts, nlane, nstep, tt, cin, cout, ep | ((tt - 1) & 0xff), ep | (tt & 0xff),
-                                          u, bring[wib], cring[wib], result, ctl.spin_limit)
-                       : edr_tile<R, false>(lpts, spts, nlane, nstep, tt, cin, cout, ep | ((tt - 1) & 0xff),
-                                           ep | (tt & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit);
-        };
         bool ok = true, finished = false;
         if (t < 0) {
             for (int tt = 0; tt < T && ok; tt++)
-                ok = tile(tt, tt > 0 ? ((tt - 1) & 1 ? wc1 : wc0) : nullptr, tt + 1 < T ? ((tt & 1) ? wc1 : wc0) : nullptr);
+                ok = edr_tile<R, COL>(lpts, spts, nlane, nstep, tt, tt > 0 ? ((tt - 1) & 1 ? wc1 : wc0) : nullptr,
+                                      tt + 1 < T ? ((tt & 1) ? wc1 : wc0) : nullptr, ep | ((tt - 1) & 0xff),
+                                      ep | (tt & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit);
             finished = true;
         } else {
             carry_t* pc = ctl.pair_carry + (size_t)it.z * 2 * ctl.stride;
             const bool stalled = p == ctl.stall_pair && t == 0;
-            ok = tile(t, t > 0 ? pc + ((t - 1) & 1) * ctl.stride : nullptr,
-                      t + 1 < T && !stalled ? pc + (t & 1) * ctl.stride : nullptr);
+            ok = edr_tile<R, COL>(lpts, spts, nlane, nstep, t, t > 0 ? pc + ((t - 1) & 1) * ctl.stride : nullptr,
+                                  t + 1 < T && !stalled ? pc + (t & 1) * ctl.stride : nullptr, ep | ((t - 1) & 0xff),
+                                  ep | (t & 0xff), u, bring[wib], cring[wib], result, ctl.spin_limit);
             finished = t == T - 1;
         }
         if (!ok) {
@@ -632,20 +614,18 @@ __global__ void __launch_bounds__(kTileWarps * 32, R == 2 ? 4 : 3) k_edr_tiles(S
 
 /* Host side: schedule (count, write) -> tiled kernel. cap is the number of pairs (exact for
  * host-known lists, an upper bound for device-counted ones); max_rows / max_cols bound the
- * shorter / longer side of every pair; form: 0 picks row or column tiles per pair, 1 / 2 force
- * row / column tiles. ev0/ev1, when given, bracket the tile kernel. */
-template <int R, class Src>
-int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_cols, int form, float u,
+ * shorter / longer side of every pair. ev0/ev1, when given, bracket the tile kernel. */
+template <int R, bool COL, class Src>
+int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
                  unsigned long long* cells, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
     int st = GAT_OK;
     cudaStream_t s = ctx->stream;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr_tiles<R, Src>, kTileWarps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr_tiles<R, COL, Src>, kTileWarps * 32, 0);
     /* a serving lane leaves sm_reserve SMs free of this persistent grid for other streams */
     const int grid = std::max(1, ctx->sm_count - ctx->sm_reserve) * (per_sm > 0 ? per_sm : 1);
-    /* carry rows run along the step side; tiles are cut along the lane side (either side of a
-     * pair when the form is chosen per pair) */
-    const int max_lane = form == 1 ? max_rows : max_cols, max_step = form == 2 ? max_rows : max_cols;
+    /* carry rows run along the step side; tiles are cut along the lane side */
+    const int max_lane = COL ? max_cols : max_rows, max_step = COL ? max_rows : max_cols;
     const int stride = max_step + 2;
     const int maxT = max_lane <= 0 ? 1 : (max_lane + 32 * R - 1) / (32 * R);
     const size_t budget = (size_t)512 << 20; /* cooperative carry rows */
@@ -663,7 +643,7 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     if (!ctr || !meta || !items || !wcarry || (coop > 0 && !pcarry)) return st;
     (void)launch_dep(ctx, k_zero_words, dim3(1), dim3(256), 0, s, ctr, (int)kCtrWords);
     const int pgrid = (int)std::max<int64_t>(1, std::min<int64_t>((cap + 255) / 256, (int64_t)ctx->sm_count * 8));
-    (void)launch_dep(ctx, k_sched_count<R, Src>, dim3(pgrid), dim3(256), 0, s, src, (int)cap, (int)coop, form, ctr, meta);
+    (void)launch_dep(ctx, k_sched_count<R, COL, Src>, dim3(pgrid), dim3(256), 0, s, src, (int)cap, (int)coop, ctr, meta);
     count_launch(ctx);
     (void)launch_dep(ctx, k_sched_write<Src>, dim3(pgrid), dim3(256), 0, s, src, (int)cap, ctr, meta, items, edr_epochs(ctx));
     count_launch(ctx);
@@ -673,7 +653,7 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
                 ctx->d_flag, stall >= 0 ? (1 << 12) : kSpinLimit, stall};
     timed_begin(ctx, GAT_KERNEL_EDR);
     if (ev0) cudaEventRecord(ev0, s);
-    (void)launch_dep(ctx, k_edr_tiles<R, Src>, dim3(grid), dim3(kTileWarps * 32), 0, s, src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
+    (void)launch_dep(ctx, k_edr_tiles<R, COL, Src>, dim3(grid), dim3(kTileWarps * 32), 0, s, src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
     if (ev1) cudaEventRecord(ev1, s);
     timed_end(ctx, GAT_KERNEL_EDR, 0.0);
     count_launch(ctx);
@@ -681,18 +661,19 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     return GAT_OK;
 }
 
-/* Tile shapes: rows (or columns) per lane 2, 4, 8 and the form rule: shape = R | form << 4
- * (form 0 per pair, 1 row tiles, 2 column tiles) */
-constexpr int kShapeForm = 4;
+/* Tile shapes: rows (or columns) per lane 2, 4, 8, in row or column form. shape = R | COL << 4 */
+constexpr int kShapeCol = 16;
 
 template <class Src>
 int launch_shape(gat_ctx* ctx, int shape, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
                  unsigned long long* cells, cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
-    const int form = shape >> kShapeForm;
-    switch (shape & 15) {
-        case 2: return launch_tiles<2, Src>(ctx, src, cap, max_rows, max_cols, form, u, cells, ev0, ev1);
-        case 8: return launch_tiles<8, Src>(ctx, src, cap, max_rows, max_cols, form, u, cells, ev0, ev1);
-        default: return launch_tiles<4, Src>(ctx, src, cap, max_rows, max_cols, form, u, cells, ev0, ev1);
+    switch (shape) {
+        case 2: return launch_tiles<2, false, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 4: return launch_tiles<4, false, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 8: return launch_tiles<8, false, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 2 | kShapeCol: return launch_tiles<2, true, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        case 8 | kShapeCol: return launch_tiles<8, true, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
+        default: return launch_tiles<4, true, Src>(ctx, src, cap, max_rows, max_cols, u, cells, ev0, ev1);
     }
 }
 
@@ -711,10 +692,13 @@ template <class Src>
 int edr_launch(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int max_cols, float u,
                unsigned long long* cells) {
     if (cap <= 0) return GAT_OK;
-    int cand[3], nc = 0;
-    for (int r : {4, 8, 2}) {
-        if (ctx->edr_rows && ctx->edr_rows != r) continue;
-        cand[nc++] = r | (ctx->edr_form << kShapeForm);
+    int cand[6], nc = 0;
+    for (int form = 0; form < 2; form++) {
+        if (ctx->edr_form && ctx->edr_form != form + 1) continue;
+        for (int r : {4, 8, 2}) {
+            if (ctx->edr_rows && ctx->edr_rows != r) continue;
+            cand[nc++] = r | (form ? kShapeCol : 0);
+        }
     }
     if (nc == 1) return launch_shape(ctx, cand[0], src, cap, max_rows, max_cols, u, cells);
     const uint64_t key = ((uint64_t)Src::kKind << 60) | ((uint64_t)(ctx->edr_rows | ctx->edr_form << 4) << 52) |

@@ -102,10 +102,9 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  *   same for every choice. 2, 4 or 8 fixes the value. Setting the knob clears the tuned table.
  * gat_ctx_get_tuning(GAT_TUNE_EDR_ROWS) returns the knob; GAT_TUNE_EDR_TUNED returns the
  * number of tuned shape classes.
- * GAT_TUNE_EDR_FORM: 0 (default) = each pair takes the tile form with fewer lane-steps, 1 =
- *   row tiles (lanes own rows of the shorter side, steps walk the longer side), 2 = column
- *   tiles (lanes own columns, steps walk the shorter side: a shorter critical path for pairs of
- *   uneven length). Same results.
+ * GAT_TUNE_EDR_FORM: 0 (default) = autotune, 1 = row tiles (lanes own rows of the shorter
+ *   side, steps walk the longer side), 2 = column tiles (lanes own columns, steps walk the
+ *   shorter side: a shorter critical path for pairs of uneven length). Same results.
  * GAT_TUNE_TOPK_CHUNK / GAT_TUNE_TOPK_GROWTH: candidates a query evaluates in the first round
  *   of the top-k walk, and the factor each later round grows by (0 = defaults: a first round of
  *   1280 for up to 4 queries per batch and 128 for larger batches, never below 8k or 4k;
