@@ -75,26 +75,44 @@ __device__ __forceinline__ Box load_box(const gat_mbb* q, int i) {
 __device__ __forceinline__ void set_flag(int32_t* flag, int code) { atomicCAS(flag, 0, code); }
 
 /* ---------------------------------------------------------------- candidates */
-/* emit(pbeg, pend) for each candidate leaf; returns false on stack overflow */
+/* Whole subtrees. Quadtree node boxes (the Grid's and the MortonGrid's) are made from the first
+ * and last cell of the node by float expressions that are monotone in the cell's column and row
+ * (Grid.cpp:121), so every descendant's box lies within its ancestor's. When a node's box lies
+ * strictly inside the query, BoxIntersect is therefore non-zero for every descendant, the
+ * traversal takes every leaf below it, and those leaves' point ranges tile the node's own range
+ * [pbeg, pend) in visiting order (children in Morton order). The walks emit such a node as that
+ * one range: the range joiner of walk_ranges turns the leaves' ranges into exactly the same
+ * joined range, so the items are unchanged and the walk visits only the nodes that straddle the
+ * query's border. */
+__device__ __forceinline__ bool box_inside(const Box& q, const float4& m) {
+    return q.xmin < m.x && m.z < q.xmax && q.ymin < m.y && m.w < q.ymax;
+}
+
+/* emit(pbeg, pend) for each candidate leaf (or whole subtree, above); returns false on stack
+ * overflow. Stack entries are node indices, complemented for a subtree inside the query. */
 template <class Emit>
 __device__ bool grid_walk(const GridDev& g, const Box& q, Emit emit, int start = 0) {
     int stack[kStack];
     int sp = 0;
     stack[sp++] = start;
     while (sp > 0) {
-        int nd = stack[--sp];
-        int ch = g.node_child[nd];
+        const int e = stack[--sp];
+        if (e < 0) {
+            emit(g.node_pbeg[~e], g.node_pend[~e]);
+            continue;
+        }
+        const int ch = g.node_child[e];
         if (ch < 0) {
             /* leaves are taken without a test (Grid.cpp:430-433) */
-            emit(g.node_pbeg[nd], g.node_pend[nd]);
+            emit(g.node_pbeg[e], g.node_pend[e]);
             continue;
         }
         /* push in reverse so children are visited UL, UR, DL, DR (Grid.cpp:436-443) */
         for (int c = 3; c >= 0; c--) {
-            float4 m = g.node_mbb[ch + c];
+            const float4 m = g.node_mbb[ch + c];
             if (box_intersect(q, Box{m.x, m.y, m.z, m.w})) {
                 if (sp >= kStack) return false;
-                stack[sp++] = ch + c;
+                stack[sp++] = box_inside(q, m) ? ~(ch + c) : ch + c;
             }
         }
     }
@@ -169,25 +187,29 @@ __device__ __forceinline__ void morton_emit(const MortonDev& m, int level, uint3
 
 /* MortonGrid::findMatchNodeInQuadTree (MortonGrid.cpp:356-393): leaves are taken without a
  * test, children in the order UL, UR, DL, DR when BoxIntersect(query, child box) is non-zero.
- * Stack entries pack (id << 4) | level (level <= 13). */
+ * Stack entries pack (id << 4) | level (level <= 13, id < 2^26); bit 31 marks a subtree inside
+ * the query, emitted whole (box_inside). */
 template <class Emit>
 __device__ bool morton_walk(const MortonDev& m, const Box& q, Emit emit, int level0, uint32_t id0) {
+    constexpr uint32_t kWhole = 0x80000000u;
     uint32_t stack[kStack];
     int sp = 0;
     stack[sp++] = (id0 << 4) | (uint32_t)level0;
     while (sp > 0) {
         const uint32_t e = stack[--sp];
         const int level = (int)(e & 15u);
-        const uint32_t id = e >> 4;
-        if (morton_leaf(m, level, id)) {
+        const uint32_t id = (e & ~kWhole) >> 4;
+        if ((e & kWhole) || morton_leaf(m, level, id)) {
             morton_emit(m, level, id, emit);
             continue;
         }
         for (int c = 3; c >= 0; c--) {
             const uint32_t cid = (id << 2) + (uint32_t)c;
-            if (box_intersect(q, morton_box(m, level + 1, cid))) {
+            const Box b = morton_box(m, level + 1, cid);
+            if (box_intersect(q, b)) {
                 if (sp >= kStack) return false;
-                stack[sp++] = (cid << 4) | (uint32_t)(level + 1);
+                const bool whole = box_inside(q, make_float4(b.xmin, b.ymin, b.xmax, b.ymax));
+                stack[sp++] = (cid << 4) | (uint32_t)(level + 1) | (whole ? kWhole : 0u);
             }
         }
     }
