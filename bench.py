@@ -432,22 +432,28 @@ def hbm_peak():
     return float(p.get("hbm_gbs", 6650.0)), ("measured" if "hbm_gbs" in p else "fallback")
 
 
-RANGE_TRAFFIC_RATIO = 0.936  # (12.660 GB read + 0.031 GB written) / 13.557 GB algorithmic, one grid launch
+# DRAM read + write / algorithmic bytes of k_range_hash, from a one-pass ncu capture (dram__bytes_read.sum,
+# dram__bytes_write.sum) of the C3 batch on the 1M-walk set: Grid (5.850 + 0.088) GB / 41.46 GB, FSG
+# (4.650 + 0.030) GB / 41.29 GB. The locality order serves neighbouring queries' points from L2.
+RANGE_TRAFFIC_RATIO = {"grid": 0.143, "fsg": 0.113}
 
 
-def range_roofline(st, name):
+def range_roofline(st, name, index="grid"):
     gbs, src = hbm_peak()
     if st["launches"] == 0 or st["ms"] <= 0:
         return None
     per_bytes = st["work"] / st["launches"]
     per_s = st["ms"] / st["launches"] / 1e3
     ach = per_bytes / per_s / 1e9
+    ratio = RANGE_TRAFFIC_RATIO.get(index)
     return {"kernel": name, "bound": "hbm", "achieved": round(ach, 1), "peak": gbs, "unit": "GB/s",
-            "frac": round(ach / gbs, 4), "traffic": round(RANGE_TRAFFIC_RATIO * per_bytes),
+            "frac": round(ach / gbs, 4), "traffic": round(ratio * per_bytes) if ratio else None,
             "work_per_launch": per_bytes,
             "note": f"algorithmic bytes: 8 B (x, y) per candidate point + 4 B per hit; peak of {src}; traffic = "
-                    f"{RANGE_TRAFFIC_RATIO} x algorithmic, the dram read+write / algorithmic ratio of an ncu capture of "
-                    "k_range_hash on the same query distribution over a 300k-walk set (it scales with the bytes scanned)"}
+                    + (f"{ratio} x algorithmic, the dram read+write / algorithmic ratio of a one-pass ncu capture of "
+                       f"this index's k_range_hash on the 1M-walk C3 batch" if ratio else "not captured for this index")
+                    + "; DRAM traffic well below the algorithmic bytes means L2 serves most of them (locality order), "
+                      "so the kernel is issue-bound, not HBM-bound"}
 
 
 def edr_roofline(st, clk):
@@ -552,8 +558,8 @@ def run_c1(args, world, rank, local, td):
                 "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int((nq + 1) * 8 + total_ids * 4)},
         "gpu_launches": int(launches),
         "batched": {"value": round(nq * world * args.steps / (btot / 1e3), 3), "unit": "queries/s",
-                    "speedup_vs_plain": round(tot / btot, 2), "roofline": range_roofline(bscan, "k_range_hash")},
-        "roofline": range_roofline(scan, "k_range_hash"),
+                    "speedup_vs_plain": round(tot / btot, 2), "roofline": range_roofline(bscan, "k_range_hash", None)},
+        "roofline": range_roofline(scan, "k_plain_scan", None),
         "clocks": clk,
         "result_ids": total_ids,
     })
@@ -683,7 +689,7 @@ def run_c3(args, world, rank, local, td):
                 "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int((nq + 1) * 8 + g["ids"] * 4)},
         "gpu_launches": int(g["launches"]),
         "indexes": {k: {"queries_per_s": round(nq * world * args.steps / (v["ms"] / 1e3), 1), "result_ids": v["ids"],
-                        "roofline": range_roofline(v["scan"], "k_range_hash")} for k, v in res.items()},
+                        "roofline": range_roofline(v["scan"], "k_range_hash", k)} for k, v in res.items()},
         "plain_sample": {"queries": ns, "queries_per_s": round(plain_qps, 1),
                          "batched_speedup": round(nq * world * args.steps / (g["ms"] / 1e3) / plain_qps, 1)},
         "roofline": range_roofline(g["scan"], "k_range_hash"),
@@ -1425,7 +1431,7 @@ def run_suite(args, world, rank, local, td):
         "range": {
             "indexes": {k: {"queries_per_s": round(nq * world * args.steps / (v["ms"] / 1e3), 1), "result_ids": v["ids"],
                             "ms_per_step": round(v["ms"] / args.steps, 4),
-                            "roofline": range_roofline(v["scan"], "k_range_hash")} for k, v in res.items()},
+                            "roofline": range_roofline(v["scan"], "k_range_hash", k)} for k, v in res.items()},
             "plain": {"queries": ps, "steps": len(pms), "queries_per_s": round(plain_qps, 1),
                       "form": "gat_range_query_dev with GAT_EXEC_PLAIN: one query per launch sequence",
                       "sample": f"every {nq // ps}th of the 100k rectangles"},

@@ -88,6 +88,27 @@ void free_slots(gat_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
 }
 
+void* host_stage(gat_ctx* ctx, size_t bytes, int* status) {
+    if (bytes <= ctx->h_stage_bytes) return ctx->h_stage;
+    if (ctx->h_stage) {
+        /* an earlier copy may still read it */
+        cudaStreamSynchronize(ctx->stream);
+        cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = nullptr;
+        ctx->h_stage_bytes = 0;
+    }
+    const size_t nb = std::max<size_t>(bytes, (size_t)64 << 10);
+    void* p = nullptr;
+    cudaError_t e = cudaMallocHost(&p, nb);
+    if (e != cudaSuccess) {
+        *status = cuda_fail(ctx, e, "pinned staging");
+        return nullptr;
+    }
+    ctx->h_stage = p;
+    ctx->h_stage_bytes = nb;
+    return p;
+}
+
 void* scratch_zeroed(gat_ctx* ctx, int slot, size_t bytes, int* status) {
     void* p = scratch(ctx, slot, bytes, status);
     if (p && ctx->slot_fresh[slot]) {
@@ -115,9 +136,12 @@ void* index_alloc(gat_index* ix, size_t bytes, int* status) {
 }
 
 int check_device_flag(gat_ctx* ctx, const char* what) {
-    int32_t flag = 0;
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), what);
+    /* read into the context's pinned words: a copy to pageable memory goes through the driver's
+     * shared staging buffer and can wait behind other streams' pageable copies */
+    int32_t* hf = reinterpret_cast<int32_t*>(ctx->h_pinned + 63);
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(hf, ctx->d_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), what);
     GAT_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream), what);
+    const int32_t flag = *hf;
     if (flag == 0) return GAT_OK;
     cudaMemsetAsync(ctx->d_flag, 0, sizeof(int32_t), ctx->stream);
     cudaStreamSynchronize(ctx->stream);
@@ -278,6 +302,7 @@ void gat_ctx_destroy(gat_ctx* ctx) {
     if (ctx->build_pool) cudaMemPoolDestroy(ctx->build_pool);
     if (ctx->d_flag) cudaFree(ctx->d_flag);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -356,6 +381,18 @@ int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
         ctx->test_stall_pair = value;
         return GAT_OK;
     }
+    if (knob == GAT_TUNE_RANGE_SHAPE) {
+        if (value < 0 || value > 2) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: range shape must be 0, 1 or 2");
+        ctx->range_shape = value;
+        std::lock_guard<std::mutex> tk(ctx->tune_mu);
+        ctx->range_tune.clear();
+        return GAT_OK;
+    }
+    if (knob == GAT_TUNE_SERVE_RESERVE) {
+        if (value < 0 || value > 90) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: serve reserve must be 0..90");
+        ctx->serve_reserve = value;
+        return GAT_OK;
+    }
     if (knob != GAT_TUNE_EDR_ROWS) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: unknown knob");
     if (value != 0 && value != 2 && value != 4 && value != 8)
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR rows per lane must be 0 (autotune), 2, 4 or 8");
@@ -386,6 +423,10 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
         *value = ctx->test_stall_pair;
     else if (knob == GAT_TUNE_DEP_LAUNCH)
         *value = ctx->dep_launch;
+    else if (knob == GAT_TUNE_SERVE_RESERVE)
+        *value = ctx->serve_reserve;
+    else if (knob == GAT_TUNE_RANGE_SHAPE)
+        *value = ctx->range_shape;
     else
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_get_tuning: unknown knob");
     return GAT_OK;

@@ -651,11 +651,23 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     const int stall = ctx->test_stall_pair - 1;
     TileCtl ctl{items, ctr + 2, pcarry, wcarry, stride, reinterpret_cast<const unsigned long long*>(ctr + kCtrEpoch),
                 ctx->d_flag, stall >= 0 ? (1 << 12) : kSpinLimit, stall};
+    /* serving lanes: after the previous EDR grid of any sibling lane (not inside a capture, whose
+     * graph cannot wait on an event recorded outside it) */
+    std::unique_lock<std::mutex> chain;
+    if (ctx->edr_chain) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(s, &cs);
+        if (cs == cudaStreamCaptureStatusNone) {
+            chain = std::unique_lock<std::mutex>(ctx->edr_chain->mu);
+            GAT_CUDA_TRY(ctx, cudaStreamWaitEvent(s, ctx->edr_chain->ev, 0), "edr chain");
+        }
+    }
     timed_begin(ctx, GAT_KERNEL_EDR);
     if (ev0) cudaEventRecord(ev0, s);
     (void)launch_dep(ctx, k_edr_tiles<R, COL, Src>, dim3(grid), dim3(kTileWarps * 32), 0, s, src, u, ctl, reinterpret_cast<unsigned*>(ctr), cells);
     if (ev1) cudaEventRecord(ev1, s);
     timed_end(ctx, GAT_KERNEL_EDR, 0.0);
+    if (chain.owns_lock()) GAT_CUDA_TRY(ctx, cudaEventRecord(ctx->edr_chain->ev, s), "edr chain");
     count_launch(ctx);
     GAT_CUDA_TRY(ctx, cudaGetLastError(), "edr launch");
     return GAT_OK;

@@ -82,6 +82,8 @@ struct EdrPair {
 }  // namespace gat
 
 /* ---------------------------------------------------------------- handles */
+struct EdrChain;
+
 struct gat_ctx {
     int device = 0;
     int sm_count = 0;
@@ -103,6 +105,8 @@ struct gat_ctx {
     int64_t t_launches[GAT_KERNEL_CLASSES] = {0, 0, 0};
     double t_work[GAT_KERNEL_CLASSES] = {0, 0, 0};
     int64_t* h_pinned = nullptr; /* pinned host words for small D2H reads */
+    void* h_stage = nullptr;     /* pinned staging for host arrays the library builds (host_stage) */
+    size_t h_stage_bytes = 0;
     gat_ctx* root = nullptr; /* worker contexts: the context whose indexes they may use */
     /* EDR rows per lane: 0 = autotune per shape class (edr_tune), else fixed */
     int edr_rows = 0;
@@ -112,12 +116,24 @@ struct gat_ctx {
     int dep_launch = 1;                  /* programmatic dependent launch on the query path */
     int test_stall_pair = 0;             /* GAT_TUNE_TEST_STALL_CARRY (tests of the bounded wait) */
     int sm_reserve = 0;                  /* SMs the persistent EDR kernel leaves to other streams (serving lanes) */
+    int serve_reserve = 0;               /* GAT_TUNE_SERVE_RESERVE: percent of the SMs a server's top-k lanes leave free */
+    EdrChain* edr_chain = nullptr;       /* serving lanes: EDR grids of sibling lanes run one at a time */
     cudaMemPool_t build_pool = nullptr;  /* scratch slots and index-build temporaries, kept until gat_ctx_trim */
     std::map<uint64_t, int> edr_tune; /* worker contexts use their root's table */
+    int range_shape = 0;               /* GAT_TUNE_RANGE_SHAPE: 0 = tuned per batch-size class, 1, 2 fixed */
+    std::map<uint64_t, int> range_tune; /* (index kind, batch size class) -> hash kernel shape */
     std::mutex tune_mu;
     /* objects that hold device memory of this context's scratch or workers (cached CUDA graphs);
      * released first by gat_ctx_destroy and gat_ctx_trim */
     std::vector<std::pair<void*, void (*)(void*)>> owned;
+};
+
+/* The persistent EDR grids of a server's top-k lanes run one at a time: each launch waits for
+ * the completion event of the previous one (of any lane) and records its own. A grid leaves free
+ * CTA slots for the range lane only while no second grid is resident to fill them. */
+struct EdrChain {
+    std::mutex mu;
+    cudaEvent_t ev = nullptr;
 };
 
 struct gat_db {
@@ -195,6 +211,9 @@ T* index_upload(gat_index* ix, const std::vector<T>& v, int* status) {
     }
     return p;
 }
+/* pinned host staging of at least `bytes` bytes, owned by the context (one user at a time: the
+ * caller's copies from it must finish before the next call) */
+void* host_stage(gat_ctx* ctx, size_t bytes, int* status);
 /* reads and clears the device status word; returns GAT_OK or the code a kernel stored */
 int check_device_flag(gat_ctx* ctx, const char* what);
 inline void count_launch(gat_ctx* ctx, int n = 1) { ctx->launches += n; }

@@ -811,18 +811,21 @@ __global__ void k_order_scatter(int nq, const int* __restrict__ bucket, unsigned
  * sorts runs of 32 ids in registers, then every id's rank is its position in its run plus its
  * lower bound in every other run; long lists use a block-wide bitonic sort) and written to the
  * arena at the rank; the set is cleared by probing each listed id again. A query whose distinct
- * ids exceed kHashMax goes on the overflow list for the bitmap kernel; the result is the same set
- * either way. */
-constexpr int kHashBits = 13;
-constexpr int kHashSize = 1 << kHashBits; /* 32 KB of ids */
-constexpr int kHashMax = 4096;            /* distinct ids per query (load factor <= 1/2) */
-constexpr int kRankSortMax = 512;         /* lists up to this length are sorted by run ranks */
+ * ids exceed half the set's slots goes on the overflow list for the bitmap kernel; the result is
+ * the same set either way. Two shapes: 256 threads with a 8192-slot set, or 128 threads with a
+ * 4096-slot set (twice the queries in flight per SM, half the warps meeting at each barrier);
+ * run_batch picks one per batch-size class by timing both on the first batch. */
+/* A set of 2^HB slots holds up to 2^(HB-1) ids (load factor <= 1/2): 48 KB of shared memory per
+ * CTA for HB = 13 (256 threads), 24 KB for HB = 12 (128 threads). */
+constexpr int kRankSortMax = 512; /* lists up to this length are sorted by run ranks */
 
-__device__ __forceinline__ unsigned hs_slot(int t) { return ((unsigned)t * 2654435761u) >> (32 - kHashBits); }
+template <int HB>
+__device__ __forceinline__ unsigned hs_slot(int t) { return ((unsigned)t * 2654435761u) >> (32 - HB); }
 
 /* inserts t; a new id is appended to list (count: ids inserted; ovf: the list or a probe ran out) */
+template <int HB>
 __device__ __forceinline__ void hs_insert(int* tab, int* list, int t, int* count, int* ovf) {
-    unsigned h = hs_slot(t);
+    unsigned h = hs_slot<HB>(t);
     for (int p = 0; p < 64; p++) {
         int v = tab[h];
         if (v == t) return;
@@ -830,7 +833,7 @@ __device__ __forceinline__ void hs_insert(int* tab, int* list, int t, int* count
             v = atomicCAS(&tab[h], -1, t);
             if (v == -1) {
                 const int pos = atomicAdd(count, 1);
-                if (pos < kHashMax)
+                if (pos < (1 << (HB - 1)))
                     list[pos] = t;
                 else
                     *ovf = 1;
@@ -838,20 +841,21 @@ __device__ __forceinline__ void hs_insert(int* tab, int* list, int t, int* count
             }
             if (v == t) return;
         }
-        h = (h + 1) & (kHashSize - 1);
+        h = (h + 1) & ((1u << HB) - 1);
     }
     *ovf = 1;
 }
 
 /* empties the slot holding t (t is in the set) */
+template <int HB>
 __device__ __forceinline__ void hs_erase(int* tab, int t) {
-    unsigned h = hs_slot(t);
-    for (int p = 0; p < kHashSize; p++) {
+    unsigned h = hs_slot<HB>(t);
+    for (int p = 0; p < (1 << HB); p++) {
         if (tab[h] == t) {
             tab[h] = -1;
             return;
         }
-        h = (h + 1) & (kHashSize - 1);
+        h = (h + 1) & ((1u << HB) - 1);
     }
 }
 
@@ -880,16 +884,18 @@ __device__ __forceinline__ int lower_bound32(const int* run, int x) {
     return lo + (run[31] < x ? 1 : 0);
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queries, int nq, const int64_t* ioff,
-                                                         const int2* items, const float* __restrict__ X,
-                                                         const float* __restrict__ Y, const int32_t* __restrict__ tid,
-                                                         uint32_t* arena, int64_t cap, unsigned long long* ctr,
-                                                         int64_t* segbase, int64_t* segcnt, int* ovf_list,
-                                                         unsigned long long* work, const int* __restrict__ order) {
+template <int NT, int HB>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* queries, int nq, const int64_t* ioff,
+                                                           const int2* items, const float* __restrict__ X,
+                                                           const float* __restrict__ Y, const int32_t* __restrict__ tid,
+                                                           uint32_t* arena, int64_t cap, unsigned long long* ctr,
+                                                           int64_t* segbase, int64_t* segcnt, int* ovf_list,
+                                                           unsigned long long* work, const int* __restrict__ order) {
+    constexpr int kHashSize = 1 << HB;
     dep_wait();
     extern __shared__ int hs_smem[];
     int* tab = hs_smem;             /* kHashSize */
-    int* buf = hs_smem + kHashSize; /* kHashMax ids in insertion order */
+    int* buf = hs_smem + kHashSize; /* kHashSize / 2 ids in insertion order */
     __shared__ int cnt_sh, ovf_sh, q_sh, next_sh, item_sh;
     __shared__ unsigned long long base_sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -928,12 +934,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
             /* unaligned head and tail points: plain inserts */
             for (int i = r.x + lane; i < head_end; i += 32)
                 if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
-                    hs_insert(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
+                    hs_insert<HB>(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
                     hits++;
                 }
             for (int i = ve + lane; i < r.y; i += 32)
                 if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
-                    hs_insert(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
+                    hs_insert<HB>(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
                     hits++;
                 }
             const float4* X4 = reinterpret_cast<const float4*>(X + vb);
@@ -970,10 +976,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
                 int prev = __shfl_up_sync(FULL, t3, 1);
                 if (lane == 0) prev = carry;
                 carry = __shfl_sync(FULL, t3, 31);
-                if (t0 >= 0 && t0 != prev) hs_insert(tab, buf, t0, &cnt_sh, &ovf_sh);
-                if (t1 >= 0 && t1 != t0) hs_insert(tab, buf, t1, &cnt_sh, &ovf_sh);
-                if (t2 >= 0 && t2 != t1) hs_insert(tab, buf, t2, &cnt_sh, &ovf_sh);
-                if (t3 >= 0 && t3 != t2) hs_insert(tab, buf, t3, &cnt_sh, &ovf_sh);
+                if (t0 >= 0 && t0 != prev) hs_insert<HB>(tab, buf, t0, &cnt_sh, &ovf_sh);
+                if (t1 >= 0 && t1 != t0) hs_insert<HB>(tab, buf, t1, &cnt_sh, &ovf_sh);
+                if (t2 >= 0 && t2 != t1) hs_insert<HB>(tab, buf, t2, &cnt_sh, &ovf_sh);
+                if (t3 >= 0 && t3 != t2) hs_insert<HB>(tab, buf, t3, &cnt_sh, &ovf_sh);
             }
         }
         my_work += 8ull * cand + 4ull * hits;
@@ -1001,7 +1007,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
         } else if (m <= kRankSortMax) {
             /* runs of 32 sorted in registers (padded with INT_MAX), written back in place */
             const int runs = (m + 31) >> 5;
-            for (int c = warp; c < runs; c += kThreads / 32) {
+            for (int c = warp; c < runs; c += NT / 32) {
                 const int i = 32 * c + lane;
                 const int v = warp_sort32(i < m ? buf[i] : INT_MAX);
                 __syncwarp();
@@ -1014,11 +1020,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_range_hash(const gat_mbb* queri
                 for (int c = 0; c < runs; c++)
                     if (c != own) rank += lower_bound32(buf + 32 * c, x);
                 if (write) arena[base + rank] = (uint32_t)x;
-                hs_erase(tab, x);
+                hs_erase<HB>(tab, x);
             }
         } else {
             /* long lists: clear the set, then a block-wide bitonic sort padded to a power of two */
-            for (int i = threadIdx.x; i < m; i += blockDim.x) hs_erase(tab, buf[i]);
+            for (int i = threadIdx.x; i < m; i += blockDim.x) hs_erase<HB>(tab, buf[i]);
             int P = 1;
             while (P < m) P <<= 1;
             for (int i = m + threadIdx.x; i < P; i += blockDim.x) buf[i] = INT_MAX;
@@ -1370,16 +1376,31 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
     int2* items = nullptr;
     int* order = nullptr;
     int grid = 1;
-    size_t smem = 0;
     if ((st = build_items(ctx, ix, d_q, nq, nullptr, &ioff, &items)) != GAT_OK) return st;
     if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
+    /* the hash kernel's two shapes (256 threads / 8192 slots, 128 threads / 4096 slots) */
+    int hgrid[3] = {0, 0, 0};
+    size_t hsmem[3] = {0, (size_t)(8192 + 4096) * sizeof(int), (size_t)(4096 + 2048) * sizeof(int)};
+    int shape = ctx->range_shape;
+    uint64_t tune_key = 0;
+    gat_ctx* tab = ctx->root ? ctx->root : ctx;
     if (ids) {
         if (nq >= kOrderMin && (st = locality_order(ctx, ix, d_q, nq, &order)) != GAT_OK) return st;
-        smem = (size_t)(kHashSize + kHashMax) * sizeof(int);
-        allow_smem(k_range_hash, smem);
+        allow_smem(k_range_hash<256, 13>, hsmem[1]);
+        allow_smem(k_range_hash<128, 12>, hsmem[2]);
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_hash, kThreads, smem);
-        grid = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_hash<256, 13>, 256, hsmem[1]);
+        hgrid[1] = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_hash<128, 12>, 128, hsmem[2]);
+        hgrid[2] = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
+        if (shape == 0) {
+            uint64_t lg = 0;
+            while (lg < 40 && ((int64_t)1 << lg) < nq) lg++;
+            tune_key = ((uint64_t)ix->kind << 8) | lg;
+            std::lock_guard<std::mutex> lk(tab->tune_mu);
+            auto hit = tab->range_tune.find(tune_key);
+            if (hit != tab->range_tune.end()) shape = hit->second;
+        }
     } else {
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_points, kThreads, 0);
@@ -1393,17 +1414,49 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         if (!arena) return st;
         cap = (int64_t)(ctx->slot_bytes[S_RANGE_ARENA] / 4);
         /* cursor: [0] arena entries, [1] work bytes, [2] query counter, [3] overflowed queries */
-        GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 4 * sizeof(unsigned long long), s), "range");
+        auto hash_launch = [&](int sh, unsigned long long* work) {
+            cudaError_t e = cudaMemsetAsync(cursor, 0, 4 * sizeof(unsigned long long), s);
+            if (e != cudaSuccess) return e;
+            if (sh == 2)
+                k_range_hash<128, 12><<<hgrid[2], 128, hsmem[2], s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena,
+                                                                      cap, cursor, segbase, segcnt, ovf_list, work, order);
+            else
+                k_range_hash<256, 13><<<hgrid[1], 256, hsmem[1], s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena,
+                                                                      cap, cursor, segbase, segcnt, ovf_list, work, order);
+            count_launch(ctx);
+            return cudaGetLastError();
+        };
+        if (ids && shape == 0) {
+            /* first batch of its class: time both shapes on it and keep the faster (the later run
+             * below overwrites every output) */
+            cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+            float ms[3] = {0.f, 0.f, 0.f};
+            bool ok = true;
+            for (auto& e : ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+            for (int sh = 1; sh <= 2 && ok; sh++)
+                ok = cudaEventRecord(ev[sh - 1], s) == cudaSuccess && hash_launch(sh, nullptr) == cudaSuccess &&
+                     cudaEventRecord(ev[sh], s) == cudaSuccess;
+            ok = ok && cudaEventSynchronize(ev[2]) == cudaSuccess &&
+                 cudaEventElapsedTime(&ms[1], ev[0], ev[1]) == cudaSuccess &&
+                 cudaEventElapsedTime(&ms[2], ev[1], ev[2]) == cudaSuccess;
+            for (auto& e : ev)
+                if (e) cudaEventDestroy(e);
+            if (!ok) return cuda_fail(ctx, cudaGetLastError(), "range shape tuning");
+            shape = ms[2] < ms[1] ? 2 : 1;
+            std::lock_guard<std::mutex> lk(tab->tune_mu);
+            tab->range_tune[tune_key] = shape;
+        }
         unsigned long long* work = ctx->timing ? cursor + 1 : nullptr;
         timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
-        if (ids)
-            k_range_hash<<<grid, kThreads, smem, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap, cursor,
-                                                      segbase, segcnt, ovf_list, work, order);
-        else
+        if (ids) {
+            GAT_CUDA_TRY(ctx, hash_launch(shape, work), "range scan launch");
+        } else {
+            GAT_CUDA_TRY(ctx, cudaMemsetAsync(cursor, 0, 4 * sizeof(unsigned long long), s), "range");
             k_range_points<<<grid, kThreads, 0, s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_key, key_bits, arena,
                                                      cap, cursor, segbase, segcnt);
+            count_launch(ctx);
+        }
         timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
-        count_launch(ctx);
         GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
         GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
         GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");

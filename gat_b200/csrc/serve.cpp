@@ -57,6 +57,37 @@ struct Request {
     int64_t t[3] = {0, 0, 0};          /* arrival, admission, completion */
 };
 
+/* Pinned host buffers of a lane. A copy between pageable host memory and the device goes
+ * through the driver's staging buffer shared by all streams, so a lane whose copy waits for a
+ * long top-k batch on its own stream held every other lane's copies back (range batches then
+ * took as long as the top-k batch running beside them); copies from and to pinned memory are
+ * plain DMA on the lane's own stream. Grown by doubling, freed with the server. */
+struct PinnedArena {
+    char* p = nullptr;
+    size_t bytes = 0;
+    std::vector<char> fallback; /* a context without a device (queries then fail anyway) */
+    char* get(size_t b) {
+        if (b <= bytes) return p;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        const size_t nb = std::max<size_t>(b, (size_t)4 << 20);
+        void* q = nullptr;
+        if (cudaMallocHost(&q, nb) != cudaSuccess) {
+            cudaGetLastError();
+            fallback.resize(b);
+            return fallback.data();
+        }
+        p = (char*)q;
+        bytes = nb;
+        return p;
+    }
+    ~PinnedArena() {
+        if (p) cudaFreeHost(p);
+    }
+};
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
 struct Batch {
     int kind = REQ_RANGE;
     int index_kind = 0, result_kind = 0;
@@ -68,6 +99,7 @@ struct Batch {
 
 struct gat_server {
     gat_ctx* ctx = nullptr;
+    EdrChain chain; /* the top-k lanes' EDR grids, one at a time */
     const gat_index* ix[3] = {nullptr, nullptr, nullptr};
     gat_server_config cfg{};
     std::vector<gat_ctx*> lanes;
@@ -209,20 +241,25 @@ struct gat_server {
         cv_lane.notify_all();
     }
 
-    void run_range(gat_ctx* w, Batch* b) {
+    void run_range(gat_ctx* w, PinnedArena& pa, Batch* b) {
         const int n = (int)b->reqs.size();
-        std::vector<gat_mbb> q(n);
-        for (int i = 0; i < n; i++) q[i] = b->reqs[i]->box;
-        std::vector<int64_t> off((size_t)n + 1, 0);
         int64_t cap = std::max<int64_t>(1024, (int64_t)(hits_mean[b->index_kind] * n * 1.5)), need = 0;
         const bool pts = b->result_kind == GAT_RESULT_POINTS;
-        std::vector<int32_t> tid, pidx;
+        gat_mbb* q = nullptr;
+        int64_t* off = nullptr;
+        int32_t *tid = nullptr, *pidx = nullptr;
         int rc = GAT_OK;
         for (int attempt = 0; attempt < 2; attempt++) {
-            tid.resize((size_t)cap);
-            pidx.resize(pts ? (size_t)cap : 0);
-            rc = gat_range_query(w, ix[b->index_kind], q.data(), n, b->result_kind, GAT_EXEC_BATCHED, off.data(), tid.data(),
-                                 pts ? pidx.data() : nullptr, cap, &need);
+            /* [queries | offsets | ids | point indexes] in the lane's pinned buffer */
+            const size_t bq = align256((size_t)n * sizeof(gat_mbb)), bo = align256((size_t)(n + 1) * 8);
+            const size_t bt = align256((size_t)cap * 4);
+            char* base = pa.get(bq + bo + bt + (pts ? bt : 0));
+            q = reinterpret_cast<gat_mbb*>(base);
+            off = reinterpret_cast<int64_t*>(base + bq);
+            tid = reinterpret_cast<int32_t*>(base + bq + bo);
+            pidx = pts ? reinterpret_cast<int32_t*>(base + bq + bo + bt) : nullptr;
+            for (int i = 0; i < n; i++) q[i] = b->reqs[i]->box;
+            rc = gat_range_query(w, ix[b->index_kind], q, n, b->result_kind, GAT_EXEC_BATCHED, off, tid, pidx, cap, &need);
             if (rc != GAT_ERR_TRUNCATED) break;
             cap = need;
         }
@@ -230,8 +267,8 @@ struct gat_server {
         for (int i = 0; i < n; i++) {
             Request* r = b->reqs[i];
             if (rc == GAT_OK) {
-                r->tid.assign(tid.begin() + off[i], tid.begin() + off[i + 1]);
-                if (pts) r->pidx.assign(pidx.begin() + off[i], pidx.begin() + off[i + 1]);
+                r->tid.assign(tid + off[i], tid + off[i + 1]);
+                if (pts) r->pidx.assign(pidx + off[i], pidx + off[i + 1]);
             }
             finish(r, rc);
         }
@@ -239,27 +276,38 @@ struct gat_server {
             hits_mean[b->index_kind] = 0.8 * hits_mean[b->index_kind] + 0.2 * std::max(1.0, (double)off[n] / n);
     }
 
-    void run_topk(gat_ctx* w, Batch* b) {
+    void run_topk(gat_ctx* w, PinnedArena& pa, Batch* b) {
         const int n = (int)b->reqs.size();
-        std::vector<int32_t> len(n);
-        std::vector<float> lon, lat;
         int kmax = 0;
+        size_t points = 0;
+        for (Request* r : b->reqs) {
+            kmax = std::max(kmax, r->k);
+            points += r->lon.size();
+        }
+        /* [lengths | lon | lat | ids | distances] in the lane's pinned buffer */
+        const size_t bl = align256((size_t)n * 4), bp = align256(points * 4), br = align256((size_t)n * kmax * 4);
+        char* base = pa.get(bl + 2 * bp + 2 * br);
+        int32_t* len = reinterpret_cast<int32_t*>(base);
+        float* lon = reinterpret_cast<float*>(base + bl);
+        float* lat = reinterpret_cast<float*>(base + bl + bp);
+        int32_t* ids = reinterpret_cast<int32_t*>(base + bl + 2 * bp);
+        int32_t* dist = reinterpret_cast<int32_t*>(base + bl + 2 * bp + br);
+        size_t at = 0;
         for (int i = 0; i < n; i++) {
             Request* r = b->reqs[i];
             len[i] = (int32_t)r->lon.size();
-            lon.insert(lon.end(), r->lon.begin(), r->lon.end());
-            lat.insert(lat.end(), r->lat.begin(), r->lat.end());
-            kmax = std::max(kmax, r->k);
+            std::copy(r->lon.begin(), r->lon.end(), lon + at);
+            std::copy(r->lat.begin(), r->lat.end(), lat + at);
+            at += r->lon.size();
         }
-        std::vector<int32_t> ids((size_t)n * kmax), dist((size_t)n * kmax);
-        int rc = gat_topk(w, ix[GAT_INDEX_GRID], n, len.data(), lon.data(), lat.data(), kmax, b->reqs[0]->eps,
-                          GAT_EXEC_BATCHED, ids.data(), dist.data(), nullptr);
+        int rc = gat_topk(w, ix[GAT_INDEX_GRID], n, len, lon, lat, kmax, b->reqs[0]->eps, GAT_EXEC_BATCHED, ids, dist,
+                          nullptr);
         std::lock_guard<std::mutex> lk(mu);
         for (int i = 0; i < n; i++) {
             Request* r = b->reqs[i];
             if (rc == GAT_OK) {
-                r->ids.assign(ids.begin() + (size_t)i * kmax, ids.begin() + (size_t)i * kmax + r->k);
-                r->dist.assign(dist.begin() + (size_t)i * kmax, dist.begin() + (size_t)i * kmax + r->k);
+                r->ids.assign(ids + (size_t)i * kmax, ids + (size_t)i * kmax + r->k);
+                r->dist.assign(dist + (size_t)i * kmax, dist + (size_t)i * kmax + r->k);
             }
             finish(r, rc);
         }
@@ -267,6 +315,8 @@ struct gat_server {
 
     void run_lane(int i) {
         gat_ctx* w = lanes[i];
+        if (w->device >= 0) cudaSetDevice(w->device);
+        PinnedArena pa;
         for (;;) {
             Batch* b = nullptr;
             {
@@ -276,9 +326,9 @@ struct gat_server {
                 b = lane_batch[i];
             }
             if (b->kind == REQ_TOPK)
-                run_topk(w, b);
+                run_topk(w, pa, b);
             else
-                run_range(w, b);
+                run_range(w, pa, b);
             if (gat_ctx_scratch_bytes(w) > cfg.budget_bytes / (int64_t)lanes.size()) gat_ctx_trim(w);
             std::lock_guard<std::mutex> lk(mu);
             reserved -= b->reserve;
@@ -320,19 +370,31 @@ int gat_server_create(gat_ctx* ctx, const gat_index* grid, const gat_index* stig
         int rc = gat_ctx_create_worker(ctx, &w);
         if (rc != GAT_OK) {
             for (gat_ctx* x : s->lanes) gat_ctx_destroy(x);
+            if (s->chain.ev) cudaEventDestroy(s->chain.ev);
             delete s;
             return fail(ctx, rc, "gat_server_create: worker context");
         }
-        /* lane 0 takes range batches on a high-priority stream; the others leave SMs to it */
+        /* lane 0 takes range batches on a high-priority stream; the others leave SMs to it and
+         * run their EDR grids one at a time */
         if (c.lanes >= 2) {
-            if (i == 0)
+            if (i == 0) {
                 rc = ctx_use_priority_stream(w);
-            else
-                w->sm_reserve = std::max(1, w->sm_count / 8);
+            } else {
+                const int pct = ctx->serve_reserve > 0 ? ctx->serve_reserve : 12;
+                w->sm_reserve = std::max(1, w->sm_count * pct / 100);
+                if (w->device >= 0) {
+                    if (!s->chain.ev && cudaEventCreateWithFlags(&s->chain.ev, cudaEventDisableTiming) != cudaSuccess) {
+                        cudaGetLastError();
+                        rc = GAT_ERR_CUDA;
+                    }
+                    w->edr_chain = &s->chain;
+                }
+            }
         }
         s->lanes.push_back(w);
         if (rc != GAT_OK) {
             for (gat_ctx* x : s->lanes) gat_ctx_destroy(x);
+            if (s->chain.ev) cudaEventDestroy(s->chain.ev);
             delete s;
             return fail(ctx, rc, "gat_server_create: lane stream");
         }
@@ -354,6 +416,7 @@ void gat_server_destroy(gat_server* s) {
     s->scheduler.join();
     for (auto& t : s->workers) t.join();
     for (gat_ctx* w : s->lanes) gat_ctx_destroy(w);
+    if (s->chain.ev) cudaEventDestroy(s->chain.ev);
     delete s;
 }
 

@@ -1344,7 +1344,11 @@ int upload_queries(gat_ctx* ctx, int nq, const int32_t* q_len, const float* lon,
     *dxy = (float2*)(p + b_len + b_off + 2 * b_f);
     cudaStream_t s = ctx->stream;
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(*dl, q_len, (size_t)nq * 4, cudaMemcpyHostToDevice, s), "top-k H2D");
-    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(*doff, h.off.data(), (size_t)(nq + 1) * 8, cudaMemcpyHostToDevice, s), "top-k H2D");
+    /* the offsets are built here: copied from pinned staging, not from pageable memory */
+    int64_t* hoff = (int64_t*)host_stage(ctx, (size_t)(nq + 1) * 8, &st);
+    if (!hoff) return st;
+    std::copy(h.off.begin(), h.off.begin() + (nq + 1), hoff);
+    GAT_CUDA_TRY(ctx, cudaMemcpyAsync(*doff, hoff, (size_t)(nq + 1) * 8, cudaMemcpyHostToDevice, s), "top-k H2D");
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(dlon, lon, (size_t)h.total * 4, cudaMemcpyHostToDevice, s), "top-k H2D");
     GAT_CUDA_TRY(ctx, cudaMemcpyAsync(dlat, lat, (size_t)h.total * 4, cudaMemcpyHostToDevice, s), "top-k H2D");
     int grid = (int)std::min<int64_t>(ctx->sm_count * 8, (h.total + 255) / 256 + 1);

@@ -120,9 +120,18 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  *   for production. v > 0 makes the first tile of pair v - 1 of every later pipelined launch
  *   skip its carry stores and shortens each wait to about 4096 polls, so the next tile of that
  *   pair gives up: the pair gets -1, the call returns GAT_ERR_TIMEOUT, every other pair keeps
- *   its exact distance and the context stays usable. 0 (default) turns it off. */
+ *   its exact distance and the context stays usable. 0 (default) turns it off.
+ * GAT_TUNE_SERVE_RESERVE: read by gat_server_create from the context it is given: the percent of
+ *   the SMs (1..90) that the persistent EDR grids of the server's top-k lanes leave free for its
+ *   range lane; 0 (default) = 12. Same results.
+ * GAT_TUNE_RANGE_SHAPE: block shape of the batched range scan for trajectory-id sets. 0 (default)
+ *   = autotune: the first batch of each (index kind, batch size rounded up to a power of two)
+ *   class times both shapes on its own queries and keeps the faster; 1 = 256 threads per CTA
+ *   with an 8192-slot id set, 2 = 128 threads with a 4096-slot set. Same results. Setting the
+ *   knob clears the tuned table. */
 enum { GAT_TUNE_EDR_ROWS = 1, GAT_TUNE_EDR_TUNED = 2, GAT_TUNE_TOPK_CHUNK = 3, GAT_TUNE_TOPK_GROWTH = 4,
-       GAT_TUNE_EDR_FORM = 5, GAT_TUNE_INDEX_BUILD = 6, GAT_TUNE_DEP_LAUNCH = 7, GAT_TUNE_TEST_STALL_CARRY = 8 };
+       GAT_TUNE_EDR_FORM = 5, GAT_TUNE_INDEX_BUILD = 6, GAT_TUNE_DEP_LAUNCH = 7, GAT_TUNE_TEST_STALL_CARRY = 8,
+       GAT_TUNE_SERVE_RESERVE = 9, GAT_TUNE_RANGE_SHAPE = 10 };
 int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value);
 int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value);
 
