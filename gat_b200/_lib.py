@@ -45,7 +45,7 @@ class ServerConfig(C.Structure):
 
 (GAT_TUNE_EDR_ROWS, GAT_TUNE_EDR_TUNED, GAT_TUNE_TOPK_CHUNK, GAT_TUNE_TOPK_GROWTH, GAT_TUNE_EDR_FORM,
  GAT_TUNE_INDEX_BUILD, GAT_TUNE_DEP_LAUNCH, GAT_TUNE_TEST_STALL_CARRY, GAT_TUNE_SERVE_RESERVE,
- GAT_TUNE_RANGE_SHAPE) = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
+ GAT_TUNE_RANGE_SHAPE, GAT_TUNE_EDR_RESERVE) = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
 
 # (name, restype, argtypes) for every symbol of include/gat_b200.h
 SIGNATURES = [

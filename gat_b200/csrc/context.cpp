@@ -388,6 +388,12 @@ int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
         ctx->range_tune.clear();
         return GAT_OK;
     }
+    if (knob == GAT_TUNE_EDR_RESERVE) {
+        if (value < 0 || value > 90) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: EDR reserve must be 0..90");
+        ctx->sm_reserve = ctx->sm_count * value / 100;
+        ctx->edr_reserve_pct = value;
+        return GAT_OK;
+    }
     if (knob == GAT_TUNE_SERVE_RESERVE) {
         if (value < 0 || value > 90) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: serve reserve must be 0..90");
         ctx->serve_reserve = value;
@@ -427,6 +433,8 @@ int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value) {
         *value = ctx->serve_reserve;
     else if (knob == GAT_TUNE_RANGE_SHAPE)
         *value = ctx->range_shape;
+    else if (knob == GAT_TUNE_EDR_RESERVE)
+        *value = ctx->edr_reserve_pct;
     else
         return fail(ctx, GAT_ERR_ARG, "gat_ctx_get_tuning: unknown knob");
     return GAT_OK;
@@ -525,6 +533,7 @@ void gat_index_destroy(gat_index* ix) {
     cudaStreamSynchronize(ix->ctx->stream);
     for (void* p : ix->allocs) cudaFree(p);
     if (ix->d_pidx) cudaFree(ix->d_pidx);
+    if (ix->d_pbox) cudaFree(ix->d_pbox);
     delete ix;
 }
 

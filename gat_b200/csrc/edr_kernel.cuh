@@ -226,6 +226,8 @@ constexpr int kCtrEpoch = 4 + 2 * kClasses;
 constexpr int kCtrWords = kCtrEpoch + 2;
 typedef unsigned long long carry_t;
 
+constexpr int kEdrCarveoutPct = 100; /* preferred shared-memory share of the SM for k_edr_tiles (launch_tiles) */
+
 struct TileCtl {
     const int4* items; /* (pair, tile or -1 for a whole pair on one warp, cooperative slot, tiles) */
     const int* total;
@@ -621,6 +623,14 @@ int launch_tiles(gat_ctx* ctx, const Src& src, int64_t cap, int max_rows, int ma
     int st = GAT_OK;
     cudaStream_t s = ctx->stream;
     int per_sm = 0;
+    /* An SM's split between L1 and shared memory changes only while no block is resident on it.
+     * With the default (no preference) the persistent grid's blocks, which need 5 KB, leave their
+     * SMs at a small shared-memory split for the whole launch, and a kernel of another stream that
+     * needs more (the range scan's 48 KB blocks) could not start on any of them until the grid
+     * ended: range batches beside a long top-k round waited for it (16 rectangles, 1.1 ms alone:
+     * 10.5 ms median beside 18 ms EDR launches that left half the SMs free; 2.5 ms with the
+     * largest split). The tile kernel reads its points once and uses little L1. */
+    prefer_split(reinterpret_cast<const void*>(k_edr_tiles<R, COL, Src>), ctx->device, kEdrCarveoutPct);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edr_tiles<R, COL, Src>, kTileWarps * 32, 0);
     /* a serving lane leaves sm_reserve SMs free of this persistent grid for other streams */
     const int grid = std::max(1, ctx->sm_count - ctx->sm_reserve) * (per_sm > 0 ? per_sm : 1);

@@ -557,6 +557,7 @@ static int build_fsg(gat_index* ix, gat_mbb range, float cell) {
 using namespace gat;
 
 static int finish_build(gat_ctx* ctx, gat_index* ix, int st, gat_index** out) {
+    if (st == GAT_OK) st = index_point_boxes(ix);
     if (st != GAT_OK) {
         gat_index_destroy(ix);
         return st;

@@ -38,6 +38,7 @@ struct GridDev {
     const int32_t* node_child;
     const int32_t* node_pbeg;
     const int32_t* node_pend;
+    const float4* node_pbox; /* exact box of each node's points (index_point_boxes; null: none) */
 };
 
 struct StigDev {
@@ -50,6 +51,7 @@ struct StigDev {
     const int32_t* lo;     /* leaf: inclusive range */
     const int32_t* hi;
     const float4* mbb;     /* leaf MBB */
+    const float4* pbox;    /* exact box of each leaf's points (index_point_boxes; null: none) */
 };
 
 struct FsgDev {
@@ -116,6 +118,7 @@ struct gat_ctx {
     int dep_launch = 1;                  /* programmatic dependent launch on the query path */
     int test_stall_pair = 0;             /* GAT_TUNE_TEST_STALL_CARRY (tests of the bounded wait) */
     int sm_reserve = 0;                  /* SMs the persistent EDR kernel leaves to other streams (serving lanes) */
+    int edr_reserve_pct = 0;             /* GAT_TUNE_EDR_RESERVE as set (sm_reserve = sm_count * pct / 100) */
     int serve_reserve = 0;               /* GAT_TUNE_SERVE_RESERVE: percent of the SMs a server's top-k lanes leave free */
     EdrChain* edr_chain = nullptr;       /* serving lanes: EDR grids of sibling lanes run one at a time */
     cudaMemPool_t build_pool = nullptr;  /* scratch slots and index-build temporaries, kept until gat_ctx_trim */
@@ -172,6 +175,7 @@ struct gat_index {
     bool host_pending = false;
     std::mutex host_mu;
     int32_t* d_pidx = nullptr; /* device-placed index whose point index does not fit the key */
+    float4* d_pbox = nullptr;  /* derived, not saved in snapshots: GridDev::node_pbox / StigDev::pbox */
     int64_t leaves = 0, nodes = 0;
     gat::GridDev grid{};
     gat::StigDev stig{};
@@ -214,6 +218,10 @@ T* index_upload(gat_index* ix, const std::vector<T>& v, int* status) {
 /* pinned host staging of at least `bytes` bytes, owned by the context (one user at a time: the
  * caller's copies from it must finish before the next call) */
 void* host_stage(gat_ctx* ctx, size_t bytes, int* status);
+/* Derives the exact box of the points under every quadtree node (Grid) or STIG leaf, so that the
+ * range walks can mark candidate ranges whose every point is a hit (pbox.cu). Called after a
+ * Grid or STIG is built or loaded on a device context; a no-op for other kinds. */
+int index_point_boxes(gat_index* ix);
 /* reads and clears the device status word; returns GAT_OK or the code a kernel stored */
 int check_device_flag(gat_ctx* ctx, const char* what);
 inline void count_launch(gat_ctx* ctx, int n = 1) { ctx->launches += n; }

@@ -10,6 +10,8 @@
  * without the attribute. */
 #pragma once
 
+#include <mutex>
+#include <set>
 #include <utility>
 
 #include "internal.h"
@@ -17,6 +19,20 @@
 namespace gat {
 
 __device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+/* Sets a kernel's preferred split between L1 and shared memory (percent of the largest shared
+ * size) the first time it is asked for on a device; later requests for the same kernel keep the
+ * first value. An SM takes the split of the first block that lands on it while it is empty and
+ * keeps it until it is empty again, so a long-running kernel fixes the split of its SMs for every
+ * other stream's blocks. */
+inline void prefer_split(const void* kernel, int device, int pct) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done.insert({kernel, device}).second) return;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct) != cudaSuccess)
+        cudaGetLastError();
+}
 
 template <class... P, class... A>
 inline cudaError_t launch_dep(const gat_ctx* ctx, void (*kernel)(P...), dim3 grid, dim3 block, size_t smem,

@@ -31,7 +31,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kStack = 96;
-constexpr int kChunk = 1024; /* candidate points per scan item */
+constexpr int kChunk = 1024;       /* candidate points per scan item */
+constexpr int kChunkAllHit = 4096; /* points per item whose every point is a hit (ids only) */
+constexpr int kAllHit = (int)0x80000000; /* item start flag: every point of the item is a hit */
 
 struct Box {
     float xmin, ymin, xmax, ymax;
@@ -88,8 +90,17 @@ __device__ __forceinline__ bool box_inside(const Box& q, const float4& m) {
     return q.xmin < m.x && m.z < q.xmax && q.ymin < m.y && m.w < q.ymax;
 }
 
-/* emit(pbeg, pend) for each candidate leaf (or whole subtree, above); returns false on stack
- * overflow. Stack entries are node indices, complemented for a subtree inside the query. */
+/* All points hit. A range the walk takes (a leaf, or a whole subtree as above) whose exact point
+ * box (pbox.cu) lies inside the query under MBB::pInBox's inclusive comparisons has every point
+ * in the query: the scan takes its ids without testing coordinates. False without point boxes. */
+__device__ __forceinline__ bool points_inside(const Box& q, const float4* pbox, int nd) {
+    if (!pbox) return false;
+    const float4 b = pbox[nd];
+    return b.x >= q.xmin && b.z <= q.xmax && b.y >= q.ymin && b.w <= q.ymax;
+}
+
+/* emit(pbeg, pend, all_hit) for each candidate leaf (or whole subtree, above); returns false on
+ * stack overflow. Stack entries are node indices, complemented for a subtree inside the query. */
 template <class Emit>
 __device__ bool grid_walk(const GridDev& g, const Box& q, Emit emit, int start = 0) {
     int stack[kStack];
@@ -98,13 +109,13 @@ __device__ bool grid_walk(const GridDev& g, const Box& q, Emit emit, int start =
     while (sp > 0) {
         const int e = stack[--sp];
         if (e < 0) {
-            emit(g.node_pbeg[~e], g.node_pend[~e]);
+            emit(g.node_pbeg[~e], g.node_pend[~e], points_inside(q, g.node_pbox, ~e));
             continue;
         }
         const int ch = g.node_child[e];
         if (ch < 0) {
             /* leaves are taken without a test (Grid.cpp:430-433) */
-            emit(g.node_pbeg[e], g.node_pend[e]);
+            emit(g.node_pbeg[e], g.node_pend[e], points_inside(q, g.node_pbox, e));
             continue;
         }
         /* push in reverse so children are visited UL, UR, DL, DR (Grid.cpp:436-443) */
@@ -129,7 +140,7 @@ __device__ bool stig_walk(const StigDev& s, const Box& q, Emit emit, int start =
         if (s.kind[nd]) {
             /* STIG::searchNode(LeafNode*) (STIG.cpp:241-252): leaf MBB against the query */
             float4 m = s.mbb[nd];
-            if (box_intersect(Box{m.x, m.y, m.z, m.w}, q)) emit(s.lo[nd], s.hi[nd] + 1);
+            if (box_intersect(Box{m.x, m.y, m.z, m.w}, q)) emit(s.lo[nd], s.hi[nd] + 1, points_inside(q, s.pbox, nd));
             continue;
         }
         /* STIG::searchNode(InternalNode*) (STIG.cpp:201-239) with intersectBlock (:340-347) */
@@ -162,7 +173,7 @@ __device__ void fsg_walk(const FsgDev& f, const Box& q, Emit emit, int first = 0
         if (hi > f.cellnum - 1) hi = f.cellnum - 1;
         if (lo > hi) continue;
         int b = f.cbeg[lo], e = f.cend[hi];
-        if (b < e) emit(b, e);
+        if (b < e) emit(b, e, false);
     }
 }
 
@@ -182,7 +193,7 @@ __device__ __forceinline__ Box morton_box(const MortonDev& m, int level, uint32_
 template <class Emit>
 __device__ __forceinline__ void morton_emit(const MortonDev& m, int level, uint32_t id, Emit emit) {
     const uint32_t span = 1u << (2 * (m.total_level - level));
-    emit(__ldg(m.cbeg + id * span), __ldg(m.cbeg + id * span + span));
+    emit(__ldg(m.cbeg + id * span), __ldg(m.cbeg + id * span + span), false);
 }
 
 /* MortonGrid::findMatchNodeInQuadTree (MortonGrid.cpp:356-393): leaves are taken without a
@@ -237,25 +248,31 @@ __device__ int64_t walk_ranges(const GridDev& g, const StigDev& s, const FsgDev&
      * index's point order) are joined, and everything is cut into chunks of at most kChunk
      * points ending on multiples of 4, so the warps of the scan get balanced, 16-byte-aligned
      * pieces. Chunking only regroups the same points. */
+    /* Ranges whose every point is a hit (points_inside) are joined only with each other and
+     * flagged in bit 31 of the item's start (kAllHit); their chunks are longer, since the scan
+     * reads only their ids. */
     int cur_b = -1, cur_e = -1;
+    bool cur_all = false;
     auto flush = [&]() {
+        const int chunk = cur_all ? kChunkAllHit : kChunk;
         while (cur_b < cur_e) {
             int e = cur_e;
-            if (e - cur_b > kChunk) e = (cur_b + kChunk) & ~3;
-            sink(cnt, make_int2(cur_b, e));
+            if (e - cur_b > chunk) e = (cur_b + chunk) & ~3;
+            sink(cnt, make_int2(cur_b | (cur_all ? kAllHit : 0), e));
             cnt++;
             cur_b = e;
         }
     };
-    auto emit = [&](int b, int e) {
+    auto emit = [&](int b, int e, bool all) {
         if (b >= e) return;
-        if (b == cur_e) {
+        if (b == cur_e && all == cur_all) {
             cur_e = e;
             return;
         }
         flush();
         cur_b = b;
         cur_e = e;
+        cur_all = all;
     };
     bool ok = true;
     if (KIND == GAT_INDEX_GRID) {
@@ -264,7 +281,8 @@ __device__ int64_t walk_ranges(const GridDev& g, const StigDev& s, const FsgDev&
         for (int lev = 0; lev < GD && walk; lev++) {
             const int ch = g.node_child[nd];
             if (ch < 0) {
-                if ((sub & ((1 << (2 * (GD - lev))) - 1)) == 0) emit(g.node_pbeg[nd], g.node_pend[nd]);
+                if ((sub & ((1 << (2 * (GD - lev))) - 1)) == 0)
+                    emit(g.node_pbeg[nd], g.node_pend[nd], points_inside(q, g.node_pbox, nd));
                 walk = false;
                 break;
             }
@@ -282,7 +300,7 @@ __device__ int64_t walk_ranges(const GridDev& g, const StigDev& s, const FsgDev&
             if (s.kind[nd]) {
                 if ((sub & ((1 << (SD - lev)) - 1)) == 0) {
                     const float4 m = s.mbb[nd];
-                    if (box_intersect(Box{m.x, m.y, m.z, m.w}, q)) emit(s.lo[nd], s.hi[nd] + 1);
+                    if (box_intersect(Box{m.x, m.y, m.z, m.w}, q)) emit(s.lo[nd], s.hi[nd] + 1, points_inside(q, s.pbox, nd));
                 }
                 walk = false;
                 break;
@@ -489,7 +507,8 @@ __global__ void __launch_bounds__(kThreads) k_plain_scan(const gat_mbb* queries,
     unsigned long long cand = 0, hits = 0;
     auto mark = [&](int t) { atomicOr(bitmap + (t >> 5), 1u << (t & 31)); };
     for (int64_t it = gw; it < nitems; it += nw) {
-        const int2 r = items[it];
+        int2 r = items[it];
+        r.x &= ~kAllHit; /* every point is tested here, all-hit items included */
         if (lane == 0) cand += (unsigned long long)(r.y - r.x);
         const int head_end = min(r.y, (r.x + 3) & ~3);
         const int vb = head_end, ve = head_end + ((r.y - head_end) & ~3);
@@ -681,6 +700,7 @@ __global__ void __launch_bounds__(kThreads) k_range_ids(const gat_mbb* queries, 
         const int64_t ib = (int64_t)(ioff_by_pos ? j : qi) * kSub;
         for (int64_t it = ioff[ib]; it < ioff[ib + kSub]; it++) {
             int2 r = items[it];
+            r.x &= ~kAllHit; /* every point is tested here, all-hit items included */
             cand += (unsigned long long)(r.y - r.x);
             scan_range(X, Y, r.x, r.y, q, [&](int i) {
                 int t = __ldg(tid + i);
@@ -919,7 +939,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
         if (qi >= nq) break;
         const Box q = load_box(queries, qi);
         const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
-        unsigned long long cand = 0, hits = 0;
+        unsigned long long cand = 0, hits = 0, allp = 0;
         for (;;) {
             int k = 0;
             if (lane == 0) k = atomicAdd(&item_sh, 1);
@@ -927,10 +947,38 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
             const int64_t it = i0 + k;
             /* stop once every item is taken or the set has overflowed (warp-uniform reads) */
             if (it >= i1 || __shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
-            const int2 r = items[it];
-            if (lane == 0) cand += (unsigned long long)(r.y - r.x);
+            int2 r = items[it];
+            const bool all = r.x < 0;
+            r.x &= ~kAllHit;
             const int head_end = min(r.y, (r.x + 3) & ~3);
             const int vb = head_end, ve = head_end + ((r.y - head_end) & ~3);
+            if (all) {
+                /* every point of the item is a hit: only the ids are read, and the first id of
+                 * each run of equal ids is inserted (head and tail points always) */
+                if (lane == 0) allp += (unsigned long long)(r.y - r.x);
+                for (int i = r.x + lane; i < head_end; i += 32) hs_insert<HB>(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
+                for (int i = ve + lane; i < r.y; i += 32) hs_insert<HB>(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
+                const int4* T4 = reinterpret_cast<const int4*>(tid + vb);
+                const int nv = (ve - vb) >> 2;
+                int carry = -1;
+                int4 nt = make_int4(-1, -1, -1, -1);
+                if (lane < nv) nt = __ldg(T4 + lane);
+                for (int k0 = 0; k0 < nv; k0 += 32) {
+                    const int kk = k0 + lane;
+                    int4 tt = nt;
+                    if (kk + 32 < nv) nt = __ldg(T4 + kk + 32);
+                    if (kk >= nv) tt = make_int4(-1, -1, -1, -1);
+                    int prev = __shfl_up_sync(FULL, tt.w, 1);
+                    if (lane == 0) prev = carry;
+                    carry = __shfl_sync(FULL, tt.w, 31);
+                    if (tt.x >= 0 && tt.x != prev) hs_insert<HB>(tab, buf, tt.x, &cnt_sh, &ovf_sh);
+                    if (tt.y >= 0 && tt.y != tt.x) hs_insert<HB>(tab, buf, tt.y, &cnt_sh, &ovf_sh);
+                    if (tt.z >= 0 && tt.z != tt.y) hs_insert<HB>(tab, buf, tt.z, &cnt_sh, &ovf_sh);
+                    if (tt.w >= 0 && tt.w != tt.z) hs_insert<HB>(tab, buf, tt.w, &cnt_sh, &ovf_sh);
+                }
+                continue;
+            }
+            if (lane == 0) cand += (unsigned long long)(r.y - r.x);
             /* unaligned head and tail points: plain inserts */
             for (int i = r.x + lane; i < head_end; i += 32)
                 if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
@@ -947,31 +995,34 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
             const int4* T4 = reinterpret_cast<const int4*>(tid + vb);
             const int nv = (ve - vb) >> 2;
             int carry = -1; /* tid of the last point of the previous step if it was a hit */
-            /* the next step's x / y are loaded before the current step is tested */
+            /* one step tests 4 points per lane; the next step's x, y and ids are loaded before the
+             * current step is tested (the ids unconditionally: most candidates are hits, and a
+             * load issued only after the test put the whole L2 latency on every step) */
             float4 nx = make_float4(0.f, 0.f, 0.f, 0.f), ny = nx;
+            int4 nt = make_int4(-1, -1, -1, -1);
             if (lane < nv) {
                 nx = __ldg(X4 + lane);
                 ny = __ldg(Y4 + lane);
+                nt = __ldg(T4 + lane);
             }
             for (int k0 = 0; k0 < nv; k0 += 32) {
                 const int kk = k0 + lane;
                 const float4 x = nx, y = ny;
+                const int4 tt = nt;
                 if (kk + 32 < nv) {
                     nx = __ldg(X4 + kk + 32);
                     ny = __ldg(Y4 + kk + 32);
+                    nt = __ldg(T4 + kk + 32);
                 }
                 int t0 = -1, t1 = -1, t2 = -1, t3 = -1;
                 if (kk < nv) {
                     const bool h0 = in_box(q, x.x, y.x), h1 = in_box(q, x.y, y.y);
                     const bool h2 = in_box(q, x.z, y.z), h3 = in_box(q, x.w, y.w);
-                    if (h0 | h1 | h2 | h3) {
-                        const int4 tt = __ldg(T4 + kk);
-                        t0 = h0 ? tt.x : -1;
-                        t1 = h1 ? tt.y : -1;
-                        t2 = h2 ? tt.z : -1;
-                        t3 = h3 ? tt.w : -1;
-                        hits += (unsigned long long)(h0 + h1 + h2 + h3);
-                    }
+                    t0 = h0 ? tt.x : -1;
+                    t1 = h1 ? tt.y : -1;
+                    t2 = h2 ? tt.z : -1;
+                    t3 = h3 ? tt.w : -1;
+                    hits += (unsigned long long)(h0 + h1 + h2 + h3);
                 }
                 int prev = __shfl_up_sync(FULL, t3, 1);
                 if (lane == 0) prev = carry;
@@ -982,7 +1033,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
                 if (t3 >= 0 && t3 != t2) hs_insert<HB>(tab, buf, t3, &cnt_sh, &ovf_sh);
             }
         }
-        my_work += 8ull * cand + 4ull * hits;
+        /* algorithmic bytes: x and y of every tested point, the id of every hit, the id of every
+         * point of an all-hit item */
+        my_work += 8ull * cand + 4ull * hits + 4ull * allp;
         __syncthreads(); /* every insert is done */
         const int m = cnt_sh;
         const bool overflow = ovf_sh != 0;
@@ -1080,6 +1133,7 @@ __global__ void __launch_bounds__(kThreads) k_range_points(const gat_mbb* querie
         int c = 0;
         for (int64_t it = ioff[(int64_t)qi * kSub]; it < ioff[(int64_t)(qi + 1) * kSub]; it++) {
             int2 r = items[it];
+            r.x &= ~kAllHit; /* every point is tested here, all-hit items included */
             scan_range(X, Y, r.x, r.y, q, [&](int) { c++; });
         }
         int total;
@@ -1101,6 +1155,7 @@ __global__ void __launch_bounds__(kThreads) k_range_points(const gat_mbb* querie
         int written = 0;
         for (int64_t it = ioff[(int64_t)qi * kSub]; it < ioff[(int64_t)(qi + 1) * kSub]; it++) {
             int2 r = items[it];
+            r.x &= ~kAllHit;
             for (int t0 = r.x; t0 < r.y; t0 += kThreads) {
                 int i = t0 + threadIdx.x;
                 bool h = i < r.y && in_box(q, __ldg(X + i), __ldg(Y + i));

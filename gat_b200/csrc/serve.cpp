@@ -382,6 +382,7 @@ int gat_server_create(gat_ctx* ctx, const gat_index* grid, const gat_index* stig
             } else {
                 const int pct = ctx->serve_reserve > 0 ? ctx->serve_reserve : 12;
                 w->sm_reserve = std::max(1, w->sm_count * pct / 100);
+                w->edr_reserve_pct = pct;
                 if (w->device >= 0) {
                     if (!s->chain.ev && cudaEventCreateWithFlags(&s->chain.ev, cudaEventDisableTiming) != cudaSuccess) {
                         cudaGetLastError();

@@ -205,6 +205,9 @@ int gat_index_load(gat_ctx* ctx, const gat_db* db, const char* path, gat_index**
     ix->grid = in.val<GridDev>();
     ix->stig = in.val<StigDev>();
     ix->fsg = in.val<FsgDev>();
+    /* derived arrays are recomputed below, never read from the file */
+    ix->grid.node_pbox = nullptr;
+    ix->stig.pbox = nullptr;
     std::vector<void**> fl = fields(ix);
     if (in.val<uint32_t>() != fl.size() || !in.ok) {
         delete ix;
@@ -254,6 +257,10 @@ int gat_index_load(gat_ctx* ctx, const gat_db* db, const char* path, gat_index**
                 return cuda_fail(ctx, e, "gat_index_load");
             }
             *fl[i] = p;
+        }
+        if (int st = index_point_boxes(ix)) {
+            gat_index_destroy(ix);
+            return st;
         }
     }
     *out = ix;

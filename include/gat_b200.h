@@ -128,10 +128,12 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  *   = autotune: the first batch of each (index kind, batch size rounded up to a power of two)
  *   class times both shapes on its own queries and keeps the faster; 1 = 256 threads per CTA
  *   with an 8192-slot id set, 2 = 128 threads with a 4096-slot set. Same results. Setting the
- *   knob clears the tuned table. */
+ *   knob clears the tuned table.
+ * GAT_TUNE_EDR_RESERVE: percent of the SMs (0..90) that this context's persistent EDR grid
+ *   leaves to other streams (0, the default, takes them all). Same results. */
 enum { GAT_TUNE_EDR_ROWS = 1, GAT_TUNE_EDR_TUNED = 2, GAT_TUNE_TOPK_CHUNK = 3, GAT_TUNE_TOPK_GROWTH = 4,
        GAT_TUNE_EDR_FORM = 5, GAT_TUNE_INDEX_BUILD = 6, GAT_TUNE_DEP_LAUNCH = 7, GAT_TUNE_TEST_STALL_CARRY = 8,
-       GAT_TUNE_SERVE_RESERVE = 9, GAT_TUNE_RANGE_SHAPE = 10 };
+       GAT_TUNE_SERVE_RESERVE = 9, GAT_TUNE_RANGE_SHAPE = 10, GAT_TUNE_EDR_RESERVE = 11 };
 int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value);
 int gat_ctx_get_tuning(gat_ctx* ctx, int knob, int* value);
 
