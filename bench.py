@@ -31,6 +31,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 OPS_PER_CELL = 12  # int32 / fp32 instructions per DP cell of the EDR recurrence (match test, three-way min, carries)
+# ALU-pipe instructions per DP cell of k_edr_tiles (8 rows per lane, row tiles) from an ncu capture of the
+# C4 launch: ALU pipe 76.7% busy over the active cycles at 64 lanes per clock per SM, 2.257 G cells
+ALU_PER_CELL = 10.2
 
 
 def log(*a):
@@ -464,9 +467,13 @@ def edr_roofline(st, clk):
     ach = per_cells / per_s / 1e9
     mhz = clk.get("sm_mhz") or 1965.0
     peak = 148 * 128 * mhz * 1e6 / OPS_PER_CELL / 1e9
+    alu = 148 * 64 * mhz * 1e6 / ALU_PER_CELL / 1e9
     return {"kernel": "k_edr", "bound": "alu", "achieved": round(ach, 2), "peak": round(peak, 1), "unit": "Gcell/s",
             "frac": round(ach / peak, 4), "traffic": None, "work_per_launch": per_cells,
-            "note": f"peak = 148 SM x 128 int32 lanes x sampled SM clock / {OPS_PER_CELL} ops per cell (nominal issue rate)"}
+            "note": f"peak = 148 SM x 128 int32 lanes x sampled SM clock / {OPS_PER_CELL} ops per cell (nominal issue rate)",
+            "alu_pipe": {"peak": round(alu, 1), "frac": round(ach / alu, 4), "alu_instructions_per_cell": ALU_PER_CELL,
+                         "note": "148 SM x 64 ALU-pipe lanes per clock x sampled SM clock / the kernel's measured ALU "
+                                 "instructions per cell (ncu, C4 launch, 8 rows per lane)"}}
 
 
 def base_line(args, world, metric, unit, value, ms_total, config, dtype="fp32-compare/int32"):
@@ -619,6 +626,8 @@ def run_c3(args, world, rank, local, td):
     t, q = D.config3(seed=0, n=args.c3_n, nq=C3["nq"])
     log("c3 data", t.n, len(t.lon), round(time.time() - t0, 1))
     ctx = G.Context(local)
+    if args.range_shape:
+        ctx.set_tuning(L.GAT_TUNE_RANGE_SHAPE, args.range_shape)
     db = G.TrajectorySet(ctx, t)
     idx = {}
     t0 = time.time()
@@ -1633,6 +1642,8 @@ def main():
     ap.add_argument("--c3-indexes", default="grid,fsg,stig")
     ap.add_argument("--c3-n", type=int, default=C3["n"])
     ap.add_argument("--c3-plain-sample", type=int, default=2000)
+    ap.add_argument("--range-shape", type=int, default=0,
+                    help="c3: block shape of the batched range scan (0 = autotuned, 1 = 256 threads, 2 = 128 threads)")
     ap.add_argument("--c5-requests", type=int, default=0, help="C5 requests per load (default 4000; 2000 in the suite)")
     ap.add_argument("--c4k-queries", type=int, default=C4K["nq"])
     ap.add_argument("--c4k-check", type=int, default=C4K["check"])
