@@ -879,6 +879,22 @@ __device__ __forceinline__ void hs_erase(int* tab, int t) {
     }
 }
 
+/* Inserts those of a lane's 4 ids that start a run (differ from the previous point's id; -1 =
+ * not a hit). Most steps start no run (a trajectory's points in a cell are consecutive), so the
+ * warp tests once whether any lane has one instead of branching on each of the four. Called by
+ * all lanes of the warp. */
+template <int HB>
+__device__ __forceinline__ void insert_runs(int* tab, int* list, int prev, int t0, int t1, int t2, int t3, int* count,
+                                            int* ovf) {
+    const bool n0 = t0 >= 0 && t0 != prev, n1 = t1 >= 0 && t1 != t0;
+    const bool n2 = t2 >= 0 && t2 != t1, n3 = t3 >= 0 && t3 != t2;
+    if (!__any_sync(0xffffffffu, n0 | n1 | n2 | n3)) return;
+    if (n0) hs_insert<HB>(tab, list, t0, count, ovf);
+    if (n1) hs_insert<HB>(tab, list, t1, count, ovf);
+    if (n2) hs_insert<HB>(tab, list, t2, count, ovf);
+    if (n3) hs_insert<HB>(tab, list, t3, count, ovf);
+}
+
 /* ascending sort of the 32 values of a warp (one per lane), bitonic network over shuffles */
 __device__ __forceinline__ int warp_sort32(int v) {
     const int lane = threadIdx.x & 31;
@@ -971,10 +987,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
                     int prev = __shfl_up_sync(FULL, tt.w, 1);
                     if (lane == 0) prev = carry;
                     carry = __shfl_sync(FULL, tt.w, 31);
-                    if (tt.x >= 0 && tt.x != prev) hs_insert<HB>(tab, buf, tt.x, &cnt_sh, &ovf_sh);
-                    if (tt.y >= 0 && tt.y != tt.x) hs_insert<HB>(tab, buf, tt.y, &cnt_sh, &ovf_sh);
-                    if (tt.z >= 0 && tt.z != tt.y) hs_insert<HB>(tab, buf, tt.z, &cnt_sh, &ovf_sh);
-                    if (tt.w >= 0 && tt.w != tt.z) hs_insert<HB>(tab, buf, tt.w, &cnt_sh, &ovf_sh);
+                    insert_runs<HB>(tab, buf, prev, tt.x, tt.y, tt.z, tt.w, &cnt_sh, &ovf_sh);
                 }
                 continue;
             }
@@ -1027,10 +1040,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
                 int prev = __shfl_up_sync(FULL, t3, 1);
                 if (lane == 0) prev = carry;
                 carry = __shfl_sync(FULL, t3, 31);
-                if (t0 >= 0 && t0 != prev) hs_insert<HB>(tab, buf, t0, &cnt_sh, &ovf_sh);
-                if (t1 >= 0 && t1 != t0) hs_insert<HB>(tab, buf, t1, &cnt_sh, &ovf_sh);
-                if (t2 >= 0 && t2 != t1) hs_insert<HB>(tab, buf, t2, &cnt_sh, &ovf_sh);
-                if (t3 >= 0 && t3 != t2) hs_insert<HB>(tab, buf, t3, &cnt_sh, &ovf_sh);
+                insert_runs<HB>(tab, buf, prev, t0, t1, t2, t3, &cnt_sh, &ovf_sh);
             }
         }
         /* algorithmic bytes: x and y of every tested point, the id of every hit, the id of every
@@ -1482,22 +1492,27 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
             return cudaGetLastError();
         };
         if (ids && shape == 0) {
-            /* first batch of its class: time both shapes on it and keep the faster (the later run
-             * below overwrites every output) */
-            cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-            float ms[3] = {0.f, 0.f, 0.f};
+            /* first batch of its class: time both shapes on it twice, alternating (the first run
+             * meets cold caches), and keep the faster best time (the later run below overwrites
+             * every output) */
+            constexpr int kRuns = 4;
+            cudaEvent_t ev[kRuns + 1] = {};
+            float best[3] = {1e30f, 1e30f, 1e30f};
             bool ok = true;
             for (auto& e : ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
-            for (int sh = 1; sh <= 2 && ok; sh++)
-                ok = cudaEventRecord(ev[sh - 1], s) == cudaSuccess && hash_launch(sh, nullptr) == cudaSuccess &&
-                     cudaEventRecord(ev[sh], s) == cudaSuccess;
-            ok = ok && cudaEventSynchronize(ev[2]) == cudaSuccess &&
-                 cudaEventElapsedTime(&ms[1], ev[0], ev[1]) == cudaSuccess &&
-                 cudaEventElapsedTime(&ms[2], ev[1], ev[2]) == cudaSuccess;
+            ok = ok && cudaEventRecord(ev[0], s) == cudaSuccess;
+            for (int r = 0; r < kRuns && ok; r++)
+                ok = hash_launch(1 + (r & 1), nullptr) == cudaSuccess && cudaEventRecord(ev[r + 1], s) == cudaSuccess;
+            ok = ok && cudaEventSynchronize(ev[kRuns]) == cudaSuccess;
+            for (int r = 0; r < kRuns && ok; r++) {
+                float ms = 0.f;
+                ok = cudaEventElapsedTime(&ms, ev[r], ev[r + 1]) == cudaSuccess;
+                best[1 + (r & 1)] = std::min(best[1 + (r & 1)], ms);
+            }
             for (auto& e : ev)
                 if (e) cudaEventDestroy(e);
             if (!ok) return cuda_fail(ctx, cudaGetLastError(), "range shape tuning");
-            shape = ms[2] < ms[1] ? 2 : 1;
+            shape = best[2] < best[1] ? 2 : 1;
             std::lock_guard<std::mutex> lk(tab->tune_mu);
             tab->range_tune[tune_key] = shape;
         }
