@@ -1643,7 +1643,8 @@ def main():
     ap.add_argument("--c3-n", type=int, default=C3["n"])
     ap.add_argument("--c3-plain-sample", type=int, default=2000)
     ap.add_argument("--range-shape", type=int, default=0,
-                    help="c3: block shape of the batched range scan (0 = autotuned, 1 = 256 threads, 2 = 128 threads)")
+                    help="c3: block shape of the batched range scan (0 = autotuned, 1 = 256 threads, 2 = 128 threads, "
+                         "3 = split by query size)")
     ap.add_argument("--c5-requests", type=int, default=0, help="C5 requests per load (default 4000; 2000 in the suite)")
     ap.add_argument("--c4k-queries", type=int, default=C4K["nq"])
     ap.add_argument("--c4k-check", type=int, default=C4K["check"])

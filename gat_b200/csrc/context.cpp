@@ -382,7 +382,7 @@ int gat_ctx_set_tuning(gat_ctx* ctx, int knob, int value) {
         return GAT_OK;
     }
     if (knob == GAT_TUNE_RANGE_SHAPE) {
-        if (value < 0 || value > 2) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: range shape must be 0, 1 or 2");
+        if (value < 0 || value > 3) return fail(ctx, GAT_ERR_ARG, "gat_ctx_set_tuning: range shape must be 0..3");
         ctx->range_shape = value;
         std::lock_guard<std::mutex> tk(ctx->tune_mu);
         ctx->range_tune.clear();

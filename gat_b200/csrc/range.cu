@@ -820,6 +820,23 @@ __global__ void k_order_scatter(int nq, const int* __restrict__ bucket, unsigned
     order[atomicAdd(&base[bucket[qi]], 1ull)] = qi;
 }
 
+/* Split of a batch by size: the queries of `order` (or 0..nq-1) with at most `cut` candidate items
+ * first, the others after, each part in its order (a stable partition by a scan of the flags) */
+__global__ void k_small_flags(int nq, const int* __restrict__ order, const int64_t* __restrict__ ioff, int cut,
+                              int64_t* flags) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nq) return;
+    const int q = order ? order[j] : j;
+    flags[j] = ioff[(int64_t)(q + 1) * kSub] - ioff[(int64_t)q * kSub] <= cut ? 1 : 0;
+}
+__global__ void k_split_scatter(int nq, const int* __restrict__ order, const int64_t* __restrict__ flags,
+                                const int64_t* __restrict__ pos, int* out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nq) return;
+    const int q = order ? order[j] : j;
+    out[flags[j] ? pos[j] : pos[nq] + (j - pos[j])] = q;
+}
+
 /* ---------------------------------------------------------------- id sets, hash form */
 /* Queries are taken from a counter by persistent CTAs (the next query's index is fetched while
  * the current one finishes). The CTA's warps take the query's candidate items from a
@@ -838,6 +855,7 @@ __global__ void k_order_scatter(int nq, const int* __restrict__ bucket, unsigned
 /* A set of 2^HB slots holds up to 2^(HB-1) ids (load factor <= 1/2): 48 KB of shared memory per
  * CTA for HB = 13 (256 threads), 24 KB for HB = 12 (128 threads). */
 constexpr int kRankSortMax = 512; /* lists up to this length are sorted by run ranks */
+constexpr int kSmallItems = 16;   /* shape 3: queries with at most this many items go to 128-thread blocks */
 
 template <int HB>
 __device__ __forceinline__ unsigned hs_slot(int t) { return ((unsigned)t * 2654435761u) >> (32 - HB); }
@@ -938,9 +956,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
     const unsigned FULL = 0xffffffffu;
     for (int i = threadIdx.x; i < kHashSize; i += blockDim.x) tab[i] = -1;
     /* ctr: [0] arena cursor, [1] work bytes, [2] query counter, [3] overflow count */
+    /* the next query of the list order[0..nq) (or 0..nq-1), -1 past its end */
     auto fetch = [&]() {
         const int j = (int)atomicAdd(&ctr[2], 1ull);
-        return j >= nq ? nq : (order ? order[j] : j);
+        return j >= nq ? -1 : (order ? order[j] : j);
     };
     if (threadIdx.x == 0) {
         next_sh = fetch();
@@ -952,7 +971,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
     for (;;) {
         __syncthreads(); /* the set and list are clear, the next query is known */
         const int qi = next_sh;
-        if (qi >= nq) break;
+        if (qi < 0) break;
         const Box q = load_box(queries, qi);
         const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
         unsigned long long cand = 0, hits = 0, allp = 0;
@@ -1444,8 +1463,29 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
     if ((st = build_items(ctx, ix, d_q, nq, nullptr, &ioff, &items)) != GAT_OK) return st;
     if ((st = check_device_flag(ctx, "range candidates")) != GAT_OK) return st;
     /* the hash kernel's two shapes (256 threads / 8192 slots, 128 threads / 4096 slots) */
-    int hgrid[3] = {0, 0, 0};
+    int hgrid[3] = {0, 0, 0}, hper[3] = {0, 0, 0};
     size_t hsmem[3] = {0, (size_t)(8192 + 4096) * sizeof(int), (size_t)(4096 + 2048) * sizeof(int)};
+    /* shape 3: the batch split by size, queries with more than kSmallItems candidate items on the
+     * 256-thread shape and the others on the 128-thread one (split[0..ns) small, [ns, nq) large) */
+    int* split = nullptr;
+    int ns = -1;
+    auto make_split = [&]() -> int {
+        if (ns >= 0) return GAT_OK;
+        int st2 = GAT_OK;
+        int64_t* fl = (int64_t*)scratch(ctx, S_RANGE_TPOS, (size_t)2 * (nq + 1) * sizeof(int64_t), &st2);
+        split = fl ? (int*)scratch(ctx, S_RANGE_TASK, (size_t)(nq + 1) * sizeof(int), &st2) : nullptr;
+        if (!split) return st2;
+        int64_t* pos = fl + (nq + 1);
+        k_small_flags<<<(nq + 255) / 256, 256, 0, s>>>(nq, order, ioff, kSmallItems, fl);
+        count_launch(ctx);
+        if ((st2 = scan_i64(ctx, fl, pos, nq)) != GAT_OK) return st2;
+        k_split_scatter<<<(nq + 255) / 256, 256, 0, s>>>(nq, order, fl, pos, split);
+        count_launch(ctx);
+        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned + 8, pos + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range");
+        ns = (int)ctx->h_pinned[8];
+        return GAT_OK;
+    };
     int shape = ctx->range_shape;
     uint64_t tune_key = 0;
     gat_ctx* tab = ctx->root ? ctx->root : ctx;
@@ -1458,6 +1498,8 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         hgrid[1] = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_hash<128, 12>, 128, hsmem[2]);
         hgrid[2] = std::max(1, std::min(nq, std::max(1, per_sm) * ctx->sm_count));
+        hper[1] = hgrid[1];
+        hper[2] = hgrid[2];
         if (shape == 0) {
             uint64_t lg = 0;
             while (lg < 40 && ((int64_t)1 << lg) < nq) lg++;
@@ -1479,40 +1521,83 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         if (!arena) return st;
         cap = (int64_t)(ctx->slot_bytes[S_RANGE_ARENA] / 4);
         /* cursor: [0] arena entries, [1] work bytes, [2] query counter, [3] overflowed queries */
+        /* one shape over the query list lst[0..n) (lst null: 0..n-1) */
+        auto hash_run = [&](int sh, const int* lst, int n, unsigned long long* work) {
+            if (n <= 0) return;
+            if (sh == 2)
+                k_range_hash<128, 12><<<std::min(n, hper[2]), 128, hsmem[2], s>>>(
+                    d_q, n, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap, cursor, segbase, segcnt, ovf_list, work, lst);
+            else
+                k_range_hash<256, 13><<<std::min(n, hper[1]), 256, hsmem[1], s>>>(
+                    d_q, n, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap, cursor, segbase, segcnt, ovf_list, work, lst);
+            count_launch(ctx);
+        };
         auto hash_launch = [&](int sh, unsigned long long* work) {
             cudaError_t e = cudaMemsetAsync(cursor, 0, 4 * sizeof(unsigned long long), s);
             if (e != cudaSuccess) return e;
-            if (sh == 2)
-                k_range_hash<128, 12><<<hgrid[2], 128, hsmem[2], s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena,
-                                                                      cap, cursor, segbase, segcnt, ovf_list, work, order);
-            else
-                k_range_hash<256, 13><<<hgrid[1], 256, hsmem[1], s>>>(d_q, nq, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena,
-                                                                      cap, cursor, segbase, segcnt, ovf_list, work, order);
-            count_launch(ctx);
+            if (sh == 3) {
+                /* the large queries first, then (query counter reset) the small ones */
+                hash_run(1, split + ns, nq - ns, work);
+                if ((e = cudaMemsetAsync(cursor + 2, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
+                hash_run(2, split, ns, work);
+            } else {
+                hash_run(sh, order, nq, work);
+            }
             return cudaGetLastError();
         };
-        if (ids && shape == 0) {
-            /* first batch of its class: time both shapes on it twice, alternating (the first run
-             * meets cold caches), and keep the faster best time (the later run below overwrites
-             * every output) */
-            constexpr int kRuns = 4;
-            cudaEvent_t ev[kRuns + 1] = {};
-            float best[3] = {1e30f, 1e30f, 1e30f};
-            bool ok = true;
-            for (auto& e : ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
-            ok = ok && cudaEventRecord(ev[0], s) == cudaSuccess;
-            for (int r = 0; r < kRuns && ok; r++)
-                ok = hash_launch(1 + (r & 1), nullptr) == cudaSuccess && cudaEventRecord(ev[r + 1], s) == cudaSuccess;
-            ok = ok && cudaEventSynchronize(ev[kRuns]) == cudaSuccess;
-            for (int r = 0; r < kRuns && ok; r++) {
-                float ms = 0.f;
-                ok = cudaEventElapsedTime(&ms, ev[r], ev[r + 1]) == cudaSuccess;
-                best[1 + (r & 1)] = std::min(best[1 + (r & 1)], ms);
+        /* the queries the hash kernel handed on (more distinct ids than its set holds) in the
+         * bitmap form; leaves the cursor's [0] arena entries and [1] work bytes in h_pinned */
+        auto bitmap_pass = [&](unsigned long long* wk, bool timed) -> int {
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+            GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
+            const int64_t n_ovf = ctx->h_pinned[3];
+            if (n_ovf <= 0) return GAT_OK;
+            int per_sm = 0, st2 = GAT_OK;
+            if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_ids, kThreads, bm_in_smem ? smem_bm : 0);
+            const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>(n_ovf, (int64_t)std::max(1, per_sm) * ctx->sm_count));
+            uint32_t* gbm = nullptr;
+            if (!bm_in_smem) {
+                gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, (size_t)g2 * words * 4, &st2);
+                if (!gbm) return st2;
             }
-            for (auto& e : ev)
-                if (e) cudaEventDestroy(e);
+            if (timed) timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
+            k_range_ids<<<g2, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, (int)n_ovf, ioff, items, ix->d_x, ix->d_y,
+                                                                      ix->d_tid, words, gbm, arena, cap, cursor, segbase,
+                                                                      segcnt, wk, ovf_list, 0);
+            if (timed) timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
+            count_launch(ctx);
+            GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
+            GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
+            GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
+            return GAT_OK;
+        };
+        if (ids && (shape == 0 || shape == 3) && (st = make_split()) != GAT_OK) return st;
+        if (ids && shape == 0) {
+            /* first batch of its class: time the three shapes on it twice each, in rotation (the
+             * first runs meet cold caches), each with the bitmap pass for the queries its set
+             * hands on (the smaller set hands on more), and keep the best (the later run below
+             * overwrites every output) */
+            constexpr int kShapes = 3, kRuns = 2 * kShapes;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            float best[kShapes + 1] = {1e30f, 1e30f, 1e30f, 1e30f};
+            bool ok = cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+            for (int r = 0; r < kRuns && ok; r++) {
+                const int sh = 1 + r % kShapes;
+                ok = cudaEventRecord(e0, s) == cudaSuccess && hash_launch(sh, nullptr) == cudaSuccess;
+                if (ok && (st = bitmap_pass(nullptr, false)) != GAT_OK) break;
+                float ms = 0.f;
+                ok = ok && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+                     cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+                best[sh] = std::min(best[sh], ms);
+            }
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            if (st != GAT_OK) return st;
             if (!ok) return cuda_fail(ctx, cudaGetLastError(), "range shape tuning");
-            shape = best[2] < best[1] ? 2 : 1;
+            shape = 1;
+            for (int sh = 2; sh <= kShapes; sh++)
+                if (best[sh] < best[shape]) shape = sh;
             std::lock_guard<std::mutex> lk(tab->tune_mu);
             tab->range_tune[tune_key] = shape;
         }
@@ -1528,27 +1613,9 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         }
         timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
         GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
-        GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
-        GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
-        const int64_t n_ovf = ids ? ctx->h_pinned[3] : 0;
-        if (n_ovf > 0) {
-            /* queries with more distinct ids than the shared-memory set holds: bitmap form */
-            int per_sm = 0;
-            if (bm_in_smem) allow_smem(k_range_ids, smem_bm);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_range_ids, kThreads, bm_in_smem ? smem_bm : 0);
-            const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>(n_ovf, (int64_t)std::max(1, per_sm) * ctx->sm_count));
-            uint32_t* gbm = nullptr;
-            if (!bm_in_smem) {
-                gbm = (uint32_t*)scratch(ctx, S_RANGE_ARENA2, (size_t)g2 * words * 4, &st);
-                if (!gbm) return st;
-            }
-            timed_begin(ctx, GAT_KERNEL_RANGE_SCAN);
-            k_range_ids<<<g2, kThreads, bm_in_smem ? smem_bm : 0, s>>>(d_q, (int)n_ovf, ioff, items, ix->d_x, ix->d_y,
-                                                                      ix->d_tid, words, gbm, arena, cap, cursor, segbase,
-                                                                      segcnt, work, ovf_list, 0);
-            timed_end(ctx, GAT_KERNEL_RANGE_SCAN, 0.0);
-            count_launch(ctx);
-            GAT_CUDA_TRY(ctx, cudaGetLastError(), "range scan launch");
+        if (ids) {
+            if ((st = bitmap_pass(work, true)) != GAT_OK) return st;
+        } else {
             GAT_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_pinned, cursor, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s), "range");
             GAT_CUDA_TRY(ctx, cudaStreamSynchronize(s), "range scan");
         }

@@ -192,3 +192,24 @@ def test_morton_grid_rejects_other_kinds(gpu_ctx, c1):
     m = G.MortonGrid(g)
     with pytest.raises(G.GatError):
         m.save("/tmp/gat_morton_snapshot.bin")
+
+
+@pytest.mark.parametrize("shape", [1, 2, 3])
+def test_hash_shapes(gpu_ctx, c1, shape):
+    """Every block shape of the batched id-set scan (256 threads, 128 threads, the batch split by
+    query size) returns the oracle's sets, on the Grid and on STIG."""
+    from gat_b200 import _lib as L
+    t, q, db = c1
+    qq = np.concatenate([q] * 3)  # enough queries for the locality order
+    gpu_ctx.set_tuning(L.GAT_TUNE_RANGE_SHAPE, shape)
+    try:
+        g = G.Grid(gpu_ctx, db, D.BOX, 0.01, 2, 512)
+        off, ids = po.OracleGrid(t, D.BOX, 0.01, 2, 512).range(qq, 0)
+        r = g.range_query(qq, "ids")
+        assert csr_equal(r.offsets, r.tids, off, ids)
+        s = G.STIG(gpu_ctx, db, 512)
+        ref = po.OracleSTIG(t, 512).range(qq, 0)
+        r = s.range_query(qq, "ids")
+        assert csr_equal(r.offsets, r.tids, ref[0], ref[1])
+    finally:
+        gpu_ctx.set_tuning(L.GAT_TUNE_RANGE_SHAPE, 0)

@@ -125,13 +125,13 @@ def test_tuning_knob(host_ctx):
 
 def test_topk_walk_knobs(host_ctx):
     """GAT_TUNE_TOPK_CHUNK (0..2^24), GAT_TUNE_TOPK_GROWTH (0 or 2..64), the test knob
-    GAT_TUNE_TEST_STALL_CARRY (>= 0), GAT_TUNE_SERVE_RESERVE (0..90), GAT_TUNE_RANGE_SHAPE (0..2)
+    GAT_TUNE_TEST_STALL_CARRY (>= 0), GAT_TUNE_SERVE_RESERVE (0..90), GAT_TUNE_RANGE_SHAPE (0..3)
     and GAT_TUNE_EDR_RESERVE (0..90) round-trip; other values are refused."""
     for knob, good, bad in ((L.GAT_TUNE_TOPK_CHUNK, (512, 0), (-1, 1 << 25)),
                             (L.GAT_TUNE_TOPK_GROWTH, (2, 8, 0), (1, 65, -2)),
                             (L.GAT_TUNE_TEST_STALL_CARRY, (3, 0), (-1,)),
                             (L.GAT_TUNE_SERVE_RESERVE, (25, 90, 0), (-1, 91)),
-                            (L.GAT_TUNE_RANGE_SHAPE, (1, 2, 0), (-1, 3)),
+                            (L.GAT_TUNE_RANGE_SHAPE, (1, 2, 3, 0), (-1, 4)),
                             (L.GAT_TUNE_EDR_RESERVE, (50, 0), (-1, 91))):
         for v in good:
             host_ctx.set_tuning(knob, v)
