@@ -436,9 +436,9 @@ def hbm_peak():
 
 
 # DRAM read + write / algorithmic bytes of k_range_hash, from a one-pass ncu capture (dram__bytes_read.sum,
-# dram__bytes_write.sum) of the C3 batch on the 1M-walk set: Grid (5.850 + 0.088) GB / 41.46 GB, FSG
-# (4.650 + 0.030) GB / 41.29 GB. The locality order serves neighbouring queries' points from L2.
-RANGE_TRAFFIC_RATIO = {"grid": 0.143, "fsg": 0.113}
+# dram__bytes_write.sum) of the C3 batch on the 1M-walk set: Grid (3.258 + 0.087) GB / 20.79 GB, FSG
+# (5.333 + 0.088) GB / 41.29 GB. The locality order serves neighbouring queries' points from L2.
+RANGE_TRAFFIC_RATIO = {"grid": 0.161, "fsg": 0.131}
 
 
 def range_roofline(st, name, index="grid"):
@@ -452,7 +452,8 @@ def range_roofline(st, name, index="grid"):
     return {"kernel": name, "bound": "hbm", "achieved": round(ach, 1), "peak": gbs, "unit": "GB/s",
             "frac": round(ach / gbs, 4), "traffic": round(ratio * per_bytes) if ratio else None,
             "work_per_launch": per_bytes,
-            "note": f"algorithmic bytes: 8 B (x, y) per candidate point + 4 B per hit; peak of {src}; traffic = "
+            "note": f"algorithmic bytes: 8 B (x, y) per tested point + 4 B per hit + 4 B per point of an all-hit item; "
+                    f"peak of {src}; traffic = "
                     + (f"{ratio} x algorithmic, the dram read+write / algorithmic ratio of a one-pass ncu capture of "
                        f"this index's k_range_hash on the 1M-walk C3 batch" if ratio else "not captured for this index")
                     + "; DRAM traffic well below the algorithmic bytes means L2 serves most of them (locality order), "
