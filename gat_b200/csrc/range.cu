@@ -846,7 +846,7 @@ __global__ void k_split_scatter(int nq, const int* __restrict__ order, const int
  * open-addressing set in shared memory; a successful insert also appends the id to a list, so
  * the query's m distinct ids are known without scanning the set. The list is sorted (each warp
  * sorts runs of 32 ids in registers, then every id's rank is its position in its run plus its
- * lower bound in every other run; long lists use a block-wide bitonic sort) and written to the
+ * lower bound in every other run; long lists merge the sorted runs pairwise) and written to the
  * arena at the rank; the set is cleared by probing each listed id again. A query whose distinct
  * ids exceed half the set's slots goes on the overflow list for the bitmap kernel; the result is
  * the same set either way. Two shapes: 256 threads with a 8192-slot set, or 128 threads with a
@@ -1105,28 +1105,52 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
                 hs_erase<HB>(tab, x);
             }
         } else {
-            /* long lists: clear the set, then a block-wide bitonic sort padded to a power of two */
+            /* long lists: the set is cleared, runs of 32 are sorted by the warps, then merged in
+             * pairs: an id's place in the merged run is its place in its own run plus the number
+             * of ids below it in the partner run (a binary search; the ids are distinct), ping-
+             * ponging between the list and the set's first slots, which are cleared again at the
+             * end. log2(m / 32) rounds, one barrier each. */
             for (int i = threadIdx.x; i < m; i += blockDim.x) hs_erase<HB>(tab, buf[i]);
-            int P = 1;
-            while (P < m) P <<= 1;
-            for (int i = m + threadIdx.x; i < P; i += blockDim.x) buf[i] = INT_MAX;
+            const int runs = (m + 31) >> 5;
+            for (int c = warp; c < runs; c += NT / 32) {
+                const int i = 32 * c + lane;
+                const int v = warp_sort32(i < m ? buf[i] : INT_MAX);
+                __syncwarp();
+                if (i < m) buf[i] = v;
+            }
             __syncthreads();
-            for (int kk = 2; kk <= P; kk <<= 1)
-                for (int jj = kk >> 1; jj > 0; jj >>= 1) {
-                    for (int i = threadIdx.x; i < P; i += blockDim.x) {
-                        const int ixj = i ^ jj;
-                        if (ixj > i) {
-                            const int a = buf[i], b = buf[ixj];
-                            if ((a > b) == ((i & kk) == 0)) {
-                                buf[i] = b;
-                                buf[ixj] = a;
-                            }
+            int* src = buf;
+            int* dst = tab;
+            for (int L = 32; L < m; L <<= 1) {
+                for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                    const int x = src[i];
+                    const int start = i & ~(2 * L - 1);
+                    const int mid = min(start + L, m), end = min(start + 2 * L, m);
+                    const bool in_a = i < mid;
+                    int lo = in_a ? mid : start;
+                    int len = in_a ? end - mid : mid - start;
+                    const int first = lo;
+                    while (len > 0) {
+                        const int half = len >> 1;
+                        if (src[lo + half] < x) {
+                            lo += half + 1;
+                            len -= half + 1;
+                        } else {
+                            len = half;
                         }
                     }
-                    __syncthreads();
+                    dst[start + (i - (in_a ? start : mid)) + (lo - first)] = x;
                 }
-            if (write)
-                for (int i = threadIdx.x; i < m; i += blockDim.x) arena[base + i] = (uint32_t)buf[i];
+                __syncthreads();
+                int* t = src;
+                src = dst;
+                dst = t;
+            }
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                const int v = src[i];
+                if (write) arena[base + i] = (uint32_t)v;
+                tab[i] = -1; /* the same thread read slot i above when the result is in the set */
+            }
         }
         if (threadIdx.x == 0) {
             cnt_sh = 0;
