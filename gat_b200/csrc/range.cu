@@ -855,7 +855,7 @@ __global__ void k_split_scatter(int nq, const int* __restrict__ order, const int
 /* A set of 2^HB slots holds up to 2^(HB-1) ids (load factor <= 1/2): 48 KB of shared memory per
  * CTA for HB = 13 (256 threads), 24 KB for HB = 12 (128 threads). */
 constexpr int kRankSortMax = 512; /* lists up to this length are sorted by run ranks */
-constexpr int kSmallItems = 16;   /* shape 3: queries with at most this many items go to 128-thread blocks */
+constexpr int kSmallItems = 8;    /* shape 3: queries with at most this many items are scanned one per warp */
 
 template <int HB>
 __device__ __forceinline__ unsigned hs_slot(int t) { return ((unsigned)t * 2654435761u) >> (32 - HB); }
@@ -938,13 +938,104 @@ __device__ __forceinline__ int lower_bound32(const int* run, int x) {
     return lo + (run[31] < x ? 1 : 0);
 }
 
+/* One candidate item scanned by one warp: the ids of its points in q that start a run of equal
+ * ids go into the set `tab` (appended to `list`; count / ovf as hs_insert). An all-hit item
+ * (bit 31 of its start) has every point in q, so only its ids are read. cand / hits / allp add
+ * the item's tested points, hits and all-hit points (lane 0 counts the item sizes). */
+template <int HB>
+__device__ __forceinline__ void scan_item(int2 r, const Box& q, const float* __restrict__ X, const float* __restrict__ Y,
+                                          const int32_t* __restrict__ tid, int* tab, int* list, int* count, int* ovf,
+                                          unsigned long long& cand, unsigned long long& hits, unsigned long long& allp) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool all = r.x < 0;
+    r.x &= ~kAllHit;
+    const int head_end = min(r.y, (r.x + 3) & ~3);
+    const int vb = head_end, ve = head_end + ((r.y - head_end) & ~3);
+    if (all) {
+        /* every point of the item is a hit: only the ids are read, and the first id of
+         * each run of equal ids is inserted (head and tail points always) */
+        if (lane == 0) allp += (unsigned long long)(r.y - r.x);
+        for (int i = r.x + lane; i < head_end; i += 32) hs_insert<HB>(tab, list, __ldg(tid + i), count, ovf);
+        for (int i = ve + lane; i < r.y; i += 32) hs_insert<HB>(tab, list, __ldg(tid + i), count, ovf);
+        const int4* T4 = reinterpret_cast<const int4*>(tid + vb);
+        const int nv = (ve - vb) >> 2;
+        int carry = -1;
+        int4 nt = make_int4(-1, -1, -1, -1);
+        if (lane < nv) nt = __ldg(T4 + lane);
+        for (int k0 = 0; k0 < nv; k0 += 32) {
+            const int kk = k0 + lane;
+            int4 tt = nt;
+            if (kk + 32 < nv) nt = __ldg(T4 + kk + 32);
+            if (kk >= nv) tt = make_int4(-1, -1, -1, -1);
+            int prev = __shfl_up_sync(FULL, tt.w, 1);
+            if (lane == 0) prev = carry;
+            carry = __shfl_sync(FULL, tt.w, 31);
+            insert_runs<HB>(tab, list, prev, tt.x, tt.y, tt.z, tt.w, count, ovf);
+        }
+        return;
+    }
+    if (lane == 0) cand += (unsigned long long)(r.y - r.x);
+    /* unaligned head and tail points: plain inserts */
+    for (int i = r.x + lane; i < head_end; i += 32)
+        if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
+            hs_insert<HB>(tab, list, __ldg(tid + i), count, ovf);
+            hits++;
+        }
+    for (int i = ve + lane; i < r.y; i += 32)
+        if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
+            hs_insert<HB>(tab, list, __ldg(tid + i), count, ovf);
+            hits++;
+        }
+    const float4* X4 = reinterpret_cast<const float4*>(X + vb);
+    const float4* Y4 = reinterpret_cast<const float4*>(Y + vb);
+    const int4* T4 = reinterpret_cast<const int4*>(tid + vb);
+    const int nv = (ve - vb) >> 2;
+    int carry = -1; /* tid of the last point of the previous step if it was a hit */
+    /* one step tests 4 points per lane; the next step's x, y and ids are loaded before the
+     * current step is tested (the ids unconditionally: most candidates are hits, and a
+     * load issued only after the test put the whole L2 latency on every step) */
+    float4 nx = make_float4(0.f, 0.f, 0.f, 0.f), ny = nx;
+    int4 nt = make_int4(-1, -1, -1, -1);
+    if (lane < nv) {
+        nx = __ldg(X4 + lane);
+        ny = __ldg(Y4 + lane);
+        nt = __ldg(T4 + lane);
+    }
+    for (int k0 = 0; k0 < nv; k0 += 32) {
+        const int kk = k0 + lane;
+        const float4 x = nx, y = ny;
+        const int4 tt = nt;
+        if (kk + 32 < nv) {
+            nx = __ldg(X4 + kk + 32);
+            ny = __ldg(Y4 + kk + 32);
+            nt = __ldg(T4 + kk + 32);
+        }
+        int t0 = -1, t1 = -1, t2 = -1, t3 = -1;
+        if (kk < nv) {
+            const bool h0 = in_box(q, x.x, y.x), h1 = in_box(q, x.y, y.y);
+            const bool h2 = in_box(q, x.z, y.z), h3 = in_box(q, x.w, y.w);
+            t0 = h0 ? tt.x : -1;
+            t1 = h1 ? tt.y : -1;
+            t2 = h2 ? tt.z : -1;
+            t3 = h3 ? tt.w : -1;
+            hits += (unsigned long long)(h0 + h1 + h2 + h3);
+        }
+        int prev = __shfl_up_sync(FULL, t3, 1);
+        if (lane == 0) prev = carry;
+        carry = __shfl_sync(FULL, t3, 31);
+        insert_runs<HB>(tab, list, prev, t0, t1, t2, t3, count, ovf);
+    }
+}
+
 template <int NT, int HB>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* queries, int nq, const int64_t* ioff,
                                                            const int2* items, const float* __restrict__ X,
                                                            const float* __restrict__ Y, const int32_t* __restrict__ tid,
                                                            uint32_t* arena, int64_t cap, unsigned long long* ctr,
                                                            int64_t* segbase, int64_t* segcnt, int* ovf_list,
-                                                           unsigned long long* work, const int* __restrict__ order) {
+                                                           unsigned long long* work, const int* __restrict__ order,
+                                                           const int* __restrict__ small, int ns) {
     constexpr int kHashSize = 1 << HB;
     dep_wait();
     extern __shared__ int hs_smem[];
@@ -955,7 +1046,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     for (int i = threadIdx.x; i < kHashSize; i += blockDim.x) tab[i] = -1;
-    /* ctr: [0] arena cursor, [1] work bytes, [2] query counter, [3] overflow count */
+    /* ctr: [0] arena cursor, [1] work bytes, [2] query counter, [3] overflow count, [4] counter of
+     * the small queries (warp mode) */
     /* the next query of the list order[0..nq) (or 0..nq-1), -1 past its end */
     auto fetch = [&]() {
         const int j = (int)atomicAdd(&ctr[2], 1ull);
@@ -982,85 +1074,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
             const int64_t it = i0 + k;
             /* stop once every item is taken or the set has overflowed (warp-uniform reads) */
             if (it >= i1 || __shfl_sync(FULL, *(volatile int*)&ovf_sh, 0)) break;
-            int2 r = items[it];
-            const bool all = r.x < 0;
-            r.x &= ~kAllHit;
-            const int head_end = min(r.y, (r.x + 3) & ~3);
-            const int vb = head_end, ve = head_end + ((r.y - head_end) & ~3);
-            if (all) {
-                /* every point of the item is a hit: only the ids are read, and the first id of
-                 * each run of equal ids is inserted (head and tail points always) */
-                if (lane == 0) allp += (unsigned long long)(r.y - r.x);
-                for (int i = r.x + lane; i < head_end; i += 32) hs_insert<HB>(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
-                for (int i = ve + lane; i < r.y; i += 32) hs_insert<HB>(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
-                const int4* T4 = reinterpret_cast<const int4*>(tid + vb);
-                const int nv = (ve - vb) >> 2;
-                int carry = -1;
-                int4 nt = make_int4(-1, -1, -1, -1);
-                if (lane < nv) nt = __ldg(T4 + lane);
-                for (int k0 = 0; k0 < nv; k0 += 32) {
-                    const int kk = k0 + lane;
-                    int4 tt = nt;
-                    if (kk + 32 < nv) nt = __ldg(T4 + kk + 32);
-                    if (kk >= nv) tt = make_int4(-1, -1, -1, -1);
-                    int prev = __shfl_up_sync(FULL, tt.w, 1);
-                    if (lane == 0) prev = carry;
-                    carry = __shfl_sync(FULL, tt.w, 31);
-                    insert_runs<HB>(tab, buf, prev, tt.x, tt.y, tt.z, tt.w, &cnt_sh, &ovf_sh);
-                }
-                continue;
-            }
-            if (lane == 0) cand += (unsigned long long)(r.y - r.x);
-            /* unaligned head and tail points: plain inserts */
-            for (int i = r.x + lane; i < head_end; i += 32)
-                if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
-                    hs_insert<HB>(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
-                    hits++;
-                }
-            for (int i = ve + lane; i < r.y; i += 32)
-                if (in_box(q, __ldg(X + i), __ldg(Y + i))) {
-                    hs_insert<HB>(tab, buf, __ldg(tid + i), &cnt_sh, &ovf_sh);
-                    hits++;
-                }
-            const float4* X4 = reinterpret_cast<const float4*>(X + vb);
-            const float4* Y4 = reinterpret_cast<const float4*>(Y + vb);
-            const int4* T4 = reinterpret_cast<const int4*>(tid + vb);
-            const int nv = (ve - vb) >> 2;
-            int carry = -1; /* tid of the last point of the previous step if it was a hit */
-            /* one step tests 4 points per lane; the next step's x, y and ids are loaded before the
-             * current step is tested (the ids unconditionally: most candidates are hits, and a
-             * load issued only after the test put the whole L2 latency on every step) */
-            float4 nx = make_float4(0.f, 0.f, 0.f, 0.f), ny = nx;
-            int4 nt = make_int4(-1, -1, -1, -1);
-            if (lane < nv) {
-                nx = __ldg(X4 + lane);
-                ny = __ldg(Y4 + lane);
-                nt = __ldg(T4 + lane);
-            }
-            for (int k0 = 0; k0 < nv; k0 += 32) {
-                const int kk = k0 + lane;
-                const float4 x = nx, y = ny;
-                const int4 tt = nt;
-                if (kk + 32 < nv) {
-                    nx = __ldg(X4 + kk + 32);
-                    ny = __ldg(Y4 + kk + 32);
-                    nt = __ldg(T4 + kk + 32);
-                }
-                int t0 = -1, t1 = -1, t2 = -1, t3 = -1;
-                if (kk < nv) {
-                    const bool h0 = in_box(q, x.x, y.x), h1 = in_box(q, x.y, y.y);
-                    const bool h2 = in_box(q, x.z, y.z), h3 = in_box(q, x.w, y.w);
-                    t0 = h0 ? tt.x : -1;
-                    t1 = h1 ? tt.y : -1;
-                    t2 = h2 ? tt.z : -1;
-                    t3 = h3 ? tt.w : -1;
-                    hits += (unsigned long long)(h0 + h1 + h2 + h3);
-                }
-                int prev = __shfl_up_sync(FULL, t3, 1);
-                if (lane == 0) prev = carry;
-                carry = __shfl_sync(FULL, t3, 31);
-                insert_runs<HB>(tab, buf, prev, t0, t1, t2, t3, &cnt_sh, &ovf_sh);
-            }
+            scan_item<HB>(items[it], q, X, Y, tid, tab, buf, &cnt_sh, &ovf_sh, cand, hits, allp);
         }
         /* algorithmic bytes: x and y of every tested point, the id of every hit, the id of every
          * point of an all-hit item */
@@ -1156,6 +1170,80 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_range_hash(const gat_mbb* que
             cnt_sh = 0;
             ovf_sh = 0;
             item_sh = 0;
+        }
+    }
+    /* Warp mode: the small queries small[0..ns), one per warp, each with a set of 2^WB slots of
+     * its own (the warp's share of the block's shared memory, all clear after the block mode) and
+     * no block barrier; the id list is sorted by the warp (runs of 32, then run ranks). A query
+     * with more distinct ids than its set holds goes on the overflow list for the bitmap kernel. */
+    if (ns > 0) {
+        constexpr int kWarps = NT / 32;
+        constexpr int WB = HB - (kWarps == 8 ? 3 : kWarps == 4 ? 2 : 1);
+        __shared__ int wcnt[kWarps], wovf[kWarps];
+        int* wtab = hs_smem + warp * (1 << WB);
+        int* wlist = hs_smem + kHashSize + warp * (1 << (WB - 1));
+        if (lane == 0) {
+            wcnt[warp] = 0;
+            wovf[warp] = 0;
+        }
+        __syncwarp();
+        for (;;) {
+            int j = 0;
+            if (lane == 0) j = (int)atomicAdd(&ctr[4], 1ull);
+            j = __shfl_sync(FULL, j, 0);
+            if (j >= ns) break;
+            const int qi = small[j];
+            const Box q = load_box(queries, qi);
+            const int64_t i0 = ioff[(int64_t)qi * kSub], i1 = ioff[(int64_t)(qi + 1) * kSub];
+            unsigned long long cand = 0, hits = 0, allp = 0;
+            for (int64_t it = i0; it < i1; it++) {
+                __syncwarp();
+                if (__shfl_sync(FULL, *(volatile int*)&wovf[warp], 0)) break;
+                scan_item<WB>(items[it], q, X, Y, tid, wtab, wlist, &wcnt[warp], &wovf[warp], cand, hits, allp);
+            }
+            my_work += 8ull * cand + 4ull * hits + 4ull * allp;
+            __syncwarp();
+            const int m = wcnt[warp];
+            if (wovf[warp]) {
+                if (lane == 0) {
+                    const int o = (int)atomicAdd(&ctr[3], 1ull);
+                    ovf_list[o] = qi;
+                    segcnt[qi] = 0;
+                    segbase[qi] = 0;
+                }
+                for (int i = lane; i < (1 << WB); i += 32) wtab[i] = -1;
+            } else {
+                const int runs = (m + 31) >> 5;
+                for (int c = 0; c < runs; c++) {
+                    const int i = 32 * c + lane;
+                    const int v = warp_sort32(i < m ? wlist[i] : INT_MAX);
+                    __syncwarp();
+                    wlist[i] = v;
+                }
+                unsigned long long b = 0;
+                if (lane == 0) {
+                    b = atomicAdd(&ctr[0], (unsigned long long)m);
+                    segcnt[qi] = m;
+                    segbase[qi] = (int64_t)b;
+                }
+                const int64_t base = (int64_t)__shfl_sync(FULL, b, 0);
+                const bool write = base + m <= cap;
+                __syncwarp();
+                for (int i = lane; i < m; i += 32) {
+                    const int x = wlist[i], own = i >> 5;
+                    int rank = i & 31;
+                    for (int c = 0; c < runs; c++)
+                        if (c != own) rank += lower_bound32(wlist + 32 * c, x);
+                    if (write) arena[base + rank] = (uint32_t)x;
+                    hs_erase<WB>(wtab, x);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                wcnt[warp] = 0;
+                wovf[warp] = 0;
+            }
+            __syncwarp();
         }
     }
     if (work) {
@@ -1489,8 +1577,8 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
     /* the hash kernel's two shapes (256 threads / 8192 slots, 128 threads / 4096 slots) */
     int hgrid[3] = {0, 0, 0}, hper[3] = {0, 0, 0};
     size_t hsmem[3] = {0, (size_t)(8192 + 4096) * sizeof(int), (size_t)(4096 + 2048) * sizeof(int)};
-    /* shape 3: the batch split by size, queries with more than kSmallItems candidate items on the
-     * 256-thread shape and the others on the 128-thread one (split[0..ns) small, [ns, nq) large) */
+    /* shape 3: the batch split by size, queries with more than kSmallItems candidate items in
+     * 256-thread block mode and the others one per warp (split[0..ns) small, [ns, nq) large) */
     int* split = nullptr;
     int ns = -1;
     auto make_split = [&]() -> int {
@@ -1545,28 +1633,26 @@ int run_batch(gat_ctx* ctx, const gat_index* ix, const gat_mbb* d_q, int nq, int
         if (!arena) return st;
         cap = (int64_t)(ctx->slot_bytes[S_RANGE_ARENA] / 4);
         /* cursor: [0] arena entries, [1] work bytes, [2] query counter, [3] overflowed queries */
-        /* one shape over the query list lst[0..n) (lst null: 0..n-1) */
-        auto hash_run = [&](int sh, const int* lst, int n, unsigned long long* work) {
-            if (n <= 0) return;
+        /* one shape over the query list lst[0..n) (lst null: 0..n-1), and the small queries
+         * sm[0..n_sm) in warp mode after it */
+        auto hash_run = [&](int sh, const int* lst, int n, const int* sm, int n_sm, unsigned long long* work) {
+            const int g = std::max(1, std::min(n + n_sm, hper[sh == 2 ? 2 : 1]));
             if (sh == 2)
-                k_range_hash<128, 12><<<std::min(n, hper[2]), 128, hsmem[2], s>>>(
-                    d_q, n, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap, cursor, segbase, segcnt, ovf_list, work, lst);
+                k_range_hash<128, 12><<<g, 128, hsmem[2], s>>>(d_q, n, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap,
+                                                               cursor, segbase, segcnt, ovf_list, work, lst, sm, n_sm);
             else
-                k_range_hash<256, 13><<<std::min(n, hper[1]), 256, hsmem[1], s>>>(
-                    d_q, n, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap, cursor, segbase, segcnt, ovf_list, work, lst);
+                k_range_hash<256, 13><<<g, 256, hsmem[1], s>>>(d_q, n, ioff, items, ix->d_x, ix->d_y, ix->d_tid, arena, cap,
+                                                               cursor, segbase, segcnt, ovf_list, work, lst, sm, n_sm);
             count_launch(ctx);
         };
         auto hash_launch = [&](int sh, unsigned long long* work) {
-            cudaError_t e = cudaMemsetAsync(cursor, 0, 4 * sizeof(unsigned long long), s);
+            cudaError_t e = cudaMemsetAsync(cursor, 0, 5 * sizeof(unsigned long long), s);
             if (e != cudaSuccess) return e;
-            if (sh == 3) {
-                /* the large queries first, then (query counter reset) the small ones */
-                hash_run(1, split + ns, nq - ns, work);
-                if ((e = cudaMemsetAsync(cursor + 2, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
-                hash_run(2, split, ns, work);
-            } else {
-                hash_run(sh, order, nq, work);
-            }
+            if (sh == 3)
+                /* the large queries in block mode, then the small ones one per warp */
+                hash_run(1, split + ns, nq - ns, split, ns, work);
+            else
+                hash_run(sh, order, nq, nullptr, 0, work);
             return cudaGetLastError();
         };
         /* the queries the hash kernel handed on (more distinct ids than its set holds) in the
