@@ -855,7 +855,7 @@ __global__ void k_split_scatter(int nq, const int* __restrict__ order, const int
 /* A set of 2^HB slots holds up to 2^(HB-1) ids (load factor <= 1/2): 48 KB of shared memory per
  * CTA for HB = 13 (256 threads), 24 KB for HB = 12 (128 threads). */
 constexpr int kRankSortMax = 512; /* lists up to this length are sorted by run ranks */
-constexpr int kSmallItems = 8;    /* shape 3: queries with at most this many items are scanned one per warp */
+constexpr int kSmallItems = 16;   /* shape 3: queries with at most this many items are scanned one per warp */
 
 template <int HB>
 __device__ __forceinline__ unsigned hs_slot(int t) { return ((unsigned)t * 2654435761u) >> (32 - HB); }

@@ -128,7 +128,7 @@ int gat_ctx_kernel_stats(gat_ctx* ctx, int kernel_class, double* ms, int64_t* la
  *   = autotune: the first batch of each (index kind, batch size rounded up to a power of two)
  *   class times the shapes on its own queries and keeps the fastest; 1 = 256 threads per CTA
  *   with an 8192-slot id set, 2 = 128 threads with a 4096-slot set, 3 = the batch split by size
- *   (queries with more than 8 candidate items on shape 1, the others one per warp with a
+ *   (queries with more than 16 candidate items on shape 1, the others one per warp with a
  *   1024-slot set and no block barrier, in the same launch). Same results.
  *   Setting the knob clears the tuned table.
  * GAT_TUNE_EDR_RESERVE: percent of the SMs (0..90) that this context's persistent EDR grid
