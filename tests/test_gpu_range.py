@@ -196,8 +196,8 @@ def test_morton_grid_rejects_other_kinds(gpu_ctx, c1):
 
 @pytest.mark.parametrize("shape", [1, 2, 3])
 def test_hash_shapes(gpu_ctx, c1, shape):
-    """Every block shape of the batched id-set scan (256 threads, 128 threads, the batch split by
-    query size) returns the oracle's sets, on the Grid and on STIG."""
+    """Every block shape of the batched id-set scan (256 threads, 128 threads, small queries one
+    per warp after the others in block mode) returns the oracle's sets, on the Grid and on STIG."""
     from gat_b200 import _lib as L
     t, q, db = c1
     qq = np.concatenate([q] * 3)  # enough queries for the locality order
