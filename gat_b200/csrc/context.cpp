@@ -90,6 +90,7 @@ void free_slots(gat_ctx* ctx) {
 
 void* host_stage(gat_ctx* ctx, size_t bytes, int* status) {
     if (bytes <= ctx->h_stage_bytes) return ctx->h_stage;
+    const size_t had = ctx->h_stage_bytes;
     if (ctx->h_stage) {
         /* an earlier copy may still read it */
         cudaStreamSynchronize(ctx->stream);
@@ -97,7 +98,7 @@ void* host_stage(gat_ctx* ctx, size_t bytes, int* status) {
         ctx->h_stage = nullptr;
         ctx->h_stage_bytes = 0;
     }
-    const size_t nb = std::max<size_t>(bytes, (size_t)64 << 10);
+    const size_t nb = std::max<size_t>(std::max<size_t>(bytes, 2 * had), (size_t)64 << 10); /* grows by doubling */
     void* p = nullptr;
     cudaError_t e = cudaMallocHost(&p, nb);
     if (e != cudaSuccess) {

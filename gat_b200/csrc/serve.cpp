@@ -68,10 +68,11 @@ struct PinnedArena {
     std::vector<char> fallback; /* a context without a device (queries then fail anyway) */
     char* get(size_t b) {
         if (b <= bytes) return p;
+        const size_t had = bytes;
         if (p) cudaFreeHost(p);
         p = nullptr;
         bytes = 0;
-        const size_t nb = std::max<size_t>(b, (size_t)4 << 20);
+        const size_t nb = std::max<size_t>(std::max<size_t>(b, 2 * had), (size_t)4 << 20);
         void* q = nullptr;
         if (cudaMallocHost(&q, nb) != cudaSuccess) {
             cudaGetLastError();
