@@ -435,10 +435,11 @@ def hbm_peak():
     return float(p.get("hbm_gbs", 6650.0)), ("measured" if "hbm_gbs" in p else "fallback")
 
 
-# DRAM read + write / algorithmic bytes of k_range_hash, from a one-pass ncu capture (dram__bytes_read.sum,
-# dram__bytes_write.sum) of the C3 batch on the 1M-walk set: Grid (3.258 + 0.087) GB / 20.79 GB, FSG
-# (5.333 + 0.088) GB / 41.29 GB. The locality order serves neighbouring queries' points from L2.
-RANGE_TRAFFIC_RATIO = {"grid": 0.161, "fsg": 0.131}
+# DRAM read + write / algorithmic bytes of k_range_hash, from one-pass ncu captures (dram__bytes_read.sum,
+# dram__bytes_write.sum) of the C3 batch on the 1M-walk set in the tuned shape (small queries one per warp):
+# Grid (4.319 + 0.088) GB / 20.79 GB; FSG (block mode) (5.333 + 0.088) GB / 41.29 GB. The locality order serves
+# neighbouring queries' points from L2.
+RANGE_TRAFFIC_RATIO = {"grid": 0.212, "fsg": 0.131}
 
 
 def range_roofline(st, name, index="grid"):
